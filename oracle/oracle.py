@@ -1,0 +1,401 @@
+"""ctypes front end of the C oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+legs import this module.  It loads ``oracle/_build/libraptor_oracle.so``
+(building it first when it is missing and gcc is available) and, for
+cross-checks in the build container, ``oracle/_ref/libraptor_seq_ref.so``.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_I = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_P = C.c_void_p
+
+RELAX = {"jacobi": 0, "sor": 1, "ssor": 2, "l1_jacobi": 3, "mc_sor": 4, "mc_ssor": 5}
+INTERP = {"mod_classical": 1, "extended": 2}
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("solver", C.c_int), ("interp", C.c_int), ("relax", C.c_int),
+        ("jacobi_compat", C.c_int), ("num_smooth_sweeps", C.c_int),
+        ("max_coarse", C.c_int), ("max_levels", C.c_int), ("max_iterations", C.c_int),
+        ("strong_threshold", C.c_double), ("relax_weight", C.c_double),
+        ("solve_tol", C.c_double), ("interp_filter", C.c_double),
+        ("prolong_weight", C.c_double), ("prolong_smooth_steps", C.c_int),
+        ("seed_offset", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        so = _build.ORACLE_SO
+        src = os.path.join(os.path.dirname(so), "..", "raptor_oracle.c")
+        if not os.path.exists(so) or (os.path.exists(src) and
+                                      os.path.getmtime(src) > os.path.getmtime(so)):
+            _build.build_oracle()
+        L = C.CDLL(so)
+        L.oc_csr_new.restype = _P
+        L.oc_csr_new.argtypes = [C.c_int, C.c_int, C.c_int, _I, _I, _D]
+        L.oc_csr_free.argtypes = [_P]
+        L.oc_csr_info.argtypes = [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.oc_csr_export.argtypes = [_P, _I, _I, _D]
+        L.oc_csr_sort.argtypes = [_P]
+        L.oc_csr_move_diag.argtypes = [_P]
+        L.oc_diffusion_stencil_2d.argtypes = [C.c_double, C.c_double, _D]
+        L.oc_laplace_stencil_27pt.argtypes = [_D]
+        L.oc_stencil_grid.restype = _P
+        L.oc_stencil_grid.argtypes = [_D, _I, C.c_int]
+        for f in ("oc_spmv", "oc_spmv_T", "oc_spmv_append"):
+            getattr(L, f).argtypes = [_P, _D, _D]
+        L.oc_residual.argtypes = [_P, _D, _D, _D]
+        L.oc_classical_strength.restype = _P
+        L.oc_classical_strength.argtypes = [_P, C.c_double]
+        L.oc_symmetric_strength.restype = _P
+        L.oc_symmetric_strength.argtypes = [_P, C.c_double]
+        L.oc_split_pmis.argtypes = [_P, _D, _I]
+        L.oc_mis2.argtypes = [_P, _D, _I]
+        L.oc_aggregate.restype = C.c_int
+        L.oc_aggregate.argtypes = [_P, _P, _I, _I, C.c_void_p]
+        L.oc_fit_candidates.restype = _P
+        L.oc_fit_candidates.argtypes = [C.c_int, C.c_int, _I, _D, _D, C.c_double]
+        L.oc_jacobi_prolongation.restype = _P
+        L.oc_jacobi_prolongation.argtypes = [_P, _P, C.c_double, C.c_int]
+        L.oc_mod_classical_interp.restype = _P
+        L.oc_mod_classical_interp.argtypes = [_P, _P, _I]
+        L.oc_extended_interp.restype = _P
+        L.oc_extended_interp.argtypes = [_P, _P, _I, C.c_double]
+        for f in ("oc_spgemm", "oc_spgemm_T"):
+            getattr(L, f).restype = _P
+            getattr(L, f).argtypes = [_P, _P]
+        L.oc_rap.restype = _P
+        L.oc_rap.argtypes = [_P, _P, C.c_int]
+        L.oc_colour_rows.restype = C.c_int
+        L.oc_colour_rows.argtypes = [_P, _I]
+        L.oc_default_opts.argtypes = [C.POINTER(Opts)]
+        L.oc_ml_setup.restype = _P
+        L.oc_ml_setup.argtypes = [_P, C.POINTER(Opts), C.c_void_p, C.c_int]
+        L.oc_ml_free.argtypes = [_P]
+        L.oc_ml_num_levels.restype = C.c_int
+        L.oc_ml_num_levels.argtypes = [_P]
+        L.oc_ml_level_A.restype = _P
+        L.oc_ml_level_A.argtypes = [_P, C.c_int]
+        L.oc_ml_level_P.restype = _P
+        L.oc_ml_level_P.argtypes = [_P, C.c_int]
+        L.oc_ml_cycle.argtypes = [_P, _D, _D]
+        L.oc_ml_solve.restype = C.c_int
+        L.oc_ml_solve.argtypes = [_P, _D, _D, _D, C.c_int]
+        L.oc_pcg.restype = C.c_int
+        L.oc_pcg.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+        L.oc_cg.restype = C.c_int
+        L.oc_cg.argtypes = [_P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+        L.oc_bicgstab.restype = C.c_int
+        L.oc_bicgstab.argtypes = [_P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+        L.oc_pre_bicgstab.restype = C.c_int
+        L.oc_pre_bicgstab.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+        L.oc_form_rand_weights.argtypes = [C.c_int, C.c_int, _D]
+        L.oc_dense_lu.argtypes = [C.c_int, _D, _I]
+        L.oc_dense_lu_solve.argtypes = [C.c_int, _D, _I, _D]
+        _lib = L
+    return _lib
+
+
+class CSR:
+    """Owning handle on an oracle CSR matrix."""
+
+    def __init__(self, ptr):
+        self.ptr = ptr
+
+    @classmethod
+    def from_arrays(cls, n_rows, n_cols, rowptr, cols, vals):
+        rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+        ci = np.ascontiguousarray(cols, dtype=np.int32)
+        cv = np.ascontiguousarray(vals, dtype=np.float64)
+        if len(ci) == 0:
+            ci = np.zeros(1, np.int32)
+            cv = np.zeros(1, np.float64)
+        return cls(lib().oc_csr_new(int(n_rows), int(n_cols), int(rp[-1]), rp, ci, cv))
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _lib is not None:
+            _lib.oc_csr_free(self.ptr)
+            self.ptr = None
+
+    @property
+    def shape(self):
+        r, c, z = C.c_int(), C.c_int(), C.c_int()
+        lib().oc_csr_info(self.ptr, C.byref(r), C.byref(c), C.byref(z))
+        return r.value, c.value, z.value
+
+    def arrays(self):
+        n, m, z = self.shape
+        rp = np.zeros(n + 1, np.int32)
+        ci = np.zeros(max(z, 1), np.int32)
+        cv = np.zeros(max(z, 1), np.float64)
+        lib().oc_csr_export(self.ptr, rp, ci, cv)
+        return rp, ci[:z], cv[:z]
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        n, m, _ = self.shape
+        rp, ci, cv = self.arrays()
+        return sp.csr_matrix((cv, ci, rp), shape=(n, m))
+
+
+class Borrowed(CSR):
+    """CSR owned by an oracle hierarchy (not freed here)."""
+
+    def __del__(self):
+        pass
+
+
+def stencil_grid(stencil, grid):
+    st = np.ascontiguousarray(stencil, np.float64)
+    g = np.ascontiguousarray(grid, np.int32)
+    return CSR(lib().oc_stencil_grid(st, g, len(g)))
+
+
+def diffusion_stencil_2d(eps=1.0, theta=0.0):
+    out = np.zeros(9)
+    lib().oc_diffusion_stencil_2d(eps, theta, out)
+    return out
+
+
+def laplace_stencil_27pt():
+    out = np.zeros(27)
+    lib().oc_laplace_stencil_27pt(out)
+    return out
+
+
+def spmv(A, x):
+    b = np.zeros(A.shape[0])
+    lib().oc_spmv(A.ptr, np.ascontiguousarray(x, np.float64), b)
+    return b
+
+
+def spmv_T(A, x):
+    b = np.zeros(A.shape[1])
+    lib().oc_spmv_T(A.ptr, np.ascontiguousarray(x, np.float64), b)
+    return b
+
+
+def residual(A, x, b):
+    r = np.zeros(A.shape[0])
+    lib().oc_residual(A.ptr, np.ascontiguousarray(x, np.float64),
+                      np.ascontiguousarray(b, np.float64), r)
+    return r
+
+
+def sort_diag_first(A):
+    lib().oc_csr_sort(A.ptr)
+    lib().oc_csr_move_diag(A.ptr)
+    return A
+
+
+def classical_strength(A, theta):
+    return CSR(lib().oc_classical_strength(A.ptr, theta))
+
+
+def symmetric_strength(A, theta):
+    return CSR(lib().oc_symmetric_strength(A.ptr, theta))
+
+
+def split_pmis(S, weights):
+    st = np.zeros(S.shape[0], np.int32)
+    lib().oc_split_pmis(S.ptr, np.ascontiguousarray(weights[: S.shape[0]], np.float64), st)
+    return st
+
+
+def mis2(S, weights):
+    st = np.zeros(S.shape[0], np.int32)
+    lib().oc_mis2(S.ptr, np.ascontiguousarray(weights[: S.shape[0]], np.float64), st)
+    return st
+
+
+def aggregate(A, S, states, r=None):
+    agg = np.zeros(S.shape[0], np.int32)
+    st = np.ascontiguousarray(states, np.int32).copy()
+    rr = None
+    if r is not None:
+        rr = np.ascontiguousarray(r, np.float64)
+    n_aggs = lib().oc_aggregate(A.ptr, S.ptr, st, agg,
+                                rr.ctypes.data_as(C.c_void_p) if rr is not None else None)
+    return n_aggs, agg
+
+
+def fit_candidates(n, n_aggs, agg, B):
+    R = np.zeros(max(n_aggs, 1))
+    T = CSR(lib().oc_fit_candidates(n, n_aggs, np.ascontiguousarray(agg, np.int32),
+                                    np.ascontiguousarray(B, np.float64), R, 1e-10))
+    return T, R[:n_aggs]
+
+
+def jacobi_prolongation(A, T, omega=4.0 / 3, steps=1):
+    return CSR(lib().oc_jacobi_prolongation(A.ptr, T.ptr, omega, steps))
+
+
+def interpolation(A, S, states, kind="mod_classical", filt=0.0):
+    st = np.ascontiguousarray(states, np.int32)
+    if kind == "extended":
+        return CSR(lib().oc_extended_interp(A.ptr, S.ptr, st, filt))
+    return CSR(lib().oc_mod_classical_interp(A.ptr, S.ptr, st))
+
+
+def spgemm(A, B):
+    return CSR(lib().oc_spgemm(A.ptr, B.ptr))
+
+
+def rap(A, P, diag_first=True):
+    return CSR(lib().oc_rap(A.ptr, P.ptr, 1 if diag_first else 0))
+
+
+def colour_rows(A):
+    c = np.zeros(A.shape[0], np.int32)
+    nc = lib().oc_colour_rows(A.ptr, c)
+    return nc, c
+
+
+def rand_weights(n, first_row=0):
+    w = np.zeros(max(n, 1))
+    lib().oc_form_rand_weights(n, first_row, w)
+    return w[:n]
+
+
+def default_opts(**kw):
+    o = Opts()
+    lib().oc_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if k == "relax" and isinstance(v, str):
+            v = RELAX[v]
+        if k == "interp" and isinstance(v, str):
+            v = INTERP[v]
+        if k == "solver" and isinstance(v, str):
+            v = {"rs": 0, "sa": 1}[v]
+        setattr(o, k, v)
+    return o
+
+
+class Hierarchy:
+    """An oracle AMG hierarchy (ParMultilevel restated)."""
+
+    def __init__(self, A, weights=None, **kw):
+        self.opts = default_opts(**kw)
+        w = None
+        nw = 0
+        if weights is not None:
+            self._w = np.ascontiguousarray(weights, np.float64)
+            w = self._w.ctypes.data_as(C.c_void_p)
+            nw = len(self._w)
+        self.ptr = lib().oc_ml_setup(A.ptr, C.byref(self.opts), w, nw)
+        self.n = A.shape[0]
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _lib is not None:
+            _lib.oc_ml_free(self.ptr)
+            self.ptr = None
+
+    @property
+    def num_levels(self):
+        return lib().oc_ml_num_levels(self.ptr)
+
+    def A(self, l):
+        return Borrowed(lib().oc_ml_level_A(self.ptr, l))
+
+    def P(self, l):
+        return Borrowed(lib().oc_ml_level_P(self.ptr, l))
+
+    def cycle(self, x, b):
+        x = np.ascontiguousarray(x, np.float64).copy()
+        lib().oc_ml_cycle(self.ptr, x, np.ascontiguousarray(b, np.float64))
+        return x
+
+    def solve(self, x, b, cap=1000):
+        x = np.ascontiguousarray(x, np.float64).copy()
+        hist = np.zeros(cap)
+        it = lib().oc_ml_solve(self.ptr, x, np.ascontiguousarray(b, np.float64), hist, cap)
+        return x, it, hist[: min(it + 1, cap)]
+
+
+def pcg(A, ml, x, b, tol=1e-5, max_iter=-1, cap=10000):
+    x = np.ascontiguousarray(x, np.float64).copy()
+    hist = np.zeros(cap)
+    nh = lib().oc_pcg(A.ptr, ml.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter,
+                      hist, cap)
+    return x, hist[: min(abs(nh), cap)], nh
+
+
+def cg(A, x, b, tol=1e-5, max_iter=-1, cap=10000):
+    x = np.ascontiguousarray(x, np.float64).copy()
+    hist = np.zeros(cap)
+    nh = lib().oc_cg(A.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter, hist, cap)
+    return x, hist[: min(abs(nh), cap)]
+
+
+def bicgstab(A, x, b, tol=1e-5, max_iter=-1, cap=10000, ml=None):
+    x = np.ascontiguousarray(x, np.float64).copy()
+    hist = np.zeros(cap)
+    if ml is None:
+        nh = lib().oc_bicgstab(A.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter,
+                               hist, cap)
+    else:
+        nh = lib().oc_pre_bicgstab(A.ptr, ml.ptr, x, np.ascontiguousarray(b, np.float64), tol,
+                                   max_iter, hist, cap)
+    return x, hist[: min(abs(nh), cap)]
+
+
+# --- the reference's own sequential routines (build container only) --------
+
+_ref = None
+
+
+def ref_lib():
+    """The reference's sequential sources compiled under oracle/_ref, or None."""
+    global _ref
+    if _ref is None:
+        so = _build.REF_SO
+        if not os.path.exists(so):
+            try:
+                so = _build.build_reference()
+            except Exception:  # noqa: BLE001 - no compiler or no checkout
+                so = None
+        if not so or not os.path.exists(so):
+            return None
+        L = C.CDLL(so)
+        L.rs_free.argtypes = [_P]
+        L.rs_info.argtypes = [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.rs_export.argtypes = [_P, _I, _I, _D]
+        L.rs_spmv.argtypes = [C.c_int, C.c_int, _I, _I, _D, _D, _D]
+        L.rs_residual.argtypes = [C.c_int, C.c_int, _I, _I, _D, _D, _D, _D]
+        for f in ("rs_spgemm", "rs_spgemm_T"):
+            getattr(L, f).restype = _P
+            getattr(L, f).argtypes = [C.c_int, C.c_int, _I, _I, _D, C.c_int, C.c_int, _I, _I, _D]
+        L.rs_strength.restype = _P
+        L.rs_strength.argtypes = [C.c_int, _I, _I, _D, C.c_double, C.c_int]
+        L.rs_split_pmis.argtypes = [C.c_int, _I, _I, _D, _D, _I]
+        L.rs_mis2.argtypes = [C.c_int, _I, _I, _D, _D, _I]
+        L.rs_interp.restype = _P
+        L.rs_interp.argtypes = [C.c_int, _I, _I, _D, _I, _I, _D, _I, C.c_int]
+        _ref = L
+    return _ref
+
+
+def ref_take(ptr):
+    """Copy a shim result into numpy arrays and free it."""
+    L = ref_lib()
+    r, c, z = C.c_int(), C.c_int(), C.c_int()
+    L.rs_info(ptr, C.byref(r), C.byref(c), C.byref(z))
+    rp = np.zeros(r.value + 1, np.int32)
+    ci = np.zeros(max(z.value, 1), np.int32)
+    cv = np.zeros(max(z.value, 1), np.float64)
+    L.rs_export(ptr, rp, ci, cv)
+    L.rs_free(ptr)
+    return (r.value, c.value), rp, ci[: z.value], cv[: z.value]
