@@ -1,0 +1,196 @@
+/*
+ * raptor_b200.h -- C ABI of libraptor_b200, a B200-native (sm_100a) rebuild
+ * of RAPtor's algebraic-multigrid solve path at MPI world size 1.
+ *
+ * Plain C: opaque handles, pointers and sizes, integer status codes.  Every
+ * call is ordered on the library stream (rb_set_stream) and returns RB_OK or a
+ * negative rb_status; rb_last_error() describes the last failure of the
+ * calling thread.  One handle is used by one host thread at a time.
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the reference project 13manan/raptor).  At world size 1 a ParCSRMatrix is
+ * its on_proc block, so one device CSR matrix stands for it.
+ */
+#ifndef RAPTOR_B200_H
+#define RAPTOR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------- status */
+typedef enum rb_status {
+    RB_OK = 0,
+    RB_ERR_INVALID = -1,       /* bad argument or size mismatch (par_vector.cpp:105-111 exits) */
+    RB_ERR_CUDA = -2,          /* CUDA runtime failure */
+    RB_ERR_OOM = -3,           /* device allocation failed */
+    RB_ERR_BREAKDOWN = -4,     /* p.Ap < 0 in CG (par_cg.cpp:195-202 exits) or NaN in a dot */
+    RB_ERR_NOT_CONVERGED = -5, /* iteration limit reached without meeting the tolerance */
+    RB_ERR_NO_DEVICE = -6      /* no CUDA device or the kernels are missing for it */
+} rb_status;
+
+typedef struct rb_csr_s* rb_csr;   /* device CSR matrix, FP64 values, int32 indices */
+typedef struct rb_vec_s* rb_vec;   /* device FP64 vector */
+typedef struct rb_amg_s* rb_amg;   /* AMG hierarchy (ParMultilevel) */
+
+/* Description of the last failure on this thread ("" when none). */
+const char* rb_last_error(void);
+/* Select the CUDA device and create the library stream. */
+int rb_init(int device);
+/* Order all later calls on a caller-owned stream (0 = library stream). */
+int rb_set_stream(void* cuda_stream);
+/* Wait for all work queued on the library stream. */
+int rb_synchronize(void);
+/* Library version string. */
+const char* rb_version(void);
+
+/* ------------------------------------------------------------ containers */
+/* ParCSRMatrix(...) + finalize (core/par_matrix.hpp:481-611, par_matrix.cpp:111-157).
+ * Copies host (on_device=0) or device (on_device=1) arrays. */
+int rb_csr_create(int n_rows, int n_cols, int64_t nnz, const int* rowptr, const int* cols,
+                  const double* vals, int on_device, rb_csr* out);
+int rb_csr_destroy(rb_csr A);
+int rb_csr_info(rb_csr A, int* n_rows, int* n_cols, int64_t* nnz);
+/* Copy the matrix to host buffers of n_rows+1, nnz and nnz entries. */
+int rb_csr_download(rb_csr A, int* rowptr, int* cols, double* vals);
+/* Device pointers of the matrix arrays (borrowed). */
+int rb_csr_device_arrays(rb_csr A, int** rowptr, int** cols, double** vals);
+/* CSRMatrix::sort then move_diag (core/matrix.cpp:588-618, :730-786). */
+int rb_csr_sort_diag_first(rb_csr A);
+/* Transpose with rows of the result in increasing source-row order
+ * (CSRMatrix::transpose / CSR_to_CSC, core/matrix.cpp:148-154, :492-538). */
+int rb_csr_transpose(rb_csr A, rb_csr* out);
+
+/* ParVector (core/par_vector.hpp:44-176) */
+int rb_vec_create(int n, rb_vec* out);
+int rb_vec_destroy(rb_vec v);
+int rb_vec_size(rb_vec v, int* n);
+int rb_vec_upload(rb_vec v, const double* host);
+int rb_vec_download(rb_vec v, double* host);
+int rb_vec_set(rb_vec v, double value);          /* ParVector::set_const_value */
+int rb_vec_device_ptr(rb_vec v, double** ptr);
+int rb_vec_copy(rb_vec dst, rb_vec src);         /* ParVector::copy */
+int rb_vec_axpy(rb_vec y, rb_vec x, double a);   /* ParVector::axpy, vector.cpp:53-59 */
+int rb_vec_scale(rb_vec y, double a);            /* ParVector::scale, vector.cpp:89-95 */
+int rb_vec_dot(rb_vec a, rb_vec b, double* out); /* ParVector::inner_product, par_vector.cpp:101-121 */
+int rb_vec_norm2(rb_vec a, double* out);         /* ParVector::norm(2), par_vector.cpp:88-98 */
+
+/* --------------------------------------------------------- SpMV family */
+/* ParMatrix::mult, b = A x (util/linalg/par_spmv.cpp:25-59 -> spmv.cpp:52-67) */
+int rb_spmv(rb_csr A, rb_vec x, rb_vec b);
+/* ParMatrix::residual, r = b - A x (par_spmv.cpp:215-252 -> spmv.cpp:69-85) */
+int rb_residual(rb_csr A, rb_vec x, rb_vec b, rb_vec r);
+/* ParMatrix::mult_T, b = A^T x (par_spmv.cpp:157-187 -> spmv.cpp:150-163) */
+int rb_spmv_T(rb_csr A, rb_vec x, rb_vec b);
+/* ParMatrix::mult_append, b += A x (par_spmv.cpp:91-125 -> spmv.cpp:88-103) */
+int rb_spmv_append(rb_csr A, rb_vec x, rb_vec b);
+
+/* --------------------------------------------------------------- gallery */
+/* diffusion_stencil_2d (gallery/diffusion.hpp:58-85) */
+int rb_diffusion_stencil_2d(double eps, double theta, double* out9);
+/* laplace_stencil_27pt (gallery/laplacian27pt.hpp:27-37) */
+int rb_laplace_stencil_27pt(double* out27);
+/* par_stencil_grid (gallery/par_stencil.hpp:16-236) */
+int rb_stencil_grid(const double* stencil, const int* grid, int dim, rb_csr* out);
+/* readParMatrix for PETSc binary AIJ files (gallery/par_matrix_IO.cpp:22+) */
+int rb_read_petsc(const char* path, rb_csr* out);
+
+/* ----------------------------------------------------- setup components */
+#define RB_STRENGTH_CLASSICAL 0 /* strength_t Classical (core/types.hpp:158) */
+#define RB_STRENGTH_SYMMETRIC 1 /* strength_t Symmetric */
+#define RB_INTERP_MODCLASSICAL 1 /* interp_t ModClassical (core/types.hpp:161) */
+#define RB_INTERP_EXTENDED 2     /* interp_t Extended */
+
+/* ParCSRMatrix::strength (par_strength.cpp:536-546 -> :8-339 / :342-531).
+ * A must have its diagonal first (rb_csr_sort_diag_first). */
+int rb_strength(rb_csr A, int kind, double theta, rb_csr* S);
+/* split_pmis (ruge_stuben/par_cf_splitting.cpp:75-89, 1229-1381); weights has
+ * n_rows entries; states (host, n_rows) receive 1 = C, 0 = F, -2 = isolated. */
+int rb_split_pmis(rb_csr S, const double* weights, int* states);
+/* mod_classical_interpolation (par_interpolation.cpp:991-1451) and
+ * extended_interpolation + filter_interp (:280-989, :175-278). */
+int rb_interpolation(rb_csr A, rb_csr S, const int* states, int kind, double filter,
+                     rb_csr* P);
+/* C = A B (ParCSRMatrix::mult, par_matmult.cpp:73-107 -> matmult.cpp:71-137 +
+ * add.cpp:39-78): rows sorted by column, |c| <= 1e-16 dropped. */
+int rb_spgemm(rb_csr A, rb_csr B, rb_csr* C);
+/* A_c = P^T (A P) (par_matmult.cpp:141-196, 387-570), then sort + move_diag
+ * when diag_first (ruge_stuben/par_ruge_stuben_solver.hpp:139-143). */
+int rb_rap(rb_csr A, rb_csr P, int diag_first, rb_csr* Ac);
+
+/* -------------------------------------------------------------- hierarchy */
+#define RB_RELAX_JACOBI 0    /* relax_t Jacobi (core/types.hpp:164) */
+#define RB_RELAX_SOR 1       /* relax_t SOR: multicolour forward Gauss-Seidel stand-in */
+#define RB_RELAX_SSOR 2      /* relax_t SSOR: multicolour forward + backward */
+#define RB_RELAX_L1JACOBI 3  /* L1-Jacobi, x += w (b - A x) / sum_j |a_ij| */
+#define RB_SOLVER_RS 0       /* ParRugeStubenSolver */
+#define RB_SOLVER_SA 1       /* ParSmoothedAggregationSolver */
+#define RB_PREC_FP64 0
+#define RB_PREC_FP32 1       /* hierarchy values and V-cycle in FP32 */
+
+/* Fields of ParMultilevel (multilevel/par_multilevel.hpp:626-658),
+ * ParRugeStubenSolver (ruge_stuben/par_ruge_stuben_solver.hpp:15-25, 164-170)
+ * and ParSmoothedAggregationSolver (par_smoothed_aggregation_solver.hpp:17-32),
+ * plus the cycle precision and the reference-compatible Jacobi switch. */
+typedef struct rb_amg_opts {
+    int solver;               /* RB_SOLVER_RS / RB_SOLVER_SA */
+    int strength_type;        /* RB_STRENGTH_*; RS default Classical, SA Symmetric */
+    int interp_type;          /* RB_INTERP_* (RS) */
+    int relax_type;           /* RB_RELAX_* */
+    int num_smooth_sweeps;    /* 1 */
+    int max_coarse;           /* 50 */
+    int max_levels;           /* 25 */
+    int max_iterations;       /* 100 (solve) */
+    double strong_threshold;  /* 0.25 in the reference's examples */
+    double relax_weight;      /* 1.0 */
+    double solve_tol;         /* 1e-7 */
+    double interp_filter;     /* 0.3 (Extended) */
+    double prolong_weight;    /* 4/3 (SA) */
+    int prolong_smooth_steps; /* 1 (SA) */
+    int precision;            /* RB_PREC_FP64 / RB_PREC_FP32 */
+    int jacobi_compat;        /* 1: Jacobi leaves x unchanged, as par_relax.cpp:127,146 does */
+    int seed_offset;          /* first_local_row in srand(2448422 + first_local_row) */
+} rb_amg_opts;
+
+void rb_amg_default_opts(rb_amg_opts* opts);
+/* ParMultilevel::setup (par_multilevel.hpp:126-212 + extend_hierarchy +
+ * duplicate_coarse :229-339).  weights: n_rows values or NULL for the
+ * reference's glibc rand() weights. */
+int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_amg* out);
+int rb_amg_destroy(rb_amg ml);
+int rb_amg_num_levels(rb_amg ml, int* num_levels);
+/* rows and nonzeros of A_l and P_l (print_hierarchy, par_multilevel.hpp:540-563) */
+int rb_amg_level_info(rb_amg ml, int level, int* n_rows, int64_t* nnz_A, int64_t* nnz_P);
+/* FP64 copy of A_l (which=0), P_l (1) or R_l = P_l^T (2). */
+int rb_amg_level_matrix(rb_amg ml, int level, int which, rb_csr* out);
+/* C/F states of level l (host, n_rows). */
+int rb_amg_level_states(rb_amg ml, int level, int* states);
+/* ParMultilevel::cycle (par_multilevel.hpp:341-457): one V-cycle on x. */
+int rb_amg_cycle(rb_amg ml, rb_vec x, rb_vec b);
+/* ParMultilevel::solve (par_multilevel.hpp:459-538).  hist receives
+ * ||r_k||/||b|| for k = 0..iters (up to cap entries). */
+int rb_amg_solve(rb_amg ml, rb_vec x, rb_vec b, int* iters, double* hist, int cap);
+
+/* ------------------------------------------------------------------ Krylov */
+#define RB_PCG_REFERENCE 0 /* par_cg.cpp:121-263 exactly: stop on r.z < tol*sqrt(b.Mb) */
+#define RB_PCG_TRUE_RESIDUAL 1 /* stop on ||b - A x|| / ||b|| < tol */
+
+/* PCG (krylov/par_cg.cpp:121-263).  hist receives the reference's history
+ * (sqrt(r.z) then r.z/b.Mb) in RB_PCG_REFERENCE mode, ||r||/||b|| otherwise;
+ * n_hist receives the entry count. */
+int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, int mode,
+           double* hist, int cap, int* n_hist);
+/* CG (krylov/par_cg.cpp:8-118); hist = ||r||/||b||. */
+int rb_cg(rb_csr A, rb_vec x, rb_vec b, double tol, int max_iter, double* hist, int cap,
+          int* n_hist);
+/* BiCGStab (krylov/par_bicgstab.cpp:11-126) when ml is NULL, Pre_BiCGStab
+ * (:240-371, right-preconditioned) otherwise; hist = ||r||. */
+int rb_bicgstab(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter,
+                double* hist, int cap, int* n_hist);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

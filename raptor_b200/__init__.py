@@ -1,0 +1,430 @@
+"""raptor_b200 -- RAPtor's algebraic-multigrid solve path on one B200.
+
+A Python mirror of the reference's C++ API (13manan/raptor, world size 1)
+over the C ABI of libraptor_b200.so.  Names, argument meaning and error
+behaviour follow the reference:
+
+    A = par_stencil_grid(laplace_stencil_27pt(), [n, n, n])   # gallery/par_stencil.hpp
+    x = ParVector(A.global_num_rows); b = ParVector(A.global_num_rows)
+    x.set_const_value(1.0); A.mult(x, b); x.set_const_value(0.0)
+    ml = ParRugeStubenSolver(0.25, PMIS, Extended, Classical, L1Jacobi)
+    ml.setup(A)
+    res = []
+    PCG(A, ml, x, b, res, tol=1e-8)                             # krylov/par_cg.hpp
+
+Every computation runs in the CUDA library; importing works without a GPU,
+but any compute call then raises RaptorError(RB_ERR_NO_DEVICE).
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._capi import (AmgOpts, Breakdown, NotConverged, RaptorError, check, lib,  # noqa: F401
+                    last_error)
+
+# enums (core/types.hpp:158-164) --------------------------------------------
+Classical, Symmetric = 0, 1                 # strength_t
+RS, CLJP, Falgout, PMIS, HMIS = 0, 1, 2, 3, 4   # coarsen_t (PMIS is built)
+Direct, ModClassical, Extended = 0, 1, 2    # interp_t
+Jacobi, SOR, SSOR, L1Jacobi = 0, 1, 2, 3    # relax_t (+ L1-Jacobi)
+FP64, FP32 = 0, 1                           # cycle precision
+PCG_REFERENCE, PCG_TRUE_RESIDUAL = 0, 1
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class ParVector:
+    """Device FP64 vector (core/par_vector.hpp:44-176)."""
+
+    def __init__(self, global_n, local_n=None, first_local=0, values=None):
+        self.global_n = int(global_n)
+        self.local_n = self.global_n if local_n is None else int(local_n)
+        h = C.c_void_p()
+        check(lib().rb_vec_create(self.local_n, C.byref(h)))
+        self.h = h
+        if values is not None:
+            self.set_values(values)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().rb_vec_destroy(self.h)
+            except Exception:  # noqa: BLE001 - interpreter shutdown
+                pass
+            self.h = None
+
+    def __len__(self):
+        return self.local_n
+
+    def set_values(self, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        if v.shape != (self.local_n,):
+            raise RaptorError(-1, "vector size mismatch")
+        check(lib().rb_vec_upload(self.h, v))
+        return self
+
+    def numpy(self):
+        out = np.empty(self.local_n, dtype=np.float64)
+        check(lib().rb_vec_download(self.h, out))
+        return out
+
+    def set_const_value(self, v):
+        check(lib().rb_vec_set(self.h, float(v)))
+
+    def set_rand_values(self, seed=0):
+        self.set_values(np.random.default_rng(seed).random(self.local_n))
+
+    def copy(self, y):
+        check(lib().rb_vec_copy(self.h, y.h))
+
+    def axpy(self, x, alpha):
+        check(lib().rb_vec_axpy(self.h, x.h, float(alpha)))
+
+    def scale(self, alpha):
+        check(lib().rb_vec_scale(self.h, float(alpha)))
+
+    def inner_product(self, x):
+        out = C.c_double()
+        check(lib().rb_vec_dot(self.h, x.h, C.byref(out)))
+        return out.value
+
+    def norm(self, p=2):
+        if p != 2:
+            return float(np.linalg.norm(self.numpy(), p))
+        out = C.c_double()
+        check(lib().rb_vec_norm2(self.h, C.byref(out)))
+        return out.value
+
+    def device_ptr(self):
+        p = C.c_void_p()
+        check(lib().rb_vec_device_ptr(self.h, C.byref(p)))
+        return p.value
+
+
+class ParCSRMatrix:
+    """Device CSR matrix, FP64 values, int32 indices (core/par_matrix.hpp:481-611)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def from_arrays(cls, n_rows, n_cols, rowptr, cols, vals):
+        rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+        ci = np.ascontiguousarray(cols, dtype=np.int32)
+        cv = np.ascontiguousarray(vals, dtype=np.float64)
+        if ci.size == 0:
+            ci = np.zeros(1, np.int32)
+            cv = np.zeros(1, np.float64)
+        h = C.c_void_p()
+        check(lib().rb_csr_create(int(n_rows), int(n_cols), int(rp[-1]), _ptr(rp), _ptr(ci),
+                                  _ptr(cv), 0, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_scipy(cls, M):
+        M = M.tocsr()
+        return cls.from_arrays(M.shape[0], M.shape[1], M.indptr, M.indices, M.data)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().rb_csr_destroy(self.h)
+            except Exception:  # noqa: BLE001
+                pass
+            self.h = None
+
+    def info(self):
+        r, c, z = C.c_int(), C.c_int(), C.c_int64()
+        check(lib().rb_csr_info(self.h, C.byref(r), C.byref(c), C.byref(z)))
+        return r.value, c.value, z.value
+
+    @property
+    def global_num_rows(self):
+        return self.info()[0]
+
+    @property
+    def global_num_cols(self):
+        return self.info()[1]
+
+    @property
+    def local_nnz(self):
+        return self.info()[2]
+
+    def arrays(self):
+        n, m, z = self.info()
+        rp = np.zeros(n + 1, np.int32)
+        ci = np.zeros(max(z, 1), np.int32)
+        cv = np.zeros(max(z, 1), np.float64)
+        check(lib().rb_csr_download(self.h, _ptr(rp), _ptr(ci), _ptr(cv)))
+        return rp, ci[:z], cv[:z]
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        n, m, _ = self.info()
+        rp, ci, cv = self.arrays()
+        return sp.csr_matrix((cv, ci, rp), shape=(n, m))
+
+    # ParMatrix::mult / residual / mult_T / mult_append (par_matrix.hpp:243-250)
+    def mult(self, x, b):
+        check(lib().rb_spmv(self.h, x.h, b.h))
+
+    def residual(self, x, b, r):
+        check(lib().rb_residual(self.h, x.h, b.h, r.h))
+
+    def mult_T(self, x, b):
+        check(lib().rb_spmv_T(self.h, x.h, b.h))
+
+    def mult_append(self, x, b):
+        check(lib().rb_spmv_append(self.h, x.h, b.h))
+
+    def sort_diag_first(self):
+        check(lib().rb_csr_sort_diag_first(self.h))
+        return self
+
+    def transpose(self):
+        h = C.c_void_p()
+        check(lib().rb_csr_transpose(self.h, C.byref(h)))
+        return ParCSRMatrix(h)
+
+    def strength(self, strength_type=Classical, theta=0.0):
+        h = C.c_void_p()
+        check(lib().rb_strength(self.h, int(strength_type), float(theta), C.byref(h)))
+        return ParCSRMatrix(h)
+
+    def mult_matrix(self, B):
+        h = C.c_void_p()
+        check(lib().rb_spgemm(self.h, B.h, C.byref(h)))
+        return ParCSRMatrix(h)
+
+
+# gallery ---------------------------------------------------------------------
+def diffusion_stencil_2d(eps=1.0, theta=0.0):
+    out = np.zeros(9)
+    check(lib().rb_diffusion_stencil_2d(float(eps), float(theta), out))
+    return out
+
+
+def laplace_stencil_27pt():
+    out = np.zeros(27)
+    check(lib().rb_laplace_stencil_27pt(out))
+    return out
+
+
+def par_stencil_grid(stencil, grid, dim=None):
+    g = np.ascontiguousarray(grid, np.int32)
+    st = np.ascontiguousarray(stencil, np.float64)
+    h = C.c_void_p()
+    check(lib().rb_stencil_grid(st, g, int(dim or len(g)), C.byref(h)))
+    return ParCSRMatrix(h)
+
+
+def readParMatrix(path):
+    h = C.c_void_p()
+    check(lib().rb_read_petsc(str(path).encode(), C.byref(h)))
+    return ParCSRMatrix(h)
+
+
+# setup components ---------------------------------------------------------
+def split_pmis(S, weights=None):
+    n = S.global_num_rows
+    st = np.zeros(max(n, 1), np.int32)
+    w = None if weights is None else np.ascontiguousarray(weights[:n], np.float64)
+    check(lib().rb_split_pmis(S.h, _ptr(w) if w is not None else None, st))
+    return st[:n]
+
+
+def interpolation(A, S, states, interp_type=ModClassical, filter_threshold=0.0):
+    h = C.c_void_p()
+    st = np.ascontiguousarray(states, np.int32)
+    check(lib().rb_interpolation(A.h, S.h, st, int(interp_type), float(filter_threshold), C.byref(h)))
+    return ParCSRMatrix(h)
+
+
+def mod_classical_interpolation(A, S, states):
+    return interpolation(A, S, states, ModClassical)
+
+
+def extended_interpolation(A, S, states, filter_threshold=0.3):
+    return interpolation(A, S, states, Extended, filter_threshold)
+
+
+def rap(A, P, diag_first=True):
+    h = C.c_void_p()
+    check(lib().rb_rap(A.h, P.h, 1 if diag_first else 0, C.byref(h)))
+    return ParCSRMatrix(h)
+
+
+# multilevel ---------------------------------------------------------------
+class ParMultilevel:
+    """ParMultilevel (multilevel/par_multilevel.hpp:75-659) on the device."""
+
+    _FIELDS = ("strong_threshold", "relax_weight", "num_smooth_sweeps", "max_coarse",
+               "max_levels", "max_iterations", "solve_tol", "interp_filter")
+
+    def __init__(self, strong_threshold=0.0, strength_type=Classical, relax_type=SOR):
+        self.opts = AmgOpts()
+        lib().rb_amg_default_opts(C.byref(self.opts))
+        self.opts.strong_threshold = strong_threshold
+        self.opts.strength_type = strength_type
+        self.opts.relax_type = relax_type
+        self.h = None
+        self.weights = None
+        self.residuals = []
+        self.store_residuals = True
+
+    def __getattr__(self, name):
+        if name in ParMultilevel._FIELDS or name in ("precision", "jacobi_compat", "seed_offset",
+                                                     "relax_type", "strength_type", "interp_type"):
+            return getattr(self.__dict__["opts"], name)
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name in ParMultilevel._FIELDS or name in ("precision", "jacobi_compat", "seed_offset",
+                                                     "relax_type", "strength_type", "interp_type"):
+            setattr(self.opts, name, value)
+        else:
+            object.__setattr__(self, name, value)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().rb_amg_destroy(self.h)
+            except Exception:  # noqa: BLE001
+                pass
+            self.h = None
+
+    def setup(self, A):
+        if self.h:
+            lib().rb_amg_destroy(self.h)
+            self.h = None
+        h = C.c_void_p()
+        w = None
+        if self.weights is not None:
+            self._w = np.ascontiguousarray(self.weights, np.float64)
+            w = _ptr(self._w)
+        check(lib().rb_amg_setup(A.h, C.byref(self.opts), w, C.byref(h)))
+        self.h = h
+        self.A = A
+
+    @property
+    def num_levels(self):
+        n = C.c_int()
+        check(lib().rb_amg_num_levels(self.h, C.byref(n)))
+        return n.value
+
+    def level_info(self, l):
+        n, za, zp = C.c_int(), C.c_int64(), C.c_int64()
+        check(lib().rb_amg_level_info(self.h, l, C.byref(n), C.byref(za), C.byref(zp)))
+        return n.value, za.value, zp.value
+
+    def level_matrix(self, l, which="A"):
+        h = C.c_void_p()
+        check(lib().rb_amg_level_matrix(self.h, l, {"A": 0, "P": 1, "R": 2}[which], C.byref(h)))
+        return ParCSRMatrix(h)
+
+    def level_states(self, l):
+        n = self.level_info(l)[0]
+        st = np.zeros(max(n, 1), np.int32)
+        check(lib().rb_amg_level_states(self.h, l, st))
+        return st[:n]
+
+    def cycle(self, x, b, level=0):
+        check(lib().rb_amg_cycle(self.h, x.h, b.h))
+
+    def solve(self, x, b):
+        cap = self.opts.max_iterations + 1
+        hist = np.zeros(cap)
+        it = C.c_int()
+        rc = lib().rb_amg_solve(self.h, x.h, b.h, C.byref(it), _ptr(hist), cap)
+        self.residuals = list(hist[: it.value + 1])
+        if rc not in (0, -5):
+            check(rc)
+        return it.value
+
+    def get_residuals(self):
+        return self.residuals
+
+    def print_hierarchy(self):
+        print("Num Levels = %d" % self.num_levels)
+        print("A\tNRow\tNCol\tNNZ")
+        for l in range(self.num_levels):
+            n, za, _ = self.level_info(l)
+            print("%d\t%d\t%d\t%d" % (l, n, n, za))
+
+
+class ParRugeStubenSolver(ParMultilevel):
+    """ParRugeStubenSolver (ruge_stuben/par_ruge_stuben_solver.hpp:12-170)."""
+
+    def __init__(self, strong_threshold=0.0, coarsen_type=PMIS, interp_type=Direct,
+                 strength_type=Classical, relax_type=SOR):
+        super().__init__(strong_threshold, strength_type, relax_type)
+        if coarsen_type != PMIS:
+            raise RaptorError(-1, "only PMIS coarsening is built")
+        if interp_type not in (ModClassical, Extended):
+            raise RaptorError(-1, "interpolation must be ModClassical or Extended")
+        self.opts.interp_type = interp_type
+
+
+# Krylov -------------------------------------------------------------------
+def _hist_call(fn, cap):
+    hist = np.zeros(cap)
+    nh = C.c_int()
+    rc = fn(hist, nh)
+    return rc, list(hist[: min(nh.value, cap)])
+
+
+def PCG(A, ml, x, b, res, tol=1e-5, max_iter=-1, mode=PCG_REFERENCE):
+    """krylov/par_cg.cpp:121-263; appends the history to `res`."""
+    cap = max(max_iter, 0) + 2 if max_iter > 0 else (int(1.3 * A.global_num_rows) + 4)
+    cap = min(cap, 1 << 20)
+    rc, h = _hist_call(lambda hist, nh: lib().rb_pcg(A.h, ml.h, x.h, b.h, float(tol), int(max_iter),
+                                                     int(mode), _ptr(hist), cap, C.byref(nh)), cap)
+    res.extend(h)
+    if rc not in (0, -5):
+        check(rc)
+    return rc
+
+
+def CG(A, x, b, res, tol=1e-5, max_iter=-1):
+    cap = max(max_iter, 0) + 2 if max_iter > 0 else (int(1.3 * A.global_num_rows) + 4)
+    cap = min(cap, 1 << 20)
+    rc, h = _hist_call(lambda hist, nh: lib().rb_cg(A.h, x.h, b.h, float(tol), int(max_iter),
+                                                    _ptr(hist), cap, C.byref(nh)), cap)
+    res.extend(h)
+    if rc not in (0, -5):
+        check(rc)
+    return rc
+
+
+def BiCGStab(A, x, b, res, tol=1e-5, max_iter=-1):
+    cap = max(max_iter, 0) + 2 if max_iter > 0 else (int(1.3 * A.global_num_rows) + 4)
+    cap = min(cap, 1 << 20)
+    rc, h = _hist_call(lambda hist, nh: lib().rb_bicgstab(A.h, None, x.h, b.h, float(tol),
+                                                          int(max_iter), _ptr(hist), cap,
+                                                          C.byref(nh)), cap)
+    res.extend(h)
+    if rc not in (0, -5):
+        check(rc)
+    return rc
+
+
+def Pre_BiCGStab(A, x, b, ml, res, tol=1e-5, max_iter=-1):
+    cap = max(max_iter, 0) + 2 if max_iter > 0 else (int(1.3 * A.global_num_rows) + 4)
+    cap = min(cap, 1 << 20)
+    rc, h = _hist_call(lambda hist, nh: lib().rb_bicgstab(A.h, ml.h, x.h, b.h, float(tol),
+                                                          int(max_iter), _ptr(hist), cap,
+                                                          C.byref(nh)), cap)
+    res.extend(h)
+    if rc not in (0, -5):
+        check(rc)
+    return rc
+
+
+def init(device=0):
+    check(lib().rb_init(int(device)))
+
+
+def version():
+    return lib().rb_version().decode()

@@ -1,0 +1,636 @@
+// capi.cu -- the extern "C" boundary (include/raptor_b200.h).
+//
+// Every entry point catches library errors and CUDA failures and turns them
+// into an rb_status plus a per-thread message; nothing throws across the C
+// boundary.  There is no host fallback: without a device every compute call
+// fails with RB_ERR_NO_DEVICE.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "blas1.cuh"
+#include "hierarchy.cuh"
+#include "rb_internal.cuh"
+
+namespace rb {
+const char* last_error_cstr();
+ReduceSlot global_reduce_slot(int grid);
+}  // namespace rb
+
+using namespace rb;
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        set_last_error("");
+        return f();
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return RB_ERR_OOM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return RB_ERR_INVALID;
+    }
+}
+
+bool g_init = false;
+
+void ensure_device() {
+    if (g_init) return;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) throw Error(RB_ERR_NO_DEVICE, "no CUDA device available");
+    RB_CUDA(cudaSetDevice(0));
+    (void)stream();
+    g_init = true;
+}
+
+#define NEED(p) RB_REQUIRE((p) != nullptr, #p " is NULL")
+
+}  // namespace
+
+extern "C" {
+
+const char* rb_last_error(void) { return last_error_cstr(); }
+
+const char* rb_version(void) { return "raptor_b200 1.0 (sm_100a)"; }
+
+int rb_init(int device) {
+    return guarded([&]() -> int {
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0) throw Error(RB_ERR_NO_DEVICE, "no CUDA device available");
+        RB_REQUIRE(device >= 0 && device < n, "device index out of range");
+        RB_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        RB_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major != 10)
+            throw Error(RB_ERR_NO_DEVICE, "libraptor_b200 holds sm_100a kernels only; device is sm_" +
+                                              std::to_string(prop.major) + std::to_string(prop.minor));
+        (void)stream();
+        g_init = true;
+        return RB_OK;
+    });
+}
+
+int rb_set_stream(void* s) {
+    return guarded([&]() -> int {
+        ensure_device();
+        set_stream((cudaStream_t)s);
+        return RB_OK;
+    });
+}
+
+int rb_synchronize(void) {
+    return guarded([&]() -> int {
+        ensure_device();
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+// ------------------------------------------------------------ containers --
+int rb_csr_create(int n_rows, int n_cols, int64_t nnz, const int* rowptr, const int* cols,
+                  const double* vals, int on_device, rb_csr* out) {
+    return guarded([&]() -> int {
+        ensure_device();
+        NEED(out); NEED(rowptr);
+        RB_REQUIRE(nnz == 0 || (cols && vals), "cols/vals are NULL");
+        std::unique_ptr<rb_csr_s> A(new_csr(n_rows, n_cols, nnz));
+        auto kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if (!on_device) {
+            RB_REQUIRE(rowptr[0] == 0 && rowptr[n_rows] == nnz, "rowptr does not span nnz");
+            for (int i = 0; i < n_rows; i++)
+                RB_REQUIRE(rowptr[i] <= rowptr[i + 1], "rowptr is not monotone");
+            for (int64_t j = 0; j < nnz; j++)
+                RB_REQUIRE(cols[j] >= 0 && cols[j] < n_cols, "column index out of range");
+        }
+        RB_CUDA(cudaMemcpyAsync(A->rowptr.get(), rowptr, sizeof(int) * ((size_t)n_rows + 1), kind, stream()));
+        if (nnz) {
+            RB_CUDA(cudaMemcpyAsync(A->cols.get(), cols, sizeof(int) * nnz, kind, stream()));
+            RB_CUDA(cudaMemcpyAsync(A->vals.get(), vals, sizeof(double) * nnz, kind, stream()));
+        }
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        *out = A.release();
+        return RB_OK;
+    });
+}
+
+int rb_csr_destroy(rb_csr A) {
+    return guarded([&]() -> int {
+        delete A;
+        return RB_OK;
+    });
+}
+
+int rb_csr_info(rb_csr A, int* n_rows, int* n_cols, int64_t* nnz) {
+    return guarded([&]() -> int {
+        NEED(A);
+        if (n_rows) *n_rows = A->n_rows;
+        if (n_cols) *n_cols = A->n_cols;
+        if (nnz) *nnz = A->nnz;
+        return RB_OK;
+    });
+}
+
+int rb_csr_download(rb_csr A, int* rowptr, int* cols, double* vals) {
+    return guarded([&]() -> int {
+        NEED(A);
+        if (rowptr) A->rowptr.download(rowptr, (size_t)A->n_rows + 1);
+        if (cols) A->cols.download(cols, (size_t)A->nnz);
+        if (vals) A->vals.download(vals, (size_t)A->nnz);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_csr_device_arrays(rb_csr A, int** rowptr, int** cols, double** vals) {
+    return guarded([&]() -> int {
+        NEED(A);
+        if (rowptr) *rowptr = A->rowptr.get();
+        if (cols) *cols = A->cols.get();
+        if (vals) *vals = A->vals.get();
+        return RB_OK;
+    });
+}
+
+int rb_csr_sort_diag_first(rb_csr A) {
+    return guarded([&]() -> int {
+        NEED(A);
+        sort_rows_diag_first(*A, true);
+        RB_CHECK_LAUNCH();
+        return RB_OK;
+    });
+}
+
+int rb_csr_transpose(rb_csr A, rb_csr* out) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(out);
+        *out = transpose(*A);
+        return RB_OK;
+    });
+}
+
+// --------------------------------------------------------------- vectors --
+int rb_vec_create(int n, rb_vec* out) {
+    return guarded([&]() -> int {
+        ensure_device();
+        NEED(out);
+        RB_REQUIRE(n >= 0, "negative vector size");
+        auto* v = new rb_vec_s();
+        v->n = n;
+        v->v.alloc((size_t)n + 1);
+        v->v.zero();
+        *out = v;
+        return RB_OK;
+    });
+}
+
+int rb_vec_destroy(rb_vec v) {
+    return guarded([&]() -> int {
+        delete v;
+        return RB_OK;
+    });
+}
+
+int rb_vec_size(rb_vec v, int* n) {
+    return guarded([&]() -> int {
+        NEED(v); NEED(n);
+        *n = v->n;
+        return RB_OK;
+    });
+}
+
+int rb_vec_upload(rb_vec v, const double* host) {
+    return guarded([&]() -> int {
+        NEED(v); NEED(host);
+        v->v.upload(host, v->n);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_vec_download(rb_vec v, double* host) {
+    return guarded([&]() -> int {
+        NEED(v); NEED(host);
+        v->v.download(host, v->n);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_vec_set(rb_vec v, double value) {
+    return guarded([&]() -> int {
+        NEED(v);
+        if (v->n) k_fill<double><<<grid_for(v->n, 256), 256, 0, stream()>>>(v->n, v->v.get(), value);
+        RB_CHECK_LAUNCH();
+        return RB_OK;
+    });
+}
+
+int rb_vec_device_ptr(rb_vec v, double** ptr) {
+    return guarded([&]() -> int {
+        NEED(v); NEED(ptr);
+        *ptr = v->v.get();
+        return RB_OK;
+    });
+}
+
+int rb_vec_copy(rb_vec dst, rb_vec src) {
+    return guarded([&]() -> int {
+        NEED(dst); NEED(src);
+        RB_REQUIRE(dst->n == src->n, "vector sizes differ");
+        RB_CUDA(cudaMemcpyAsync(dst->v.get(), src->v.get(), sizeof(double) * dst->n,
+                                cudaMemcpyDeviceToDevice, stream()));
+        return RB_OK;
+    });
+}
+
+int rb_vec_axpy(rb_vec y, rb_vec x, double a) {
+    return guarded([&]() -> int {
+        NEED(y); NEED(x);
+        RB_REQUIRE(y->n == x->n, "vector sizes differ");
+        if (y->n) k_axpy<double><<<grid_for(y->n, 256), 256, 0, stream()>>>(y->n, y->v.get(), x->v.get(), a);
+        RB_CHECK_LAUNCH();
+        return RB_OK;
+    });
+}
+
+int rb_vec_scale(rb_vec y, double a) {
+    return guarded([&]() -> int {
+        NEED(y);
+        if (y->n) k_scale<double><<<grid_for(y->n, 256), 256, 0, stream()>>>(y->n, y->v.get(), a);
+        RB_CHECK_LAUNCH();
+        return RB_OK;
+    });
+}
+
+int rb_vec_dot(rb_vec a, rb_vec b, double* out) {
+    return guarded([&]() -> int {
+        NEED(a); NEED(b); NEED(out);
+        RB_REQUIRE(a->n == b->n, "Cannot perform inner product: dimensions do not match");
+        DevArray<double> r(1);
+        dot_async(a->v.get(), b->v.get(), a->n, r.get());
+        *out = read_scalar(r.get());
+        return RB_OK;
+    });
+}
+
+int rb_vec_norm2(rb_vec a, double* out) {
+    return guarded([&]() -> int {
+        NEED(a); NEED(out);
+        DevArray<double> r(1);
+        dot_async(a->v.get(), a->v.get(), a->n, r.get());
+        *out = std::sqrt(read_scalar(r.get()));
+        return RB_OK;
+    });
+}
+
+// ----------------------------------------------------------- SpMV family --
+int rb_spmv(rb_csr A, rb_vec x, rb_vec b) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows, "spmv: sizes do not match");
+        spmv64(view(*A), x->v.get(), b->v.get());
+        return RB_OK;
+    });
+}
+
+int rb_residual(rb_csr A, rb_vec x, rb_vec b, rb_vec r) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b); NEED(r);
+        RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows && r->n == A->n_rows,
+                   "residual: sizes do not match");
+        residual64(view(*A), x->v.get(), b->v.get(), r->v.get());
+        return RB_OK;
+    });
+}
+
+int rb_spmv_T(rb_csr A, rb_vec x, rb_vec b) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_rows && b->n == A->n_cols, "spmv_T: sizes do not match");
+        // the transpose is a gather over A^T: deterministic, no atomics
+        std::unique_ptr<rb_csr_s> T(transpose(*A));
+        spmv64(view(*T), x->v.get(), b->v.get());
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_spmv_append(rb_csr A, rb_vec x, rb_vec b) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows, "spmv_append: sizes do not match");
+        spmv_append64(view(*A), x->v.get(), b->v.get());
+        return RB_OK;
+    });
+}
+
+// --------------------------------------------------------------- gallery --
+int rb_diffusion_stencil_2d(double eps, double theta, double* st) {
+    return guarded([&]() -> int {
+        NEED(st);
+        // gallery/diffusion.hpp:58-85, same expression order
+        double C = std::cos(theta), S = std::sin(theta);
+        double CS = C * S, CC = C * C, SS = S * S;
+        volatile double v1 = ((-1 * eps - 1) * CC + (-1 * eps - 1) * SS + (3 * eps - 3) * CS) / 6.0;
+        volatile double v2 = ((2 * eps - 4) * CC + (-4 * eps + 2) * SS) / 6.0;
+        volatile double v3 = ((-1 * eps - 1) * CC + (-1 * eps - 1) * SS + (-3 * eps + 3) * CS) / 6.0;
+        volatile double v4 = ((-4 * eps + 2) * CC + (2 * eps - 4) * SS) / 6.0;
+        volatile double v5 = ((8 * eps + 8) * CC + (8 * eps + 8) * SS) / 6.0;
+        double vals[9] = {v1, v2, v3, v4, v5, v4, v3, v2, v1};
+        memcpy(st, vals, sizeof(vals));
+        return RB_OK;
+    });
+}
+
+int rb_laplace_stencil_27pt(double* st) {
+    return guarded([&]() -> int {
+        NEED(st);
+        for (int i = 0; i < 27; i++) st[i] = -1;
+        st[13] = 26;
+        return RB_OK;
+    });
+}
+
+int rb_stencil_grid_impl(const double* stencil, const int* grid, int dim, rb_csr* out);
+
+int rb_stencil_grid(const double* stencil, const int* grid, int dim, rb_csr* out) {
+    return guarded([&]() -> int {
+        ensure_device();
+        NEED(stencil); NEED(grid); NEED(out);
+        return rb_stencil_grid_impl(stencil, grid, dim, out);
+    });
+}
+
+int rb_read_petsc(const char* path, rb_csr* out) {
+    return guarded([&]() -> int {
+        ensure_device();
+        NEED(path); NEED(out);
+        FILE* f = fopen(path, "rb");
+        RB_REQUIRE(f != nullptr, std::string("cannot open ") + path);
+        std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
+        auto be32 = [&](int* dst, size_t n) {
+            std::vector<unsigned char> buf(4 * n);
+            RB_REQUIRE(fread(buf.data(), 1, buf.size(), f) == buf.size(), "truncated PETSc file");
+            for (size_t i = 0; i < n; i++)
+                dst[i] = (int)((unsigned)buf[4 * i] << 24 | (unsigned)buf[4 * i + 1] << 16 |
+                               (unsigned)buf[4 * i + 2] << 8 | (unsigned)buf[4 * i + 3]);
+        };
+        int hdr[4];
+        be32(hdr, 4);
+        RB_REQUIRE(hdr[0] == 1211216, "not a PETSc binary AIJ matrix");
+        const int m = hdr[1], n = hdr[2], nnz = hdr[3];
+        std::vector<int> lens(m), rp(m + 1, 0), ci(nnz);
+        be32(lens.data(), m);
+        be32(ci.data(), nnz);
+        for (int i = 0; i < m; i++) rp[i + 1] = rp[i] + lens[i];
+        std::vector<double> cv(nnz);
+        std::vector<unsigned char> buf(8 * (size_t)nnz);
+        RB_REQUIRE(fread(buf.data(), 1, buf.size(), f) == buf.size(), "truncated PETSc file");
+        for (int j = 0; j < nnz; j++) {
+            uint64_t u = 0;
+            for (int k = 0; k < 8; k++) u = (u << 8) | buf[8 * (size_t)j + k];
+            memcpy(&cv[j], &u, 8);
+        }
+        int rc = rb_csr_create(m, n, nnz, rp.data(), ci.data(), cv.data(), 0, out);
+        if (rc != RB_OK) return rc;
+        sort_rows_diag_first(**out, false);   // finalize() sorts rows
+        return RB_OK;
+    });
+}
+
+// ------------------------------------------------------ setup components --
+int rb_strength(rb_csr A, int kind, double theta, rb_csr* S) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(S);
+        RB_REQUIRE(kind == RB_STRENGTH_CLASSICAL || kind == RB_STRENGTH_SYMMETRIC, "unknown strength kind");
+        *S = strength(*A, kind, theta);
+        return RB_OK;
+    });
+}
+
+int rb_split_pmis(rb_csr S, const double* weights, int* states) {
+    return guarded([&]() -> int {
+        NEED(S); NEED(states);
+        const int n = S->n_rows;
+        std::vector<double> w = weights ? std::vector<double>(weights, weights + n) : rand_weights(n, 0);
+        DevArray<double> wd((size_t)std::max(n, 1));
+        wd.upload(w.data(), n);
+        DevArray<int> st((size_t)std::max(n, 1));
+        split_pmis(*S, wd.get(), st.get());
+        st.download(states, n);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_interpolation(rb_csr A, rb_csr S, const int* states, int kind, double filter, rb_csr* P) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(S); NEED(states); NEED(P);
+        RB_REQUIRE(kind == RB_INTERP_MODCLASSICAL || kind == RB_INTERP_EXTENDED, "unknown interpolation kind");
+        DevArray<int> st((size_t)std::max(A->n_rows, 1));
+        st.upload(states, A->n_rows);
+        *P = interpolation(*A, *S, st.get(), kind, filter);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_spgemm(rb_csr A, rb_csr B, rb_csr* C) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(B); NEED(C);
+        *C = spgemm(*A, *B);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_rap(rb_csr A, rb_csr P, int diag_first, rb_csr* Ac) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(P); NEED(Ac);
+        *Ac = rap(*A, *P, nullptr, diag_first != 0);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+// ------------------------------------------------------------- hierarchy --
+void rb_amg_default_opts(rb_amg_opts* o) {
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->solver = RB_SOLVER_RS;
+    o->strength_type = RB_STRENGTH_CLASSICAL;
+    o->interp_type = RB_INTERP_MODCLASSICAL;
+    o->relax_type = RB_RELAX_JACOBI;
+    o->num_smooth_sweeps = 1;
+    o->max_coarse = 50;
+    o->max_levels = 25;
+    o->max_iterations = 100;
+    o->strong_threshold = 0.25;
+    o->relax_weight = 1.0;
+    o->solve_tol = 1e-7;
+    o->interp_filter = 0.3;
+    o->prolong_weight = 4.0 / 3.0;
+    o->prolong_smooth_steps = 1;
+    o->precision = RB_PREC_FP64;
+    o->jacobi_compat = 0;
+    o->seed_offset = 0;
+}
+
+int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_amg* out) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(out);
+        RB_REQUIRE(A->n_rows == A->n_cols, "AMG needs a square matrix");
+        rb_amg_opts o;
+        if (opts) o = *opts;
+        else rb_amg_default_opts(&o);
+        RB_REQUIRE(o.solver == RB_SOLVER_RS, "only the Ruge-Stuben solver is built in this library");
+        RB_REQUIRE(o.num_smooth_sweeps >= 0, "num_smooth_sweeps < 0");
+        std::unique_ptr<rb_amg_s> ml(new rb_amg_s());
+        ml->h.setup(*A, o, weights);
+        *out = ml.release();
+        return RB_OK;
+    });
+}
+
+int rb_amg_destroy(rb_amg ml) {
+    return guarded([&]() -> int {
+        delete ml;
+        return RB_OK;
+    });
+}
+
+int rb_amg_num_levels(rb_amg ml, int* num_levels) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(num_levels);
+        *num_levels = ml->h.num_levels();
+        return RB_OK;
+    });
+}
+
+int rb_amg_level_info(rb_amg ml, int level, int* n_rows, int64_t* nnz_A, int64_t* nnz_P) {
+    return guarded([&]() -> int {
+        NEED(ml);
+        RB_REQUIRE(level >= 0 && level < ml->h.num_levels(), "level out of range");
+        const MasterLevel& M = ml->h.master[level];
+        if (n_rows) *n_rows = M.A->n_rows;
+        if (nnz_A) *nnz_A = M.A->nnz;
+        if (nnz_P) *nnz_P = M.P ? M.P->nnz : 0;
+        return RB_OK;
+    });
+}
+
+static rb_csr_s* clone_csr(const rb_csr_s& M) {
+    rb_csr_s* C = new_csr(M.n_rows, M.n_cols, M.nnz);
+    RB_CUDA(cudaMemcpyAsync(C->rowptr.get(), M.rowptr.get(), sizeof(int) * ((size_t)M.n_rows + 1),
+                            cudaMemcpyDeviceToDevice, stream()));
+    if (M.nnz) {
+        RB_CUDA(cudaMemcpyAsync(C->cols.get(), M.cols.get(), sizeof(int) * M.nnz,
+                                cudaMemcpyDeviceToDevice, stream()));
+        RB_CUDA(cudaMemcpyAsync(C->vals.get(), M.vals.get(), sizeof(double) * M.nnz,
+                                cudaMemcpyDeviceToDevice, stream()));
+    }
+    return C;
+}
+
+int rb_amg_level_matrix(rb_amg ml, int level, int which, rb_csr* out) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(out);
+        RB_REQUIRE(level >= 0 && level < ml->h.num_levels(), "level out of range");
+        const MasterLevel& M = ml->h.master[level];
+        const rb_csr_s* src = which == 0 ? M.A.get() : which == 1 ? M.P.get() : M.R.get();
+        RB_REQUIRE(src != nullptr, "the coarsest level has no P/R");
+        *out = clone_csr(*src);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_amg_level_states(rb_amg ml, int level, int* states) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(states);
+        RB_REQUIRE(level >= 0 && level < ml->h.num_levels() - 1, "level has no splitting");
+        const MasterLevel& M = ml->h.master[level];
+        M.states.download(states, M.A->n_rows);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_amg_cycle(rb_amg ml, rb_vec x, rb_vec b) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(x); NEED(b);
+        const int n = ml->h.master[0].A->n_rows;
+        RB_REQUIRE(x->n == n && b->n == n, "cycle: vector sizes do not match");
+        ml->h.cycle(x->v.get(), b->v.get(), false);
+        return RB_OK;
+    });
+}
+
+int rb_amg_solve(rb_amg ml, rb_vec x, rb_vec b, int* iters, double* hist, int cap) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(x); NEED(b);
+        const int n = ml->h.master[0].A->n_rows;
+        RB_REQUIRE(x->n == n && b->n == n, "solve: vector sizes do not match");
+        int it = 0;
+        std::vector<double> h(std::max(cap, 1));
+        int rc = ml->h.solve(x->v.get(), b->v.get(), hist ? hist : h.data(), hist ? cap : 0, &it);
+        if (iters) *iters = it;
+        return rc;
+    });
+}
+
+// ---------------------------------------------------------------- Krylov --
+int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, int mode,
+           double* hist, int cap, int* n_hist) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(ml); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows, "PCG: sizes do not match");
+        RB_REQUIRE(mode == RB_PCG_REFERENCE || mode == RB_PCG_TRUE_RESIDUAL, "unknown PCG mode");
+        int nh = 0;
+        std::vector<double> h(1);
+        int rc = ml->h.pcg(*A, x->v.get(), b->v.get(), tol, max_iter, mode, hist ? hist : h.data(),
+                           hist ? cap : 0, &nh);
+        if (n_hist) *n_hist = nh;
+        return rc;
+    });
+}
+
+int rb_cg(rb_csr A, rb_vec x, rb_vec b, double tol, int max_iter, double* hist, int cap,
+          int* n_hist) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows, "CG: sizes do not match");
+        int nh = 0;
+        std::vector<double> h(1);
+        int rc = krylov_cg(*A, x->v.get(), b->v.get(), tol, max_iter, hist ? hist : h.data(),
+                           hist ? cap : 0, &nh);
+        if (n_hist) *n_hist = nh;
+        return rc;
+    });
+}
+
+int rb_bicgstab(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, double* hist,
+                int cap, int* n_hist) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows, "BiCGStab: sizes do not match");
+        int nh = 0;
+        std::vector<double> h(1);
+        int rc = krylov_bicgstab(*A, ml ? &ml->h : nullptr, x->v.get(), b->v.get(), tol, max_iter,
+                                 hist ? hist : h.data(), hist ? cap : 0, &nh);
+        if (n_hist) *n_hist = nh;
+        return rc;
+    });
+}
+
+}  // extern "C"

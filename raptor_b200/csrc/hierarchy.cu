@@ -1,0 +1,821 @@
+// hierarchy.cu -- ParMultilevel on the device: setup, V-cycle, stationary
+// solve, and the Krylov methods that use it (PCG, CG, BiCGStab).
+//
+// Setup runs the Ruge-Stuben chain of extend_hierarchy on the GPU
+// (strength -> PMIS -> interpolation -> R = P^T -> A_c = R (A P)) in FP64,
+// then derives the cycle data: per-level value copies in the cycle precision
+// (FP32 halves the bytes of this bandwidth-bound path), inverse diagonals or
+// l1 row norms, a multicolour row ordering for the Gauss-Seidel stand-in, the
+// row-kernel width chosen by timing, and the LU of A_c^T.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <map>
+#include <memory>
+
+#include "blas1.cuh"
+#include "hierarchy.cuh"
+
+namespace rb {
+
+// ---------------------------------------------------------------- kernels --
+template <typename T>
+__global__ void k_diag_inv(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const double* __restrict__ cv, double omega, int l1, T* dinv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = rp[i], e = rp[i + 1];
+    double d = 0.0;
+    if (l1) {
+        for (int j = s; j < e; j++) d += fabs(cv[j]);
+    } else if (s < e && ci[s] == i) {
+        d = cv[s];
+    }
+    dinv[i] = (T)(fabs(d) > 1e-16 ? omega / d : 0.0);
+}
+
+template <typename T>
+__global__ void k_to_prec(long n, const double* __restrict__ in, T* __restrict__ out) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (T)in[i];
+}
+
+// One colour of a multicolour Gauss-Seidel sweep: rows of one colour are not
+// coupled, so each row applies SOR_forward's update (par_relax.cpp:66) or
+// SOR_backward's (:102) independently.  Rows lacking a leading diagonal are
+// skipped as the reference does.
+template <int G, typename T>
+__global__ void __launch_bounds__(kRowBlock)
+k_mc_sweep(int nrows, const int* __restrict__ rows, const int* __restrict__ rp,
+           const int* __restrict__ ci, const T* __restrict__ cv, T* x, const T* __restrict__ b,
+           double omega, int backward) {
+    using Acc = typename AccOf<T>::type;
+    constexpr int RPW = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / G, gl = lane & (G - 1);
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long base = gwarp * RPW; base < nrows; base += nwarps * RPW) {
+        const long t = base + sub;
+        const bool valid = t < nrows;
+        int i = 0, s = 0, e = 0;
+        if (valid) { i = rows[t]; s = rp[i]; e = rp[i + 1]; }
+        const bool has_diag = valid && s < e && ci[s] == i;
+        Acc sum = 0;
+        if (has_diag)
+            for (int j = s + 1 + gl; j < e; j += G) sum += (Acc)cv[j] * (Acc)x[ci[j]];
+        sum = group_sum<G>(sum);
+        if (has_diag && gl == 0) {
+            const Acc d = (Acc)cv[s], xi = (Acc)x[i], bi = (Acc)b[i], w = (Acc)omega;
+            if (backward) x[i] = (T)((Acc(1) - w) * xi + w * ((bi - sum) / d));
+            else x[i] = (T)((xi + w * (bi - xi - sum)) / d);
+        }
+    }
+}
+
+// --------------------------------------------------------------- helpers --
+template <typename T>
+static void launch_vec(void (*k)(long, T*, T), long n, T* x, T v) {
+    if (n > 0) k<<<grid_for(n, 256), 256, 0, stream()>>>(n, x, v);
+    RB_CHECK_LAUNCH();
+}
+
+template <typename T>
+void Level<T>::alloc_vectors() {
+    x.alloc((size_t)n + 1);
+    b.alloc((size_t)n + 1);
+    r.alloc((size_t)n + 1);
+    xt.alloc((size_t)n + 1);
+}
+
+// Time the row kernel for each group width and keep the fastest.
+template <typename T>
+static int autotune_group(const CsrView<T>& M, T* xin, T* yout) {
+    if (M.n_rows < 4096) return pick_group(M.n_rows, M.nnz);
+    static const int cands[4] = {4, 8, 16, 32};
+    cudaEvent_t e0, e1;
+    RB_CUDA(cudaEventCreate(&e0));
+    RB_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bestG = pick_group(M.n_rows, M.nnz);
+    for (int G : cands) {
+        launch_rows(M.rowptr, M.cols, M.vals, M.n_rows, M.nnz, xin, EpiStore<T>{yout}, G);
+        RB_CUDA(cudaEventRecord(e0, stream()));
+        for (int rep = 0; rep < 3; rep++)
+            launch_rows(M.rowptr, M.cols, M.vals, M.n_rows, M.nnz, xin, EpiStore<T>{yout}, G);
+        RB_CUDA(cudaEventRecord(e1, stream()));
+        RB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        RB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) { best = ms; bestG = G; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return bestG;
+}
+
+template <typename T>
+static CsrView<T> make_view(const rb_csr_s& M, DevArray<T>& vals) {
+    CsrView<T> v;
+    v.n_rows = M.n_rows;
+    v.n_cols = M.n_cols;
+    v.nnz = M.nnz;
+    v.rowptr = M.rowptr.get();
+    v.cols = M.cols.get();
+    if constexpr (std::is_same<T, double>::value) {
+        v.vals = M.vals.get();
+    } else {
+        vals.alloc((size_t)std::max<long long>(M.nnz, 1));
+        if (M.nnz)
+            k_to_prec<T><<<grid_for(M.nnz, 256), 256, 0, stream()>>>(M.nnz, M.vals.get(), vals.get());
+        RB_CHECK_LAUNCH();
+        v.vals = vals.get();
+    }
+    return v;
+}
+
+// ------------------------------------------------------------------ setup --
+void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* weights_host) {
+    opts = o;
+    auto t0 = std::chrono::steady_clock::now();
+    // levels[0]->A = Af->copy(); sort(); move_diag()   (par_multilevel.hpp:141-143)
+    rb_csr_s* A0 = new_csr(Af.n_rows, Af.n_cols, Af.nnz);
+    RB_CUDA(cudaMemcpyAsync(A0->rowptr.get(), Af.rowptr.get(), sizeof(int) * (Af.n_rows + 1),
+                            cudaMemcpyDeviceToDevice, stream()));
+    if (Af.nnz) {
+        RB_CUDA(cudaMemcpyAsync(A0->cols.get(), Af.cols.get(), sizeof(int) * Af.nnz,
+                                cudaMemcpyDeviceToDevice, stream()));
+        RB_CUDA(cudaMemcpyAsync(A0->vals.get(), Af.vals.get(), sizeof(double) * Af.nnz,
+                                cudaMemcpyDeviceToDevice, stream()));
+    }
+    sort_rows_diag_first(*A0, true);
+    master.clear();
+    master.emplace_back();
+    master[0].A.reset(A0);
+
+    // form_rand_weights (par_multilevel.hpp:165-168, 215-225)
+    std::vector<double> w;
+    if (weights_host) w.assign(weights_host, weights_host + Af.n_rows);
+    else w = rand_weights(Af.n_rows, o.seed_offset);
+    DevArray<double> wdev((size_t)std::max(Af.n_rows, 1));
+    wdev.upload(w.data(), w.size());
+
+    while (master.back().A->n_rows > o.max_coarse &&
+           (o.max_levels == -1 || (int)master.size() < o.max_levels)) {
+        MasterLevel& L = master.back();
+        const rb_csr_s& A = *L.A;
+        std::unique_ptr<rb_csr_s> S(strength(A, o.strength_type, o.strong_threshold));
+        L.states.alloc((size_t)std::max(A.n_rows, 1));
+        split_pmis(*S, wdev.get(), L.states.get());
+        L.P.reset(interpolation(A, *S, L.states.get(), o.interp_type, o.interp_filter));
+        S.reset();
+        L.R.reset(transpose(*L.P));
+        rb_csr_s* Ac = rap(A, *L.P, L.R.get(), true);
+        if (Ac->n_rows == 0 || Ac->n_rows == A.n_rows) {
+            // no coarsening possible: keep this level as the coarsest
+            delete Ac;
+            L.P.reset();
+            L.R.reset();
+            break;
+        }
+        master.emplace_back();
+        master.back().A.reset(Ac);
+    }
+    RB_CUDA(cudaStreamSynchronize(stream()));
+    setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    build_cycle_data();
+}
+
+template <typename T>
+void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
+    const int L = (int)master.size();
+    lv.clear();
+    lv.resize(L);
+    const bool l1 = opts.relax_type == RB_RELAX_L1JACOBI;
+    const bool mc = opts.relax_type == RB_RELAX_SOR || opts.relax_type == RB_RELAX_SSOR;
+    for (int l = 0; l < L; l++) {
+        Level<T>& V = lv[l];
+        const MasterLevel& M = master[l];
+        V.n = M.A->n_rows;
+        V.A = make_view<T>(*M.A, V.Avals);
+        if (l < L - 1) {
+            V.P = make_view<T>(*M.P, V.Pvals);
+            V.R = make_view<T>(*M.R, V.Rvals);
+            V.dinv.alloc((size_t)std::max(V.n, 1));
+            if (V.n)
+                k_diag_inv<T><<<grid_for(V.n, 256), 256, 0, stream()>>>(
+                    V.n, M.A->rowptr.get(), M.A->cols.get(), M.A->vals.get(), opts.relax_weight,
+                    l1 ? 1 : 0, V.dinv.get());
+            RB_CHECK_LAUNCH();
+            if (mc) {
+                DevArray<int> colour((size_t)std::max(V.n, 1));
+                const int nc = colour_rows(*M.A, colour.get());
+                std::vector<int> hc(V.n);
+                colour.download(hc.data(), V.n);
+                RB_CUDA(cudaStreamSynchronize(stream()));
+                V.colour_ptr.assign(nc + 1, 0);
+                for (int i = 0; i < V.n; i++) V.colour_ptr[hc[i] + 1]++;
+                for (int c = 0; c < nc; c++) V.colour_ptr[c + 1] += V.colour_ptr[c];
+                std::vector<int> fillp(V.colour_ptr.begin(), V.colour_ptr.end() - 1), rows(V.n);
+                for (int i = 0; i < V.n; i++) rows[fillp[hc[i]]++] = i;
+                V.colour_rows.alloc((size_t)std::max(V.n, 1));
+                V.colour_rows.upload(rows.data(), V.n);
+            }
+        }
+        V.alloc_vectors();
+    }
+    // autotune the row-kernel width of every operator of the cycle
+    for (int l = 0; l < L; l++) {
+        Level<T>& V = lv[l];
+        V.gA = autotune_group(V.A, V.x.get(), V.r.get());
+        if (l < L - 1) {
+            V.gP = autotune_group(V.P, lv[l + 1].x.get(), V.xt.get());
+            V.gR = autotune_group(V.R, V.r.get(), lv[l + 1].b.get());
+        }
+    }
+    RB_CUDA(cudaStreamSynchronize(stream()));
+}
+
+void Hierarchy::build_cycle_data() {
+    const int L = (int)master.size();
+    // coarse LU of A_c^T (duplicate_coarse, par_multilevel.hpp:229-339)
+    const rb_csr_s& Ac = *master[L - 1].A;
+    coarse_n = Ac.n_rows;
+    RB_REQUIRE(coarse_n <= 6000, "coarsest level too large for the dense solve");
+    lu.alloc((size_t)std::max(coarse_n * coarse_n, 1));
+    piv.alloc((size_t)std::max(coarse_n, 1));
+    lu.zero();
+    DevArray<int> info(1);
+    info.zero();
+    if (coarse_n) {
+        k_dense_from_csr<<<grid_for(coarse_n, 128), 128, 0, stream()>>>(
+            coarse_n, Ac.rowptr.get(), Ac.cols.get(), Ac.vals.get(), lu.get());
+        RB_CHECK_LAUNCH();
+        k_lu_factor<<<1, 256, 0, stream()>>>(coarse_n, lu.get(), piv.get(), info.get());
+        RB_CHECK_LAUNCH();
+    }
+    if (opts.precision == RB_PREC_FP32) build_levels(lv32);
+    else build_levels(lv64);
+    // Krylov work vectors (FP64, finest size)
+    const int n = master[0].A->n_rows;
+    kr.alloc((size_t)n + 1);
+    kz.alloc((size_t)n + 1);
+    kp.alloc((size_t)n + 1);
+    kAp.alloc((size_t)n + 1);
+    ks.alloc((size_t)n + 1);
+    kAs.alloc((size_t)n + 1);
+    krs.alloc((size_t)n + 1);
+    kph.alloc((size_t)n + 1);
+    ksh.alloc((size_t)n + 1);
+    scal.alloc(1);
+    scal.zero();
+    RB_CUDA(cudaMallocHost(&host_scal, sizeof(KScal)));
+    gA0 = autotune_group(view(*master[0].A), kp.get(), kAp.get());
+}
+
+Hierarchy::~Hierarchy() {
+    release_graphs();
+    if (host_scal) cudaFreeHost(host_scal);
+}
+
+void Hierarchy::release_graphs() {
+    for (auto& kv : graphs) {
+        if (kv.second) cudaGraphExecDestroy(kv.second);
+    }
+    graphs.clear();
+}
+
+size_t Hierarchy::device_bytes() const {
+    size_t b = 0;
+    for (const auto& M : master) {
+        b += M.A->nnz * 12 + (M.A->n_rows + 1) * 4;
+        if (M.P) b += M.P->nnz * 12 * 2 + (M.P->n_rows + M.P->n_cols + 2) * 4;
+    }
+    return b;
+}
+
+// ------------------------------------------------------------------ cycle --
+// ParMultilevel::cycle (par_multilevel.hpp:341-457).  x_zero says the
+// caller's x is zero (the preconditioner's z = 0 and every coarse x_{l+1} = 0),
+// which turns the first Jacobi sweep into x = w D^-1 b.
+template <typename T>
+void Hierarchy::smooth(Level<T>& V, T*& cur, T*& other, const T* b, bool x_zero) {
+    const int sweeps = opts.num_smooth_sweeps;
+    const int rt = opts.relax_type;
+    const bool jacobi_type = (rt == RB_RELAX_JACOBI && !opts.jacobi_compat) || rt == RB_RELAX_L1JACOBI;
+    if (x_zero && !(jacobi_type && sweeps > 0)) launch_vec<T>(k_fill<T>, V.n, cur, T(0));
+    if (rt == RB_RELAX_JACOBI && opts.jacobi_compat) return;   // par_relax.cpp:127,146
+    if (jacobi_type) {
+        for (int s = 0; s < sweeps; s++) {
+            if (s == 0 && x_zero) {
+                k_scale_first<T, T><<<grid_for(V.n, 256), 256, 0, stream()>>>(V.n, b, V.dinv.get(), cur);
+                RB_CHECK_LAUNCH();
+                continue;
+            }
+            launch_rows(V.A.rowptr, V.A.cols, V.A.vals, V.n, V.A.nnz, cur,
+                        EpiJacobi<T, T, T>{cur, b, V.dinv.get(), other}, V.gA);
+            std::swap(cur, other);
+        }
+        return;
+    }
+    // multicolour SOR / SSOR, in place
+    const int nc = (int)V.colour_ptr.size() - 1;
+    auto sweep = [&](int c, int backward) {
+        const int cnt = V.colour_ptr[c + 1] - V.colour_ptr[c];
+        if (cnt <= 0) return;
+        const int G = V.gA;
+        const unsigned grid = row_grid(cnt, G);
+        const int* rows = V.colour_rows.get() + V.colour_ptr[c];
+        switch (G) {
+            case 4: k_mc_sweep<4, T><<<grid, kRowBlock, 0, stream()>>>(cnt, rows, V.A.rowptr, V.A.cols, V.A.vals, cur, b, opts.relax_weight, backward); break;
+            case 8: k_mc_sweep<8, T><<<grid, kRowBlock, 0, stream()>>>(cnt, rows, V.A.rowptr, V.A.cols, V.A.vals, cur, b, opts.relax_weight, backward); break;
+            case 16: k_mc_sweep<16, T><<<grid, kRowBlock, 0, stream()>>>(cnt, rows, V.A.rowptr, V.A.cols, V.A.vals, cur, b, opts.relax_weight, backward); break;
+            default: k_mc_sweep<32, T><<<grid, kRowBlock, 0, stream()>>>(cnt, rows, V.A.rowptr, V.A.cols, V.A.vals, cur, b, opts.relax_weight, backward); break;
+        }
+        RB_CHECK_LAUNCH();
+    };
+    for (int s = 0; s < sweeps; s++) {
+        for (int c = 0; c < nc; c++) sweep(c, 0);
+        if (rt == RB_RELAX_SSOR)
+            for (int c = nc - 1; c >= 0; c--) sweep(c, 1);
+    }
+}
+
+// y = x + P xc written to a second buffer (prolongation that also moves the
+// iterate to the buffer the post-smoother should start from)
+template <typename TY>
+struct EpiAddTo {
+    const TY* x0;
+    TY* y;
+    template <typename A>
+    __device__ void operator()(long i, A s, double&) const { y[i] = (TY)((A)x0[i] + s); }
+};
+
+template <typename T>
+void Hierarchy::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool x_zero) {
+    Level<T>& V = lv[l];
+    const int L = (int)lv.size();
+    if (l == L - 1) {
+        if (coarse_n)
+            k_lu_solve<T><<<1, 256, sizeof(double) * coarse_n, stream()>>>(coarse_n, lu.get(),
+                                                                          piv.get(), b, x);
+        RB_CHECK_LAUNCH();
+        return;
+    }
+    Level<T>& C = lv[l + 1];
+    T* cur = x;
+    T* other = V.xt.get();
+    smooth(V, cur, other, b, x_zero);
+    // r = b - A x ; b_c = R r   (par_multilevel.hpp:409-411)
+    launch_rows(V.A.rowptr, V.A.cols, V.A.vals, V.n, V.A.nnz, cur,
+                EpiResidual<T, T>{b, V.r.get()}, V.gA);
+    launch_rows(V.R.rowptr, V.R.cols, V.R.vals, C.n, V.R.nnz, V.r.get(),
+                EpiStore<T>{C.b.get()}, V.gR);
+    cycle_level(lv, l + 1, C.x.get(), C.b.get(), true);
+    // x += P x_c (par_multilevel.hpp:430), into the buffer from which the
+    // post-smoothing ping-pong ends in x
+    const int rt = opts.relax_type;
+    const bool jacobi_type = (rt == RB_RELAX_JACOBI && !opts.jacobi_compat) || rt == RB_RELAX_L1JACOBI;
+    T* start = x;
+    if (jacobi_type && (opts.num_smooth_sweeps & 1)) start = (x == V.xt.get()) ? nullptr : V.xt.get();
+    if (!start) start = x;
+    if (cur == start) {
+        launch_rows(V.P.rowptr, V.P.cols, V.P.vals, V.n, V.P.nnz, C.x.get(), EpiAppend<T>{cur}, V.gP);
+    } else {
+        launch_rows(V.P.rowptr, V.P.cols, V.P.vals, V.n, V.P.nnz, C.x.get(),
+                    EpiAddTo<T>{cur, start}, V.gP);
+        cur = start;
+    }
+    other = (cur == x) ? V.xt.get() : x;
+    smooth(V, cur, other, b, false);
+    if (cur != x) {
+        RB_CUDA(cudaMemcpyAsync(x, cur, sizeof(T) * V.n, cudaMemcpyDeviceToDevice, stream()));
+    }
+}
+
+// One V-cycle on FP64 vectors of the finest size; converts at the edges of
+// an FP32 hierarchy.
+void Hierarchy::cycle64(double* x, const double* b, bool x_zero) {
+    if (opts.precision == RB_PREC_FP32) {
+        Level<float>& V = lv32[0];
+        const int n = V.n;
+        float* bb = V.b.get();
+        float* xx = V.x.get();
+        k_convert<float, double><<<grid_for(n, 256), 256, 0, stream()>>>(n, b, bb);
+        RB_CHECK_LAUNCH();
+        if (!x_zero) {
+            k_convert<float, double><<<grid_for(n, 256), 256, 0, stream()>>>(n, x, xx);
+            RB_CHECK_LAUNCH();
+        }
+        cycle_level(lv32, 0, xx, bb, x_zero);
+        k_convert<double, float><<<grid_for(n, 256), 256, 0, stream()>>>(n, xx, x);
+        RB_CHECK_LAUNCH();
+    } else {
+        cycle_level(lv64, 0, x, b, x_zero);
+    }
+}
+
+// Kernel nodes of a captured graph (the count the capture recorded is the
+// fallback if the node query fails).
+static long long count_kernel_nodes(cudaGraph_t g, long long fallback) {
+    size_t num = 0;
+    if (cudaGraphGetNodes(g, nullptr, &num) != cudaSuccess) return fallback;
+    std::vector<cudaGraphNode_t> nodes(num);
+    if (num && cudaGraphGetNodes(g, nodes.data(), &num) != cudaSuccess) return fallback;
+    long long k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
+}
+
+// Capture fn into a graph keyed by `key` on first use, then replay.
+void Hierarchy::run_graph(const std::string& key, const std::function<void()>& fn) {
+    if (!use_graphs) { fn(); return; }
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+        const long long c0 = launch_counter();
+        cudaGraph_t g;
+        RB_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
+        try {
+            fn();
+        } catch (...) {
+            cudaStreamEndCapture(stream(), &g);
+            throw;
+        }
+        RB_CUDA(cudaStreamEndCapture(stream(), &g));
+        cudaGraphExec_t ge;
+        RB_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        // kernels launched while capturing were recorded, not run
+        const long long captured = launch_counter() - c0;
+        launch_counter() = c0;
+        graph_kernels[key] = count_kernel_nodes(g, captured);
+        cudaGraphDestroy(g);
+        it = graphs.emplace(key, ge).first;
+    }
+    RB_CUDA(cudaGraphLaunch(it->second, stream()));
+    launch_counter() += graph_kernels[key];
+}
+
+static std::string pkey(const char* tag, const void* a, const void* b, const void* c = nullptr) {
+    char buf[160];
+    snprintf(buf, sizeof(buf), "%s:%p:%p:%p", tag, a, b, c);
+    return buf;
+}
+
+void Hierarchy::cycle(double* x, const double* b, bool x_zero) {
+    run_graph(pkey(x_zero ? "cyc0" : "cyc", x, b), [&] { cycle64(x, b, x_zero); });
+}
+
+// ------------------------------------------------------------ reductions --
+namespace {
+struct FinPAp {
+    KScal* s;
+    __device__ void operator()(double t) const {
+        s->pAp = t;
+        s->alpha = s->rz / t;
+        if (!(t >= 0.0) || !isfinite(t)) s->breakdown = 1;
+    }
+};
+struct FinRZ {
+    KScal* s;
+    __device__ void operator()(double t) const {
+        s->beta = t / s->rz;
+        s->rz_prev = s->rz;
+        s->rz = t;
+        if (!isfinite(t)) s->breakdown = 1;
+    }
+};
+struct FinField {
+    double* f;
+    __device__ void operator()(double t) const { *f = t; }
+};
+}  // namespace
+
+ReduceSlot global_reduce_slot(int grid);
+
+static unsigned red_grid(long n) {
+    return (unsigned)std::max(1L, std::min((long)sm_count() * 4, (n + 255) / 256));
+}
+
+void Hierarchy::dot_into(const double* a, const double* b, long n, double* field) {
+    const unsigned g = red_grid(n);
+    k_dot_fin<<<g, 256, 0, stream()>>>(a, b, n, global_reduce_slot(g), FinField{field});
+    RB_CHECK_LAUNCH();
+}
+
+KScal Hierarchy::read_scal() {
+    RB_CUDA(cudaMemcpyAsync(host_scal, scal.get(), sizeof(KScal), cudaMemcpyDeviceToHost, stream()));
+    RB_CUDA(cudaStreamSynchronize(stream()));
+    return *host_scal;
+}
+
+// ParVector::norm(2): sqrt of the sum of squares (entries <= 1e-16 add
+// nothing measurable).
+double Hierarchy::norm64(const double* v, long n) {
+    dot_into(v, v, n, &scal.get()->tmp);
+    return std::sqrt(read_scal().tmp);
+}
+
+// ------------------------------------------------------------------ solve --
+// ParMultilevel::solve (par_multilevel.hpp:459-538)
+int Hierarchy::solve(double* x, const double* b, double* hist, int cap, int* iters) {
+    const rb_csr_s& A = *master[0].A;
+    const long n = A.n_rows;
+    const double b_norm = norm64(b, n);
+    residual64(view(A), x, b, kr.get());
+    double r_norm = norm64(kr.get(), n);
+    if (std::fabs(b_norm) > 1e-16) r_norm /= b_norm;
+    int it = 0;
+    if (cap > 0) hist[0] = r_norm;
+    while (r_norm > opts.solve_tol && it < opts.max_iterations) {
+        cycle(x, b, false);
+        it++;
+        residual64(view(A), x, b, kr.get());
+        r_norm = norm64(kr.get(), n);
+        if (std::fabs(b_norm) > 1e-16) r_norm /= b_norm;
+        if (it < cap) hist[it] = r_norm;
+    }
+    *iters = it;
+    return (r_norm > opts.solve_tol) ? RB_ERR_NOT_CONVERGED : RB_OK;
+}
+
+// -------------------------------------------------------------------- PCG --
+// PCG (krylov/par_cg.cpp:121-263).  The iteration body is one CUDA graph:
+// Ap = A p fused with p.Ap (alpha computed on the device), x += alpha p with
+// r -= alpha Ap fused with r.r, the V-cycle z = M r, r.z (beta on the
+// device), p = z + beta p.  The host reads the scalars once per iteration for
+// the history and the stopping test.
+int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, int max_iter,
+                   int mode, double* hist, int cap, int* n_hist) {
+    const long n = A.n_rows;
+    RB_REQUIRE(n == master[0].A->n_rows, "PCG: A and the hierarchy differ in size");
+    if (max_iter <= 0) max_iter = (int)(1.3 * n) + 2;
+    double* r = kr.get();
+    double* z = kz.get();
+    double* p = kp.get();
+    double* Ap = kAp.get();
+    KScal* S = scal.get();
+    const CsrView<double> Av = view(A);
+    const int G = (&A == master[0].A.get()) ? gA0 : pick_group(n, A.nnz);
+    int nh = 0;
+    auto push = [&](double v) {
+        if (nh < cap) hist[nh] = v;
+        nh++;
+    };
+    RB_CUDA(cudaMemsetAsync(S, 0, sizeof(KScal), stream()));
+    // b.Mb (par_cg.cpp:150-161)
+    cycle(z, b, true);
+    dot_into(b, z, n, &S->tmp);
+    const double b_inner = read_scal().tmp;
+    const double norm_b = std::sqrt(b_inner);
+    const double bb = norm64(b, n);
+    double tol_ref = tol;
+    if (norm_b > 1e-16) tol_ref = tol * norm_b;
+    // r0 = b - A x0 ; z = M r ; p = z ; rz = r.z
+    residual64(Av, x, b, r);
+    cycle(z, r, true);
+    RB_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
+    dot_into(r, z, n, &S->rz);
+    dot_into(r, r, n, &S->rr);
+    KScal hs = read_scal();
+    if (mode == RB_PCG_REFERENCE) push(std::sqrt(hs.rz));
+    else push(std::sqrt(hs.rr) / (bb > 0 ? bb : 1.0));
+    if (mode == RB_PCG_TRUE_RESIDUAL && std::sqrt(hs.rr) <= tol * bb) {
+        *n_hist = nh;
+        return RB_OK;
+    }
+    const unsigned rg = red_grid(n);
+    auto body = [&](bool full_r) {
+        // Ap = A p ; p.Ap ; alpha = rz / pAp
+        {
+            ReduceSlot rs = global_reduce_slot(row_grid(n, G));
+            const unsigned grid = row_grid(n, G);
+            EpiStoreDot epi{p, Ap};
+            switch (G) {
+                case 4: k_csr_rows_dot<4><<<grid, kRowBlock, 0, stream()>>>(n, Av.rowptr, Av.cols, Av.vals, p, epi, rs, FinPAp{S}); break;
+                case 8: k_csr_rows_dot<8><<<grid, kRowBlock, 0, stream()>>>(n, Av.rowptr, Av.cols, Av.vals, p, epi, rs, FinPAp{S}); break;
+                case 16: k_csr_rows_dot<16><<<grid, kRowBlock, 0, stream()>>>(n, Av.rowptr, Av.cols, Av.vals, p, epi, rs, FinPAp{S}); break;
+                default: k_csr_rows_dot<32><<<grid, kRowBlock, 0, stream()>>>(n, Av.rowptr, Av.cols, Av.vals, p, epi, rs, FinPAp{S}); break;
+            }
+            RB_CHECK_LAUNCH();
+        }
+        // x += alpha p ; r -= alpha Ap (or r = b - A x every 8th iteration)
+        k_cg_update<<<rg, 256, 0, stream()>>>(n, x, r, p, Ap, S, full_r ? 0 : 1,
+                                              global_reduce_slot(rg), FinSetRR{S});
+        RB_CHECK_LAUNCH();
+        if (full_r) {
+            residual64(Av, x, b, r);
+            dot_into(r, r, n, &S->rr);
+        }
+        // z = M r ; rz_new = r.z ; beta
+        cycle64(z, r, true);
+        k_dot_fin<<<rg, 256, 0, stream()>>>(r, z, n, global_reduce_slot(rg), FinRZ{S});
+        RB_CHECK_LAUNCH();
+    };
+    int iter = 0;
+    int status = RB_ERR_NOT_CONVERGED;
+    while (iter < max_iter) {
+        iter++;
+        const bool full_r = (mode == RB_PCG_REFERENCE) ? (iter % 8 == 0) : (iter % 50 == 0);
+        run_graph(pkey(full_r ? "pcgF" : "pcg", x, b, &A), [&] { body(full_r); });
+        hs = read_scal();
+        if (hs.breakdown) {
+            *n_hist = nh;
+            return RB_ERR_BREAKDOWN;
+        }
+        bool done;
+        if (mode == RB_PCG_REFERENCE) {
+            push(hs.rz / b_inner);
+            done = hs.rz < tol_ref;
+        } else {
+            push(std::sqrt(hs.rr) / (bb > 0 ? bb : 1.0));
+            done = std::sqrt(hs.rr) <= tol * bb;
+            if (done) {
+                // confirm with the true residual
+                residual64(Av, x, b, r);
+                dot_into(r, r, n, &S->rr);
+                double tr = std::sqrt(read_scal().rr);
+                if (nh - 1 < cap) hist[nh - 1] = tr / (bb > 0 ? bb : 1.0);
+                if (tr > tol * bb) {
+                    done = false;
+                    // restart the recurrence from the true residual
+                    cycle(z, r, true);
+                    RB_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
+                    dot_into(r, z, n, &S->rz);
+                    continue;
+                }
+            }
+        }
+        if (done) { status = RB_OK; break; }
+        // p = z + beta p  (restart p = z after a full residual)
+        const bool restart = (mode == RB_PCG_REFERENCE) && full_r;
+        k_cg_p<<<grid_for(n, 256), 256, 0, stream()>>>(n, p, z, S, restart ? 1 : 0);
+        RB_CHECK_LAUNCH();
+    }
+    *n_hist = nh;
+    last_iters = iter;
+    return status;
+}
+
+// -------------------------------------------------------------------- CG --
+// CG (krylov/par_cg.cpp:8-118); uses only the Krylov vectors of a hierarchy
+// sized for A (callers without a hierarchy get a work-only one).
+int krylov_cg(const rb_csr_s& A, double* x, const double* b, double tol, int max_iter,
+              double* hist, int cap, int* n_hist) {
+    const long n = A.n_rows;
+    if (max_iter <= 0) max_iter = (int)(1.3 * n) + 2;
+    DevArray<double> r((size_t)n + 1), p((size_t)n + 1), Ap((size_t)n + 1);
+    DevArray<KScal> S(1);
+    S.zero();
+    KScal* hs = nullptr;
+    RB_CUDA(cudaMallocHost(&hs, sizeof(KScal)));
+    std::unique_ptr<KScal, decltype(&cudaFreeHost)> guard(hs, &cudaFreeHost);
+    auto rd = [&]() {
+        RB_CUDA(cudaMemcpyAsync(hs, S.get(), sizeof(KScal), cudaMemcpyDeviceToHost, stream()));
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return *hs;
+    };
+    const unsigned rg = red_grid(n);
+    auto dot = [&](const double* a, const double* c, double* f) {
+        k_dot_fin<<<rg, 256, 0, stream()>>>(a, c, n, global_reduce_slot(rg), FinField{f});
+        RB_CHECK_LAUNCH();
+    };
+    dot(b, b, &S.get()->bb);
+    double b_norm = std::sqrt(rd().bb);
+    if (b_norm < 1e-16) b_norm = 1.0;
+    const CsrView<double> Av = view(A);
+    residual64(Av, x, b, r.get());
+    RB_CUDA(cudaMemcpyAsync(p.get(), r.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
+    dot(r.get(), r.get(), &S.get()->rz);
+    double rr = rd().rz;
+    double norm_r = std::sqrt(rr);
+    int nh = 0;
+    auto push = [&](double v) { if (nh < cap) hist[nh] = v; nh++; };
+    push(norm_r / b_norm);
+    if (norm_r != 0.0) tol = tol * norm_r;
+    int iter = 0;
+    const int G = pick_group(n, A.nnz);
+    while (norm_r > tol && iter < max_iter) {
+        ReduceSlot rs = global_reduce_slot(row_grid(n, G));
+        launch_rows(Av.rowptr, Av.cols, Av.vals, n, Av.nnz, p.get(), EpiStore<double>{Ap.get()}, G);
+        dot(Ap.get(), p.get(), &S.get()->pAp);
+        (void)rs;
+        KScal s = rd();
+        if (s.pAp < 0.0 || !std::isfinite(s.pAp)) { *n_hist = nh; return RB_ERR_BREAKDOWN; }
+        const double alpha = rr / s.pAp;
+        k_axpy<double><<<grid_for(n, 256), 256, 0, stream()>>>(n, x, p.get(), alpha);
+        RB_CHECK_LAUNCH();
+        if ((iter % 8) && iter > 0) {
+            k_axpy<double><<<grid_for(n, 256), 256, 0, stream()>>>(n, r.get(), Ap.get(), -1.0 * alpha);
+            RB_CHECK_LAUNCH();
+        } else {
+            residual64(Av, x, b, r.get());
+        }
+        dot(r.get(), r.get(), &S.get()->rz);
+        const double next = rd().rz;
+        const double beta = next / rr;
+        k_scale<double><<<grid_for(n, 256), 256, 0, stream()>>>(n, p.get(), beta);
+        RB_CHECK_LAUNCH();
+        k_axpy<double><<<grid_for(n, 256), 256, 0, stream()>>>(n, p.get(), r.get(), 1.0);
+        RB_CHECK_LAUNCH();
+        rr = next;
+        norm_r = std::sqrt(rr);
+        push(norm_r / b_norm);
+        iter++;
+    }
+    *n_hist = nh;
+    return norm_r > tol ? RB_ERR_NOT_CONVERGED : RB_OK;
+}
+
+// -------------------------------------------------------------- BiCGStab --
+// BiCGStab (krylov/par_bicgstab.cpp:11-126) and Pre_BiCGStab (:240-371,
+// right preconditioning; the reference reads its iteration counter
+// uninitialised and never sizes p_hat/s_hat -- here both start defined).
+int krylov_bicgstab(const rb_csr_s& A, Hierarchy* ml, double* x, const double* b, double tol,
+                    int max_iter, double* hist, int cap, int* n_hist) {
+    const long n = A.n_rows;
+    if (max_iter <= 0) max_iter = (int)(1.3 * n) + 2;
+    DevArray<double> r((size_t)n + 1), rs_((size_t)n + 1), s((size_t)n + 1), p((size_t)n + 1),
+        Ap((size_t)n + 1), As((size_t)n + 1), ph, sh;
+    if (ml) { ph.alloc((size_t)n + 1); sh.alloc((size_t)n + 1); }
+    DevArray<double> sc(8);
+    sc.zero();
+    double* hs = nullptr;
+    RB_CUDA(cudaMallocHost(&hs, sizeof(double) * 8));
+    std::unique_ptr<double, decltype(&cudaFreeHost)> guard(hs, &cudaFreeHost);
+    const unsigned rg = red_grid(n);
+    auto dot = [&](const double* a, const double* c, int f) {
+        k_dot_fin<<<rg, 256, 0, stream()>>>(a, c, n, global_reduce_slot(rg), FinField{sc.get() + f});
+        RB_CHECK_LAUNCH();
+    };
+    auto rd = [&]() {
+        RB_CUDA(cudaMemcpyAsync(hs, sc.get(), sizeof(double) * 8, cudaMemcpyDeviceToHost, stream()));
+        RB_CUDA(cudaStreamSynchronize(stream()));
+    };
+    auto cp = [&](double* d, const double* src) {
+        RB_CUDA(cudaMemcpyAsync(d, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
+    };
+    auto axpy = [&](double* y, const double* xx, double a) {
+        k_axpy<double><<<grid_for(n, 256), 256, 0, stream()>>>(n, y, xx, a);
+        RB_CHECK_LAUNCH();
+    };
+    const CsrView<double> Av = view(A);
+    const int G = pick_group(n, A.nnz);
+    residual64(Av, x, b, r.get());
+    cp(rs_.get(), r.get());
+    cp(p.get(), r.get());
+    dot(r.get(), rs_.get(), 0);
+    dot(r.get(), r.get(), 1);
+    rd();
+    double rr = hs[0];
+    double norm_r = std::sqrt(hs[1]);
+    int nh = 0;
+    auto push = [&](double v) { if (nh < cap) hist[nh] = v; nh++; };
+    push(norm_r);
+    if (norm_r != 0.0) tol = tol * norm_r;
+    int iter = 0;
+    while (norm_r > tol && iter < max_iter) {
+        const double* pv = p.get();
+        if (ml) { ml->cycle(ph.get(), p.get(), true); pv = ph.get(); }
+        launch_rows(Av.rowptr, Av.cols, Av.vals, n, Av.nnz, pv, EpiStore<double>{Ap.get()}, G);
+        dot(Ap.get(), rs_.get(), 2);
+        rd();
+        const double alpha = rr / hs[2];
+        cp(s.get(), r.get());
+        axpy(s.get(), Ap.get(), -1.0 * alpha);
+        const double* sv = s.get();
+        if (ml) { ml->cycle(sh.get(), s.get(), true); sv = sh.get(); }
+        launch_rows(Av.rowptr, Av.cols, Av.vals, n, Av.nnz, sv, EpiStore<double>{As.get()}, G);
+        dot(As.get(), s.get(), 3);
+        dot(As.get(), As.get(), 4);
+        rd();
+        const double omega = hs[3] / hs[4];
+        axpy(x, pv, alpha);
+        axpy(x, sv, omega);
+        cp(r.get(), s.get());
+        axpy(r.get(), As.get(), -1.0 * omega);
+        dot(r.get(), rs_.get(), 5);
+        dot(r.get(), r.get(), 6);
+        rd();
+        const double next = hs[5];
+        const double beta = (next / rr) * (alpha / omega);
+        k_scale<double><<<grid_for(n, 256), 256, 0, stream()>>>(n, p.get(), beta);
+        RB_CHECK_LAUNCH();
+        axpy(p.get(), r.get(), 1.0);
+        axpy(p.get(), Ap.get(), -1.0 * beta * omega);
+        rr = next;
+        norm_r = std::sqrt(hs[6]);
+        push(norm_r);
+        iter++;
+        if (!std::isfinite(norm_r)) { *n_hist = nh; return RB_ERR_BREAKDOWN; }
+    }
+    *n_hist = nh;
+    return norm_r > tol ? RB_ERR_NOT_CONVERGED : RB_OK;
+}
+
+template void Hierarchy::build_levels<double>(std::vector<Level<double>>&);
+template void Hierarchy::build_levels<float>(std::vector<Level<float>>&);
+
+}  // namespace rb

@@ -1,0 +1,91 @@
+// hierarchy.cuh -- the device AMG hierarchy (ParMultilevel at world size 1).
+#pragma once
+
+#include <functional>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "blas1.cuh"
+#include "rb_internal.cuh"
+
+namespace rb {
+
+// FP64 result of setup for one level (multilevel/par_level.hpp:15-43).
+struct MasterLevel {
+    std::unique_ptr<rb_csr_s> A;   // diagonal first
+    std::unique_ptr<rb_csr_s> P;   // n_l x n_{l+1}
+    std::unique_ptr<rb_csr_s> R;   // P^T, stored so restriction is a gather
+    DevArray<int> states;          // C/F splitting
+};
+
+// Cycle data of one level in the cycle precision T.
+template <typename T>
+struct Level {
+    int n = 0;
+    CsrView<T> A, P, R;
+    DevArray<T> Avals, Pvals, Rvals;   // value copies when T != double
+    DevArray<T> dinv;                  // w / a_ii (Jacobi) or w / sum|a_ij| (L1)
+    DevArray<int> colour_rows;         // rows grouped by colour (multicolour SOR)
+    std::vector<int> colour_ptr;
+    DevArray<T> x, b, r, xt;
+    int gA = 0, gP = 0, gR = 0;        // lanes per row picked by the autotuner
+    void alloc_vectors();
+};
+
+struct Hierarchy {
+    rb_amg_opts opts{};
+    std::vector<MasterLevel> master;
+    std::vector<Level<double>> lv64;
+    std::vector<Level<float>> lv32;
+    int coarse_n = 0;
+    DevArray<double> lu;
+    DevArray<int> piv;
+    // Krylov work vectors (finest size) and device scalars
+    DevArray<double> kr, kz, kp, kAp, ks, kAs, krs, kph, ksh;
+    DevArray<KScal> scal;
+    KScal* host_scal = nullptr;
+    int gA0 = 0;
+    bool use_graphs = true;
+    std::map<std::string, cudaGraphExec_t> graphs;
+    std::map<std::string, long long> graph_kernels;
+    double setup_seconds = 0;
+    int last_iters = 0;
+
+    ~Hierarchy();
+    void setup(const rb_csr_s& A, const rb_amg_opts& o, const double* weights_host);
+    void build_cycle_data();
+    template <typename T>
+    void build_levels(std::vector<Level<T>>& lv);
+    int num_levels() const { return (int)master.size(); }
+
+    template <typename T>
+    void smooth(Level<T>& V, T*& cur, T*& other, const T* b, bool x_zero);
+    template <typename T>
+    void cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool x_zero);
+    void cycle64(double* x, const double* b, bool x_zero);
+    void cycle(double* x, const double* b, bool x_zero);
+    void run_graph(const std::string& key, const std::function<void()>& fn);
+    void release_graphs();
+
+    void dot_into(const double* a, const double* b, long n, double* field);
+    double norm64(const double* v, long n);
+    KScal read_scal();
+
+    int solve(double* x, const double* b, double* hist, int cap, int* iters);
+    int pcg(const rb_csr_s& A, double* x, const double* b, double tol, int max_iter, int mode,
+            double* hist, int cap, int* n_hist);
+    size_t device_bytes() const;
+};
+
+int krylov_cg(const rb_csr_s& A, double* x, const double* b, double tol, int max_iter,
+              double* hist, int cap, int* n_hist);
+int krylov_bicgstab(const rb_csr_s& A, Hierarchy* ml, double* x, const double* b, double tol,
+                    int max_iter, double* hist, int cap, int* n_hist);
+
+}  // namespace rb
+
+struct rb_amg_s {
+    rb::Hierarchy h;
+};

@@ -1,0 +1,64 @@
+// rb_internal.cuh -- handle types behind the C ABI and shared declarations.
+#pragma once
+
+#include "rb_common.cuh"
+
+struct rb_csr_s {
+    int n_rows = 0, n_cols = 0;
+    long long nnz = 0;
+    rb::DevArray<int> rowptr, cols;
+    rb::DevArray<double> vals;
+};
+
+struct rb_vec_s {
+    int n = 0;
+    rb::DevArray<double> v;
+};
+
+namespace rb {
+
+// Non-owning view of a CSR matrix with values of type T.
+template <typename T>
+struct CsrView {
+    int n_rows = 0, n_cols = 0;
+    long long nnz = 0;
+    const int* rowptr = nullptr;
+    const int* cols = nullptr;
+    const T* vals = nullptr;
+};
+
+inline CsrView<double> view(const rb_csr_s& A) {
+    CsrView<double> v;
+    v.n_rows = A.n_rows; v.n_cols = A.n_cols; v.nnz = A.nnz;
+    v.rowptr = A.rowptr.get(); v.cols = A.cols.get(); v.vals = A.vals.get();
+    return v;
+}
+
+rb_csr_s* new_csr(int n_rows, int n_cols, long long nnz);
+// Sort every row by column and move the diagonal to the front.
+void sort_rows_diag_first(rb_csr_s& A, bool diag_first);
+// Transpose; rows of the result list source rows in increasing order.
+rb_csr_s* transpose(const rb_csr_s& A);
+// Exclusive scan of n ints into out (n+1 entries, out[n] = total); returns total.
+long long exclusive_scan(const int* in, int* out, int n);
+// Sum of n doubles, deterministic (fixed two-stage tree).
+void dot_async(const double* a, const double* b, int n, double* result_dev);
+
+// SpMV family on FP64 CSR (C ABI primitives).
+void spmv64(const CsrView<double>& A, const double* x, double* y);
+void residual64(const CsrView<double>& A, const double* x, const double* b, double* r);
+void spmv_append64(const CsrView<double>& A, const double* x, double* y);
+
+// Setup components (setup.cu).
+rb_csr_s* strength(const rb_csr_s& A, int kind, double theta);
+void split_pmis(const rb_csr_s& S, const double* weights_dev, int* states_dev);
+rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* states_dev, int kind,
+                        double filter);
+rb_csr_s* spgemm(const rb_csr_s& A, const rb_csr_s& B);
+rb_csr_s* rap(const rb_csr_s& A, const rb_csr_s& P, const rb_csr_s* R_in, bool diag_first);
+int colour_rows(const rb_csr_s& A, int* colour_dev);
+
+// glibc rand() weights of the reference (par_multilevel.hpp:215-225).
+std::vector<double> rand_weights(int n, int first_row);
+
+}  // namespace rb

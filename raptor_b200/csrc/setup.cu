@@ -1,0 +1,887 @@
+// setup.cu -- AMG setup kernels (Ruge-Stuben path), FP64, bit-exact.
+//
+// Compiled with -fmad=false, and every accumulation spells out __dmul_rn /
+// __dadd_rn: the reference's -O3 x86-64 build has no FMA, and a one-ulp
+// difference in an RAP value can flip a strict strength comparison on the
+// next level and change every coarser C/F splitting.  Each kernel keeps the
+// reference's per-entry accumulation order.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <cstdlib>
+
+#include "rb_internal.cuh"
+
+namespace rb {
+
+constexpr double kZeroTol = 1e-16;           // core/types.hpp:26
+constexpr double kRandMax = 2147483647.0;    // glibc RAND_MAX (par_strength.cpp:78)
+constexpr int kSelected = 1, kUnselected = 0, kUnassigned = -1, kNoNeighbors = -2;
+constexpr int kNewSelection = 3, kNewUnselection = 2;   // core/types.hpp:31-37
+
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+std::vector<double> rand_weights(int n, int first_row) {
+    // form_rand_weights, multilevel/par_multilevel.hpp:215-225
+    std::vector<double> w((size_t)n);
+    srand(2448422 + first_row);
+    for (int i = 0; i < n; i++) w[i] = double(rand()) / RAND_MAX;
+    return w;
+}
+
+// ============================================================ strength ===
+// classical_strength, par_strength.cpp:8-339 (num_variables = 1).
+template <bool FILL>
+__global__ void k_classical_strength(int n, const int* __restrict__ rp,
+                                     const int* __restrict__ ci, const double* __restrict__ cv,
+                                     double theta, int* cnt, const int* srp, int* sci,
+                                     double* scv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int rs = rp[i], re = rp[i + 1];
+    int out = FILL ? srp[i] : 0, k = 0;
+    if (re - rs) {
+        double diag;
+        if (ci[rs] == i) { diag = cv[rs]; rs++; }
+        else diag = 0.0;
+        double row_scale;
+        if (diag < 0.0) {
+            row_scale = -kRandMax;
+            for (int j = rs; j < re; j++) if (cv[j] > row_scale) row_scale = cv[j];
+        } else {
+            row_scale = kRandMax;
+            for (int j = rs; j < re; j++) if (cv[j] < row_scale) row_scale = cv[j];
+        }
+        double thr = dmul(row_scale, theta);
+        if (FILL) { sci[out] = i; scv[out] = diag; }
+        k = 1;
+        for (int j = rs; j < re; j++) {
+            double v = cv[j];
+            if (diag < 0 ? (v > thr) : (v < thr)) {
+                if (FILL) { sci[out + k] = ci[j]; scv[out + k] = v; }
+                k++;
+            }
+        }
+    }
+    if (!FILL) cnt[i] = k;
+}
+
+// symmetric_strength first pass, par_strength.cpp:385-450
+__global__ void k_sym_scales(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                             const double* __restrict__ cv, double theta, double* scales,
+                             int* neg) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int rs = rp[i], re = rp[i + 1];
+    double sc = 0.0;
+    int ng = 0;
+    if (re - rs) {
+        double diag;
+        if (ci[rs] == i) { diag = cv[rs]; rs++; }
+        else diag = 0.0;
+        double row_scale;
+        if (diag < 0.0) {
+            ng = 1;
+            row_scale = -kRandMax;
+            for (int j = rs; j < re; j++) if (cv[j] > row_scale) row_scale = cv[j];
+        } else {
+            row_scale = kRandMax;
+            for (int j = rs; j < re; j++) if (cv[j] < row_scale) row_scale = cv[j];
+        }
+        sc = dmul(row_scale, theta);
+    }
+    scales[i] = sc;
+    neg[i] = ng;
+}
+
+// symmetric_strength second pass, par_strength.cpp:457-505: the first entry
+// of every non-empty row is kept as the diagonal.
+template <bool FILL>
+__global__ void k_sym_strength(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const double* __restrict__ cv, const double* __restrict__ sc,
+                               const int* __restrict__ neg, int* cnt, const int* srp, int* sci,
+                               double* scv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int rs = rp[i], re = rp[i + 1];
+    int out = FILL ? srp[i] : 0, k = 0;
+    if (re - rs) {
+        int nd = neg[i];
+        double thr = sc[i];
+        if (FILL) { sci[out] = i; scv[out] = cv[rs]; }
+        rs++;
+        k = 1;
+        for (int j = rs; j < re; j++) {
+            double v = cv[j];
+            int c = ci[j];
+            if ((nd && v > thr) || (!nd && v < thr) || (neg[c] && v > sc[c]) ||
+                (!neg[c] && v < sc[c])) {
+                if (FILL) { sci[out + k] = c; scv[out + k] = v; }
+                k++;
+            }
+        }
+    }
+    if (!FILL) cnt[i] = k;
+}
+
+rb_csr_s* strength(const rb_csr_s& A, int kind, double theta) {
+    const int n = A.n_rows;
+    DevArray<int> cnt((size_t)n + 1);
+    const unsigned g = grid_for(n, 256);
+    rb_csr_s* S = nullptr;
+    if (kind == RB_STRENGTH_CLASSICAL) {
+        if (n) k_classical_strength<false><<<g, 256, 0, stream()>>>(
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), theta, cnt.get(), nullptr, nullptr, nullptr);
+        RB_CHECK_LAUNCH();
+        DevArray<int> rp((size_t)n + 1);
+        long long nnz = exclusive_scan(cnt.get(), rp.get(), n);
+        S = new_csr(n, A.n_cols, nnz);
+        S->rowptr = std::move(rp);
+        if (n) k_classical_strength<true><<<g, 256, 0, stream()>>>(
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), theta, nullptr, S->rowptr.get(),
+            S->cols.get(), S->vals.get());
+        RB_CHECK_LAUNCH();
+    } else {
+        DevArray<double> sc((size_t)n + 1);
+        DevArray<int> neg((size_t)n + 1);
+        if (n) k_sym_scales<<<g, 256, 0, stream()>>>(n, A.rowptr.get(), A.cols.get(),
+                                                     A.vals.get(), theta, sc.get(), neg.get());
+        RB_CHECK_LAUNCH();
+        if (n) k_sym_strength<false><<<g, 256, 0, stream()>>>(
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), sc.get(), neg.get(), cnt.get(),
+            nullptr, nullptr, nullptr);
+        RB_CHECK_LAUNCH();
+        DevArray<int> rp((size_t)n + 1);
+        long long nnz = exclusive_scan(cnt.get(), rp.get(), n);
+        S = new_csr(n, A.n_cols, nnz);
+        S->rowptr = std::move(rp);
+        if (n) k_sym_strength<true><<<g, 256, 0, stream()>>>(
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), sc.get(), neg.get(), nullptr,
+            S->rowptr.get(), S->cols.get(), S->vals.get());
+        RB_CHECK_LAUNCH();
+    }
+    return S;
+}
+
+// ================================================================ PMIS ===
+// split_pmis / pmis_main_loop, par_cf_splitting.cpp:75-131, 158-309,
+// 403-495, 1200-1381.  A round reads only weights (which change only when a
+// vertex is assigned, to 0) and writes states, so visiting the unassigned
+// vertices in parallel selects the same set as the sequential loop.
+
+// Off-diagonal column lists of S (the leading diagonal is skipped), counts.
+__global__ void k_s_colcount(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                             int* cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = rp[i], e = rp[i + 1];
+    if (s < e && ci[s] == i) s++;
+    for (int j = s; j < e; j++) atomicAdd(cnt + ci[j], 1);
+}
+
+__global__ void k_s_colfill(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                            int* fill, int* tci) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = rp[i], e = rp[i + 1];
+    if (s < e && ci[s] == i) s++;
+    for (int j = s; j < e; j++) tci[atomicAdd(fill + ci[j], 1)] = i;
+}
+
+// set_initial_states (:114-131) + initial_weights (:246-309) + the
+// pre-loop filter (:1291-1306).  Each influence adds 1.0 in sequence.
+__global__ void k_pmis_init(int n, const int* __restrict__ rp, const int* __restrict__ tp,
+                            const double* __restrict__ rnd, double* w, int* st) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int state = (rp[i + 1] - rp[i] > 1) ? kUnassigned : kNoNeighbors;
+    double wi = rnd[i];
+    for (int k = tp[i]; k < tp[i + 1]; k++) wi = dadd(wi, 1.0);
+    if (state == kUnassigned && wi < 1) { state = kUnselected; wi = 0.0; }
+    else if (state != kUnassigned) wi = 0.0;
+    w[i] = wi;
+    st[i] = state;
+}
+
+__global__ void k_pmis_select(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                              const int* __restrict__ tp, const int* __restrict__ tci,
+                              const double* __restrict__ w, int* st) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n || st[u] != kUnassigned) return;
+    double wu = w[u];
+    int s = rp[u], e = rp[u + 1];
+    if (s < e && ci[s] == u) s++;
+    for (int j = s; j < e; j++) if (w[ci[j]] > wu) return;
+    for (int j = tp[u]; j < tp[u + 1]; j++) if (w[tci[j]] > wu) return;
+    st[u] = kNewSelection;
+}
+
+__global__ void k_pmis_mark(int n, const int* __restrict__ tp, const int* __restrict__ tci,
+                            int* st) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || st[c] != kNewSelection) return;
+    for (int j = tp[c]; j < tp[c + 1]; j++) {
+        int r = tci[j];
+        if (st[r] == kUnassigned) st[r] = kNewUnselection;
+    }
+}
+
+__global__ void k_pmis_update(int n, double* w, int* st, int* remaining) {
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    int keep = 0;
+    if (u < n) {
+        int s = st[u];
+        if (s == kNewSelection) { w[u] = 0.0; st[u] = kSelected; }
+        else if (s == kUnassigned || s == kNewUnselection) {
+            if (w[u] < 1.0 || s == kNewUnselection) { w[u] = 0.0; st[u] = kUnselected; }
+            else keep = 1;
+        }
+    }
+    keep = __syncthreads_count(keep);
+    if (threadIdx.x == 0 && keep) atomicAdd(remaining, keep);
+}
+
+void split_pmis(const rb_csr_s& S, const double* weights_dev, int* states_dev) {
+    const int n = S.n_rows;
+    if (n == 0) return;
+    const unsigned g = grid_for(n, 256);
+    DevArray<int> cnt((size_t)n + 1), tp((size_t)n + 1);
+    cnt.zero();
+    k_s_colcount<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), cnt.get());
+    RB_CHECK_LAUNCH();
+    long long tn = exclusive_scan(cnt.get(), tp.get(), n);
+    DevArray<int> tci((size_t)std::max(tn, 1LL));
+    RB_CUDA(cudaMemcpyAsync(cnt.get(), tp.get(), sizeof(int) * n, cudaMemcpyDeviceToDevice, stream()));
+    k_s_colfill<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), cnt.get(), tci.get());
+    RB_CHECK_LAUNCH();
+    DevArray<double> w((size_t)n);
+    k_pmis_init<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), tp.get(), weights_dev, w.get(), states_dev);
+    RB_CHECK_LAUNCH();
+    DevArray<int> rem(1);
+    for (int round = 0; round < 100000; round++) {
+        rem.zero();
+        k_pmis_select<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), tp.get(), tci.get(),
+                                               w.get(), states_dev);
+        k_pmis_mark<<<g, 256, 0, stream()>>>(n, tp.get(), tci.get(), states_dev);
+        k_pmis_update<<<g, 256, 0, stream()>>>(n, w.get(), states_dev, rem.get());
+        RB_CHECK_LAUNCH();
+        if (read_scalar(rem.get()) == 0) return;
+    }
+    throw Error(RB_ERR_INVALID, "PMIS did not terminate");
+}
+
+// ======================================================= interpolation ===
+__global__ void k_flag_selected(int n, const int* __restrict__ st, int* f) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) f[i] = st[i] == kSelected ? 1 : 0;
+}
+
+// Position of column c within [lo, hi) of an unsorted list, or -1.
+__device__ __forceinline__ int find_in(const int* list, int lo, int hi, int c) {
+    for (int t = lo; t < hi; t++)
+        if (list[t] == c) return t;
+    return -1;
+}
+
+// --- mod_classical_interpolation, par_interpolation.cpp:991-1451 --------
+__global__ void k_modclass_count(int n, const int* __restrict__ srp, const int* __restrict__ sci,
+                                 const int* __restrict__ st, int* cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (st[i] == kSelected) { cnt[i] = 1; return; }
+    int k = 0;
+    for (int j = srp[i] + 1; j < srp[i + 1]; j++) k += st[sci[j]] == kSelected;
+    cnt[i] = k;
+}
+
+// pcols holds fine column indices while the row is assembled.
+__global__ void k_modclass_fill(int n, const int* __restrict__ arp, const int* __restrict__ aci,
+                                const double* __restrict__ acv, const int* __restrict__ srp,
+                                const int* __restrict__ sci, const double* __restrict__ scv,
+                                const int* __restrict__ st, const int* __restrict__ prp,
+                                int* pcols, double* pvals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p0 = prp[i];
+    if (st[i] == kSelected) { pcols[p0] = i; pvals[p0] = 1.0; return; }
+    int m = p0;
+    for (int j = srp[i] + 1; j < srp[i + 1]; j++) {
+        int c = sci[j];
+        if (st[c] == kSelected) { pcols[m] = c; pvals[m] = scv[j]; m++; }
+    }
+    const int p1 = m;
+    int start = arp[i], end = arp[i + 1];
+    if (start >= end) return;
+    int ctr = srp[i] + 1, end_S = srp[i + 1];
+    double weak_sum = acv[start++];
+    for (int j = start; j < end; j++) {
+        int col = aci[j];
+        double val = acv[j];
+        if (ctr < end_S && sci[ctr] == col) {
+            ctr++;
+            if (st[col] == kSelected) continue;
+            double coarse_sum = 0;
+            int sk = arp[col], ek = arp[col + 1];
+            double diag = acv[sk++];
+            int sign = diag > 0 ? 1 : -1;
+            for (int k = sk; k < ek; k++) {
+                int ck = aci[k];
+                if (st[ck] == kSelected) {
+                    double vk = acv[k];
+                    if (dmul(vk, (double)sign) < 0 && find_in(pcols, p0, p1, ck) >= 0)
+                        coarse_sum = dadd(coarse_sum, vk);
+                }
+            }
+            if (fabs(coarse_sum) < kZeroTol) weak_sum = dadd(weak_sum, val);
+            else coarse_sum = __ddiv_rn(val, coarse_sum);
+            if (coarse_sum != 0.0) {
+                for (int k = arp[col] + 1; k < ek; k++) {
+                    int ck = aci[k];
+                    if (st[ck] == kSelected) {
+                        double vk = acv[k];
+                        if (dmul(vk, (double)sign) < 0) {
+                            int idx = find_in(pcols, p0, p1, ck);
+                            if (idx >= 0) pvals[idx] = dadd(pvals[idx], dmul(coarse_sum, vk));
+                        }
+                    }
+                }
+            }
+        } else if (st[col] != kNoNeighbors) {
+            weak_sum = dadd(weak_sum, val);
+        }
+    }
+    for (int t = p0; t < p1; t++) pvals[t] = __ddiv_rn(pvals[t], -weak_sum);
+}
+
+// --- extended_interpolation, par_interpolation.cpp:280-989 ---------------
+// Upper bound of a row's pattern: strong C neighbours plus the strong C
+// neighbours of every strong F neighbour.
+__global__ void k_ext_bound(int n, const int* __restrict__ srp, const int* __restrict__ sci,
+                            const int* __restrict__ st, int* ub) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (st[i] != kUnselected) { ub[i] = 1; return; }
+    int b = 0;
+    for (int j = srp[i] + 1; j < srp[i + 1]; j++) {
+        int c = sci[j];
+        if (st[c] == kSelected) b++;
+        else if (st[c] == kUnselected) b += srp[c + 1] - srp[c] - 1;
+    }
+    ub[i] = b;
+}
+
+// Insertion-ordered unique pattern (par_interpolation.cpp:574-690).
+__global__ void k_ext_pattern(int n, const int* __restrict__ srp, const int* __restrict__ sci,
+                              const int* __restrict__ st, const int* __restrict__ uoff,
+                              int* list, int* cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int o = uoff[i];
+    if (st[i] != kUnselected) {
+        if (st[i] == kSelected) { list[o] = i; cnt[i] = 1; }
+        else cnt[i] = 0;
+        return;
+    }
+    int m = o;
+    for (int j = srp[i] + 1; j < srp[i + 1]; j++) {
+        int c = sci[j];
+        if (st[c] == kSelected) {
+            if (find_in(list, o, m, c) < 0) list[m++] = c;
+        } else if (st[c] == kUnselected) {
+            for (int k = srp[c] + 1; k < srp[c + 1]; k++) {
+                int ck = sci[k];
+                if (st[ck] == kSelected && find_in(list, o, m, ck) < 0) list[m++] = ck;
+            }
+        }
+    }
+    cnt[i] = m - o;
+}
+
+// Values (par_interpolation.cpp:692-944) and filter_interp (:175-278).
+// The row is assembled in pcols/pvals[prp[i] ...]; kept entries are
+// compacted to the front and their count written to kept[i].
+__global__ void k_ext_fill(int n, const int* __restrict__ arp, const int* __restrict__ aci,
+                           const double* __restrict__ acv, const int* __restrict__ srp,
+                           const int* __restrict__ sci, const int* __restrict__ st,
+                           const int* __restrict__ uoff, const int* __restrict__ list,
+                           const int* __restrict__ prp, int* pcols, double* pvals, double filter,
+                           int* kept) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p0 = prp[i], p1 = prp[i + 1];
+    const int o = uoff[i];
+    for (int t = p0; t < p1; t++) { pcols[t] = list[o + (t - p0)]; pvals[t] = 0.0; }
+    if (st[i] == kSelected) { pvals[p0] = 1.0; }
+    if (st[i] == kUnselected) {
+        int start = arp[i], end = arp[i + 1];
+        double weak_sum = acv[start++];
+        int ctr = srp[i] + 1, end_S = srp[i + 1];
+        for (int j = start; j < end; j++) {
+            int col = aci[j];
+            double val = acv[j];
+            int idx = find_in(pcols, p0, p1, col);
+            if (idx >= 0) {
+                pvals[idx] = dadd(pvals[idx], val);
+                if (ctr < end_S && sci[ctr] == col) ctr++;
+            } else if (ctr < end_S && sci[ctr] == col) {
+                ctr++;
+                if (st[col] != kUnselected) continue;
+                double col_sum = 0;
+                int sk = arp[col], ek = arp[col + 1];
+                double diag = acv[sk++];
+                int sign = diag > 0 ? 1 : -1;
+                for (int k = sk; k < ek; k++) {
+                    double vk = acv[k];
+                    int ck = aci[k];
+                    if (dmul(vk, (double)sign) < 0 && (ck == i || find_in(pcols, p0, p1, ck) >= 0))
+                        col_sum = dadd(col_sum, vk);
+                }
+                if (fabs(col_sum) < kZeroTol) {
+                    weak_sum = dadd(weak_sum, val);
+                } else {
+                    col_sum = __ddiv_rn(val, col_sum);
+                    for (int k = arp[col] + 1; k < ek; k++) {
+                        int ck = aci[k];
+                        double vk = acv[k];
+                        if (dmul(vk, (double)sign) < 0) {
+                            if (ck == i) weak_sum = dadd(weak_sum, dmul(col_sum, vk));
+                            else {
+                                int id = find_in(pcols, p0, p1, ck);
+                                if (id >= 0) pvals[id] = dadd(pvals[id], dmul(col_sum, vk));
+                            }
+                        }
+                    }
+                }
+            } else {
+                if (st[col] != kNoNeighbors) weak_sum = dadd(weak_sum, val);
+            }
+        }
+        if (fabs(weak_sum) > kZeroTol)
+            for (int t = p0; t < p1; t++) pvals[t] = __ddiv_rn(pvals[t], -weak_sum);
+    }
+    // filter_interp (only when 0 < filter <= 1)
+    int out = p0;
+    if (filter > kZeroTol && filter <= 1) {
+        double row_max = 0;
+        for (int t = p0; t < p1; t++) {
+            double a = fabs(pvals[t]);
+            if (a > row_max) row_max = a;
+        }
+        row_max = dmul(row_max, filter);
+        double row_sum = 0, remain_sum = 0;
+        for (int t = p0; t < p1; t++) {
+            double v = pvals[t];
+            row_sum = dadd(row_sum, v);
+            if (fabs(v) >= row_max) {
+                pcols[out] = pcols[t];
+                pvals[out] = v;
+                out++;
+                remain_sum = dadd(remain_sum, v);
+            }
+        }
+        if (fabs(remain_sum) > kZeroTol && fabs(dsub(row_sum, remain_sum)) > kZeroTol) {
+            double scale = __ddiv_rn(row_sum, remain_sum);
+            for (int t = p0; t < out; t++) pvals[t] = dmul(pvals[t], scale);
+        }
+    } else {
+        out = p1;
+    }
+    kept[i] = out - p0;
+}
+
+// Copy the first kept[i] entries of each row, mapping fine C columns to their
+// coarse index, and sort the row by column.
+__global__ void k_compact_rows(int n, const int* __restrict__ srcp, const int* __restrict__ scol,
+                               const double* __restrict__ sval, const int* __restrict__ dstp,
+                               const int* __restrict__ cmap, int* dcol, double* dval) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = srcp[i], d = dstp[i], m = dstp[i + 1] - d;
+    for (int t = 0; t < m; t++) {
+        int c = cmap[scol[s + t]];
+        double v = sval[s + t];
+        int k = t - 1;
+        while (k >= 0 && dcol[d + k] > c) {
+            dcol[d + k + 1] = dcol[d + k];
+            dval[d + k + 1] = dval[d + k];
+            k--;
+        }
+        dcol[d + k + 1] = c;
+        dval[d + k + 1] = v;
+    }
+}
+
+rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* st, int kind,
+                        double filter) {
+    const int n = A.n_rows;
+    RB_REQUIRE(S.n_rows == n, "strength matrix does not match A");
+    const unsigned g = grid_for(n, 256);
+    DevArray<int> flag((size_t)n + 1), cmap((size_t)n + 1);
+    if (n) k_flag_selected<<<g, 256, 0, stream()>>>(n, st, flag.get());
+    RB_CHECK_LAUNCH();
+    const int nc = (int)exclusive_scan(flag.get(), cmap.get(), n);
+    DevArray<int> cnt((size_t)n + 1), prp((size_t)n + 1), kept((size_t)n + 1);
+    DevArray<int> pcols;
+    DevArray<double> pvals;
+    if (kind == RB_INTERP_MODCLASSICAL) {
+        if (n) k_modclass_count<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), st, cnt.get());
+        RB_CHECK_LAUNCH();
+        long long nnz = exclusive_scan(cnt.get(), prp.get(), n);
+        rb_csr_s* P = new_csr(n, nc, nnz);
+        P->rowptr = std::move(prp);
+        DevArray<int> fine_cols((size_t)std::max(nnz, 1LL));
+        if (n) k_modclass_fill<<<g, 256, 0, stream()>>>(
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(),
+            S.vals.get(), st, P->rowptr.get(), fine_cols.get(), P->vals.get());
+        RB_CHECK_LAUNCH();
+        // map to coarse indices (rows are already in increasing column order)
+        DevArray<double> tmpv((size_t)std::max(nnz, 1LL));
+        RB_CUDA(cudaMemcpyAsync(tmpv.get(), P->vals.get(), sizeof(double) * nnz,
+                                cudaMemcpyDeviceToDevice, stream()));
+        if (n) k_compact_rows<<<g, 256, 0, stream()>>>(n, P->rowptr.get(), fine_cols.get(),
+                                                       tmpv.get(), P->rowptr.get(), cmap.get(),
+                                                       P->cols.get(), P->vals.get());
+        RB_CHECK_LAUNCH();
+        return P;
+    }
+    // Extended+i
+    DevArray<int> ub((size_t)n + 1), uoff((size_t)n + 1);
+    if (n) k_ext_bound<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), st, ub.get());
+    RB_CHECK_LAUNCH();
+    long long ubt = exclusive_scan(ub.get(), uoff.get(), n);
+    DevArray<int> list((size_t)std::max(ubt, 1LL));
+    if (n) k_ext_pattern<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), st, uoff.get(),
+                                                  list.get(), cnt.get());
+    RB_CHECK_LAUNCH();
+    long long nnz0 = exclusive_scan(cnt.get(), prp.get(), n);
+    pcols.alloc((size_t)std::max(nnz0, 1LL));
+    pvals.alloc((size_t)std::max(nnz0, 1LL));
+    if (n) k_ext_fill<<<g, 256, 0, stream()>>>(
+        n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(), st,
+        uoff.get(), list.get(), prp.get(), pcols.get(), pvals.get(), filter, kept.get());
+    RB_CHECK_LAUNCH();
+    list.release();
+    DevArray<int> frp((size_t)n + 1);
+    long long nnz = exclusive_scan(kept.get(), frp.get(), n);
+    rb_csr_s* P = new_csr(n, nc, nnz);
+    P->rowptr = std::move(frp);
+    if (n) k_compact_rows<<<g, 256, 0, stream()>>>(n, prp.get(), pcols.get(), pvals.get(),
+                                                   P->rowptr.get(), cmap.get(), P->cols.get(),
+                                                   P->vals.get());
+    RB_CHECK_LAUNCH();
+    return P;
+}
+
+// ============================================================== SpGEMM ===
+// C = A B, one warp per row of A.  spgemm_helper (util/linalg/matmult.cpp
+// :71-137) accumulates sums[col] += a_ij * b_jk walking A's row in stored
+// order; here the warp walks A's row serially and its lanes split B's row j,
+// whose columns are distinct, so every accumulator still receives its terms
+// in A's row order and the sums are bit-identical.  |sum| <= 1e-16 is
+// dropped; the row is written sorted by column (add_append's sort,
+// util/linalg/add.cpp:75).  Pass 1 counts survivors, pass 2 writes them.
+
+__device__ __forceinline__ unsigned hash_col(int c) { return (unsigned)c * 2654435761u; }
+
+// Insert/find column c in an open-addressing table of size H (power of two).
+__device__ __forceinline__ int hash_slot(int* keys, int H, int c) {
+    unsigned h = hash_col(c) & (H - 1);
+    while (true) {
+        int k = keys[h];
+        if (k == c) return (int)h;
+        if (k == -1) {
+            int old = atomicCAS(keys + h, -1, c);
+            if (old == -1 || old == c) return (int)h;
+        }
+        h = (h + 1) & (H - 1);
+    }
+}
+
+template <bool WRITE>
+__device__ void spgemm_row(int lane, int row, const int* __restrict__ arp,
+                           const int* __restrict__ aci, const double* __restrict__ acv,
+                           const int* __restrict__ brp, const int* __restrict__ bci,
+                           const double* __restrict__ bcv, int* keys, double* sums, int* clist,
+                           int H, int* cnt, const int* crp, int* cci, double* ccv) {
+    for (int t = lane; t < H; t += 32) { keys[t] = -1; sums[t] = 0.0; }
+    __syncwarp();
+    const int as = arp[row], ae = arp[row + 1];
+    for (int j = as; j < ae; j++) {
+        const int ca = aci[j];
+        const double va = acv[j];
+        const int bs = brp[ca], be = brp[ca + 1];
+        for (int k = bs + lane; k < be; k += 32) {
+            const int cb = bci[k];
+            const int slot = hash_slot(keys, H, cb);
+            sums[slot] = dadd(sums[slot], dmul(va, bcv[k]));
+        }
+        __syncwarp();
+    }
+    // compact surviving entries into clist (slot indices), warp-ordered
+    int m = 0;
+    for (int base = 0; base < H; base += 32) {
+        const int t = base + lane;
+        const bool keep = keys[t] != -1 && fabs(sums[t]) > kZeroTol;
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) clist[m + __popc(bal & ((1u << lane) - 1))] = t;
+        m += __popc(bal);
+    }
+    __syncwarp();
+    if (!WRITE) {
+        if (lane == 0) cnt[row] = m;
+        return;
+    }
+    // rank by column and write sorted
+    const int out = crp[row];
+    for (int a = lane; a < m; a += 32) {
+        const int sa = clist[a];
+        const int c = keys[sa];
+        int r = 0;
+        for (int b = 0; b < m; b++) r += keys[clist[b]] < c;
+        cci[out + r] = c;
+        ccv[out + r] = sums[sa];
+    }
+}
+
+template <bool WRITE, int H, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+k_spgemm_smem(const int* __restrict__ rows, int nrows, const int* __restrict__ arp,
+              const int* __restrict__ aci, const double* __restrict__ acv,
+              const int* __restrict__ brp, const int* __restrict__ bci,
+              const double* __restrict__ bcv, int* cnt, const int* crp, int* cci, double* ccv) {
+    extern __shared__ unsigned char smem[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* sums = reinterpret_cast<double*>(smem) + (size_t)w * H;
+    int* keys = reinterpret_cast<int*>(reinterpret_cast<double*>(smem) + (size_t)WPB * H) + (size_t)w * 2 * H;
+    int* clist = keys + H;
+    const int idx = blockIdx.x * WPB + w;
+    if (idx >= nrows) return;
+    spgemm_row<WRITE>(lane, rows[idx], arp, aci, acv, brp, bci, bcv, keys, sums, clist, H, cnt,
+                      crp, cci, ccv);
+}
+
+// Rows whose bound exceeds the shared tables: tables in global scratch.
+template <bool WRITE>
+__global__ void k_spgemm_global(const int* __restrict__ rows, int nrows,
+                                const long long* __restrict__ toff, const int* __restrict__ tsize,
+                                const int* __restrict__ arp, const int* __restrict__ aci,
+                                const double* __restrict__ acv, const int* __restrict__ brp,
+                                const int* __restrict__ bci, const double* __restrict__ bcv,
+                                int* gkeys, double* gsums, int* glist, int* cnt, const int* crp,
+                                int* cci, double* ccv) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nrows) return;
+    const long long o = toff[w];
+    spgemm_row<WRITE>(lane, rows[w], arp, aci, acv, brp, bci, bcv, gkeys + o, gsums + o, glist + o,
+                      tsize[w], cnt, crp, cci, ccv);
+}
+
+// Upper bound of the row size of C and the bin of each row.
+__global__ void k_spgemm_bound(int n, const int* __restrict__ arp, const int* __restrict__ aci,
+                               const int* __restrict__ brp, int* ub, int* bins, int* bin_count,
+                               int lim0, int lim1) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long b = 0;
+    for (int j = arp[i]; j < arp[i + 1]; j++) b += brp[aci[j] + 1] - brp[aci[j]];
+    int u = (int)(b > INT_MAX / 4 ? INT_MAX / 4 : b);
+    ub[i] = u;
+    int bin = u <= lim0 ? 0 : (u <= lim1 ? 1 : 2);
+    int p = atomicAdd(bin_count + bin, 1);
+    bins[(size_t)bin * n + p] = i;
+}
+
+namespace {
+constexpr int kH0 = 512, kW0 = 8;    // 8 warps x (512 x 16 B) = 64 KB
+constexpr int kH1 = 4096, kW1 = 2;   // 2 warps x (4096 x 16 B) = 128 KB
+
+inline int next_pow2(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+template <bool WRITE>
+void spgemm_pass(const rb_csr_s& A, const rb_csr_s& B, const int* bins, const int* bcount,
+                 const std::vector<int>& big_rows_tsize, const DevArray<long long>& toff,
+                 const DevArray<int>& tsize, DevArray<int>& gkeys, DevArray<double>& gsums,
+                 DevArray<int>& glist, int* cnt, const int* crp, int* cci, double* ccv) {
+    const int n = A.n_rows;
+    if (bcount[0]) {
+        size_t sm = (size_t)kW0 * kH0 * (sizeof(double) + 2 * sizeof(int));
+        auto kern = k_spgemm_smem<WRITE, kH0, kW0>;
+        RB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        kern<<<grid_for(bcount[0], kW0), kW0 * 32, sm, stream()>>>(
+            bins, bcount[0], A.rowptr.get(), A.cols.get(), A.vals.get(), B.rowptr.get(),
+            B.cols.get(), B.vals.get(), cnt, crp, cci, ccv);
+        RB_CHECK_LAUNCH();
+    }
+    if (bcount[1]) {
+        size_t sm = (size_t)kW1 * kH1 * (sizeof(double) + 2 * sizeof(int));
+        auto kern = k_spgemm_smem<WRITE, kH1, kW1>;
+        RB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        kern<<<grid_for(bcount[1], kW1), kW1 * 32, sm, stream()>>>(
+            bins + (size_t)n, bcount[1], A.rowptr.get(), A.cols.get(), A.vals.get(),
+            B.rowptr.get(), B.cols.get(), B.vals.get(), cnt, crp, cci, ccv);
+        RB_CHECK_LAUNCH();
+    }
+    if (bcount[2]) {
+        k_spgemm_global<WRITE><<<grid_for((long)bcount[2] * 32, 128), 128, 0, stream()>>>(
+            bins + 2 * (size_t)n, bcount[2], toff.get(), tsize.get(), A.rowptr.get(),
+            A.cols.get(), A.vals.get(), B.rowptr.get(), B.cols.get(), B.vals.get(), gkeys.get(),
+            gsums.get(), glist.get(), cnt, crp, cci, ccv);
+        RB_CHECK_LAUNCH();
+    }
+    (void)big_rows_tsize;
+}
+}  // namespace
+
+rb_csr_s* spgemm(const rb_csr_s& A, const rb_csr_s& B) {
+    RB_REQUIRE(A.n_cols == B.n_rows, "spgemm: inner dimensions differ");
+    const int n = A.n_rows;
+    DevArray<int> ub((size_t)n + 1), bins((size_t)3 * n + 3), bcnt(3);
+    bcnt.zero();
+    if (n)
+        k_spgemm_bound<<<grid_for(n, 256), 256, 0, stream()>>>(n, A.rowptr.get(), A.cols.get(),
+                                                              B.rowptr.get(), ub.get(), bins.get(),
+                                                              bcnt.get(), kH0 / 2, kH1 / 2);
+    RB_CHECK_LAUNCH();
+    int hb[3];
+    bcnt.download(hb, 3);
+    RB_CUDA(cudaStreamSynchronize(stream()));
+    // global tables for the largest rows
+    DevArray<long long> toff;
+    DevArray<int> tsize, gkeys, glist;
+    DevArray<double> gsums;
+    std::vector<int> big;
+    if (hb[2]) {
+        std::vector<int> rows(hb[2]), ubh(n);
+        RB_CUDA(cudaMemcpyAsync(rows.data(), bins.get() + 2 * (size_t)n, sizeof(int) * hb[2],
+                                cudaMemcpyDeviceToHost, stream()));
+        RB_CUDA(cudaMemcpyAsync(ubh.data(), ub.get(), sizeof(int) * n, cudaMemcpyDeviceToHost,
+                                stream()));
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        std::vector<long long> off(hb[2]);
+        std::vector<int> sz(hb[2]);
+        long long tot = 0;
+        for (int t = 0; t < hb[2]; t++) {
+            sz[t] = next_pow2(std::max(64, 2 * ubh[rows[t]]));
+            off[t] = tot;
+            tot += sz[t];
+        }
+        toff.alloc(hb[2]);
+        toff.upload(off.data(), hb[2]);
+        tsize.alloc(hb[2]);
+        tsize.upload(sz.data(), hb[2]);
+        gkeys.alloc((size_t)tot);
+        gsums.alloc((size_t)tot);
+        glist.alloc((size_t)tot);
+    }
+    DevArray<int> cnt((size_t)n + 1);
+    spgemm_pass<false>(A, B, bins.get(), hb, big, toff, tsize, gkeys, gsums, glist, cnt.get(),
+                       nullptr, nullptr, nullptr);
+    DevArray<int> crp((size_t)n + 1);
+    long long nnz = exclusive_scan(cnt.get(), crp.get(), n);
+    rb_csr_s* C = new_csr(n, B.n_cols, nnz);
+    C->rowptr = std::move(crp);
+    spgemm_pass<true>(A, B, bins.get(), hb, big, toff, tsize, gkeys, gsums, glist, nullptr,
+                      C->rowptr.get(), C->cols.get(), C->vals.get());
+    return C;
+}
+
+// ParCSRMatrix::mult then mult_T (par_matmult.cpp:73-107, 141-196): AP
+// walks A's rows in stored (diagonal-first) order; P^T A P walks the rows of
+// R = P^T, which list fine rows in increasing order like the CSC that
+// CSR_to_CSC builds.  Then sort + move_diag (par_ruge_stuben_solver.hpp:142-143).
+rb_csr_s* rap(const rb_csr_s& A, const rb_csr_s& P, const rb_csr_s* R_in, bool diag_first) {
+    RB_REQUIRE(A.n_rows == P.n_rows && A.n_cols == P.n_rows, "rap: A and P do not match");
+    rb_csr_s* AP = spgemm(A, P);
+    rb_csr_s* Rt = nullptr;
+    const rb_csr_s* R = R_in;
+    if (!R) { Rt = transpose(P); R = Rt; }
+    rb_csr_s* Ac = nullptr;
+    try {
+        Ac = spgemm(*R, *AP);
+    } catch (...) {
+        delete AP;
+        delete Rt;
+        throw;
+    }
+    delete AP;
+    delete Rt;
+    if (diag_first) sort_rows_diag_first(*Ac, true);
+    return Ac;
+}
+
+// ========================================================== colouring ===
+// Jones-Plassmann rounds (the multicolour SOR stand-in; not in the
+// reference): an uncoloured row that beats every uncoloured neighbour by a
+// fixed integer hash (ties by index) takes the smallest colour unused by its
+// coloured neighbours.  Rows coloured in a round become visible only to the
+// next round, so the colouring does not depend on thread order.
+__device__ __forceinline__ unsigned jp_hash(unsigned x) {
+    x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+    return x;
+}
+
+__global__ void k_jp_round(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           int* colour, int* left) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int coloured = 0;
+    if (i < n && colour[i] < 0) {
+        const unsigned hi = jp_hash((unsigned)i);
+        bool ok = true;
+        for (int j = rp[i]; j < rp[i + 1] && ok; j++) {
+            int c = ci[j];
+            if (c == i || colour[c] >= 0) continue;
+            unsigned hc = jp_hash((unsigned)c);
+            if (hc > hi || (hc == hi && c > i)) ok = false;
+        }
+        if (ok) {
+            unsigned long long used = 0;
+            for (int j = rp[i]; j < rp[i + 1]; j++) {
+                int c = ci[j];
+                int cc = colour[c];
+                if (c != i && cc >= 0 && cc < 64) used |= 1ull << cc;
+            }
+            int k = 0;
+            while (k < 64 && ((used >> k) & 1ull)) k++;
+            colour[i] = -2 - k;   // pending: encoded as -(k+2)
+            coloured = 1;
+        }
+    }
+    coloured = __syncthreads_count(coloured);
+    if (threadIdx.x == 0 && coloured) atomicAdd(left, coloured);
+}
+
+__global__ void k_jp_commit(int n, int* colour, int* maxc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && colour[i] <= -2) {
+        colour[i] = -colour[i] - 2;
+        atomicMax(maxc, colour[i] + 1);
+    }
+}
+
+int colour_rows(const rb_csr_s& A, int* colour) {
+    const int n = A.n_rows;
+    if (n == 0) return 0;
+    RB_CUDA(cudaMemsetAsync(colour, 0xff, sizeof(int) * n, stream()));   // -1
+    DevArray<int> cntr(2);
+    cntr.zero();
+    long long done = 0;
+    const unsigned g = grid_for(n, 256);
+    for (int round = 0; round < 100000 && done < n; round++) {
+        RB_CUDA(cudaMemsetAsync(cntr.get(), 0, sizeof(int), stream()));
+        k_jp_round<<<g, 256, 0, stream()>>>(n, A.rowptr.get(), A.cols.get(), colour, cntr.get());
+        k_jp_commit<<<g, 256, 0, stream()>>>(n, colour, cntr.get() + 1);
+        RB_CHECK_LAUNCH();
+        done += read_scalar(cntr.get());
+    }
+    RB_REQUIRE(done == n, "colouring did not terminate");
+    return read_scalar(cntr.get() + 1);
+}
+
+}  // namespace rb

@@ -1,0 +1,233 @@
+// sparse.cu -- CSR containers, row canonicalisation, transpose, scans,
+// deterministic reductions and the FP64 SpMV primitives of the C ABI.
+#include <cub/cub.cuh>
+
+#include <climits>
+#include <mutex>
+
+#include "rb_internal.cuh"
+#include "spmv.cuh"
+
+namespace rb {
+
+// ------------------------------------------------------------- context --
+namespace {
+cudaStream_t g_stream = nullptr;
+cudaStream_t g_own_stream = nullptr;
+int g_sms = 0;
+thread_local std::string g_last_error;
+}  // namespace
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+long long& launch_counter() {
+    static long long c = 0;
+    return c;
+}
+const char* last_error_cstr() { return g_last_error.c_str(); }
+
+cudaStream_t stream() {
+    if (!g_stream) {
+        if (!g_own_stream) RB_CUDA(cudaStreamCreateWithFlags(&g_own_stream, cudaStreamNonBlocking));
+        g_stream = g_own_stream;
+    }
+    return g_stream;
+}
+
+void set_stream(cudaStream_t s) { g_stream = s ? s : nullptr; }
+
+int sm_count() {
+    if (!g_sms) {
+        int dev = 0;
+        RB_CUDA(cudaGetDevice(&dev));
+        RB_CUDA(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return g_sms;
+}
+
+rb_csr_s* new_csr(int n_rows, int n_cols, long long nnz) {
+    RB_REQUIRE(n_rows >= 0 && n_cols >= 0 && nnz >= 0, "negative matrix dimension");
+    RB_REQUIRE(nnz <= INT_MAX, "matrix has more than 2^31-1 nonzeros (int32 indices)");
+    auto* A = new rb_csr_s();
+    A->n_rows = n_rows;
+    A->n_cols = n_cols;
+    A->nnz = nnz;
+    A->rowptr.alloc((size_t)n_rows + 1);
+    A->cols.alloc((size_t)(nnz > 0 ? nnz : 1));
+    A->vals.alloc((size_t)(nnz > 0 ? nnz : 1));
+    return A;
+}
+
+// ------------------------------------------------------------------ scan --
+__global__ void k_scan_tail(const int* in, int* out, int n, long long* total) {
+    long long t = (n > 0) ? (long long)out[n - 1] + (long long)in[n - 1] : 0;
+    *total = t;
+    out[n] = (int)t;
+}
+
+long long exclusive_scan(const int* in, int* out, int n) {
+    if (n == 0) {
+        RB_CUDA(cudaMemsetAsync(out, 0, sizeof(int), stream()));
+        return 0;
+    }
+    size_t bytes = 0;
+    RB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, stream()));
+    DevArray<char> tmp(bytes + 16);
+    RB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, stream()));
+    DevArray<long long> tot(1);
+    k_scan_tail<<<1, 1, 0, stream()>>>(in, out, n, tot.get());
+    RB_CHECK_LAUNCH();
+    long long t = read_scalar(tot.get());
+    RB_REQUIRE(t >= 0 && t <= INT_MAX, "prefix sum exceeds the int32 index range");
+    return t;
+}
+
+// -------------------------------------------------- row canonicalisation --
+// Insertion sort of each row by column (CSRMatrix::sort, core/matrix.cpp
+// :588-618), then the diagonal moved to the front (move_diag_helper,
+// :730-786).  One thread per row: rows of the path are short.
+__global__ void k_sort_rows(int n, const int* __restrict__ rp, int* cols, double* vals,
+                            int diag_first) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = rp[i], e = rp[i + 1];
+    for (int j = s + 1; j < e; j++) {
+        int c = cols[j];
+        double v = vals[j];
+        int k = j - 1;
+        while (k >= s && cols[k] > c) {
+            cols[k + 1] = cols[k];
+            vals[k + 1] = vals[k];
+            k--;
+        }
+        cols[k + 1] = c;
+        vals[k + 1] = v;
+    }
+    if (diag_first) {
+        for (int j = s; j < e; j++) {
+            if (cols[j] == i) {
+                double t = vals[j];
+                for (int k = j; k > s; k--) {
+                    cols[k] = cols[k - 1];
+                    vals[k] = vals[k - 1];
+                }
+                cols[s] = i;
+                vals[s] = t;
+                break;
+            }
+        }
+    }
+}
+
+void sort_rows_diag_first(rb_csr_s& A, bool diag_first) {
+    if (A.n_rows == 0) return;
+    k_sort_rows<<<grid_for(A.n_rows, 256), 256, 0, stream()>>>(A.n_rows, A.rowptr.get(),
+                                                                 A.cols.get(), A.vals.get(),
+                                                                 diag_first ? 1 : 0);
+    RB_CHECK_LAUNCH();
+}
+
+// ------------------------------------------------------------ transpose --
+__global__ void k_count_cols(long long nnz, const int* __restrict__ cols, int* cnt) {
+    long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < nnz) atomicAdd(cnt + cols[j], 1);
+}
+
+__global__ void k_scatter_T(int n, const int* __restrict__ rp, const int* __restrict__ cols,
+                            const double* __restrict__ vals, int* fill, int* tcols,
+                            double* tvals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int j = rp[i]; j < rp[i + 1]; j++) {
+        int c = cols[j];
+        int p = atomicAdd(fill + c, 1);
+        tcols[p] = i;
+        tvals[p] = vals[j];
+    }
+}
+
+rb_csr_s* transpose(const rb_csr_s& A) {
+    rb_csr_s* T = new_csr(A.n_cols, A.n_rows, A.nnz);
+    DevArray<int> cnt((size_t)A.n_cols + 1);
+    cnt.zero();
+    if (A.nnz)
+        k_count_cols<<<grid_for(A.nnz, 256), 256, 0, stream()>>>(A.nnz, A.cols.get(), cnt.get());
+    RB_CHECK_LAUNCH();
+    exclusive_scan(cnt.get(), T->rowptr.get(), A.n_cols);
+    RB_CUDA(cudaMemcpyAsync(cnt.get(), T->rowptr.get(), sizeof(int) * A.n_cols,
+                            cudaMemcpyDeviceToDevice, stream()));
+    if (A.n_rows)
+        k_scatter_T<<<grid_for(A.n_rows, 256), 256, 0, stream()>>>(
+            A.n_rows, A.rowptr.get(), A.cols.get(), A.vals.get(), cnt.get(), T->cols.get(),
+            T->vals.get());
+    RB_CHECK_LAUNCH();
+    // atomics leave each row in arbitrary order: sort by source row
+    sort_rows_diag_first(*T, false);
+    return T;
+}
+
+// ---------------------------------------------------------------- dots --
+struct FinStore {
+    double* out;
+    __device__ void operator()(double t) const { *out = t; }
+};
+
+__global__ void __launch_bounds__(256) k_dot(const double* __restrict__ a,
+                                             const double* __restrict__ b, long n,
+                                             ReduceSlot rs, FinStore fin) {
+    double t = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x)
+        t += a[i] * b[i];
+    block_reduce_finish(t, rs, fin);
+}
+
+namespace {
+struct ReduceScratch {
+    DevArray<double> partials;
+    DevArray<unsigned> ticket;
+    std::once_flag once;
+};
+ReduceScratch& scratch() {
+    static ReduceScratch s;
+    return s;
+}
+}  // namespace
+
+// One scratch for every reduction on the library stream.  It is allocated
+// once and never moved, because CUDA graphs capture its address.
+constexpr int kMaxReduceGrid = 1 << 16;
+
+ReduceSlot global_reduce_slot(int grid) {
+    auto& s = scratch();
+    RB_REQUIRE(grid <= kMaxReduceGrid, "reduction grid too large");
+    if (!s.partials.size()) {
+        s.partials.alloc(kMaxReduceGrid);
+        s.ticket.alloc(1);
+        s.ticket.zero();
+        RB_CUDA(cudaStreamSynchronize(stream()));
+    }
+    return ReduceSlot{s.partials.get(), s.ticket.get()};
+}
+
+void dot_async(const double* a, const double* b, int n, double* result_dev) {
+    const int grid = std::max(1, std::min(sm_count() * 4, (int)((n + 255) / 256)));
+    ReduceSlot rs = global_reduce_slot(grid);
+    k_dot<<<grid, 256, 0, stream()>>>(a, b, n, rs, FinStore{result_dev});
+    RB_CHECK_LAUNCH();
+}
+
+// ------------------------------------------------------- FP64 SpMV ops --
+void spmv64(const CsrView<double>& A, const double* x, double* y) {
+    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiStore<double>{y});
+}
+
+void residual64(const CsrView<double>& A, const double* x, const double* b, double* r) {
+    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiResidual<double, double>{b, r});
+}
+
+void spmv_append64(const CsrView<double>& A, const double* x, double* y) {
+    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiAppend<double>{y});
+}
+
+}  // namespace rb

@@ -1,0 +1,209 @@
+// spmv.cuh -- CSR row kernels for the solve phase (HBM-bandwidth bound).
+//
+// One kernel template covers every "row of A times a vector, then something"
+// operation of the V-cycle and the Krylov loop: b = A x (CSR_spmv,
+// util/linalg/spmv.cpp:52-67), r = b - A x (CSR_residual, :69-85),
+// b += A x (CSR_append, :88-103), a Jacobi sweep (par_relax.cpp:106-152), and
+// b = A x fused with a deterministic dot product.  G lanes share a row; a
+// warp walks 32/G consecutive rows per step so the column/value streams of
+// neighbouring rows are read by one coalesced warp access, the gathered x
+// goes through the read-only path, and partial sums meet in a shuffle tree.
+#pragma once
+
+#include "rb_common.cuh"
+
+namespace rb {
+
+constexpr int kRowBlock = 256;
+
+template <typename T> struct AccOf { using type = T; };
+template <> struct AccOf<float> { using type = float; };
+
+// Block-level tree reduction followed by a fixed-order reduction of the block
+// partials by the last block to finish; the result is bit-reproducible for a
+// given grid.  fin(total) runs in one thread of the last block.
+struct ReduceSlot {
+    double* partials;   // gridDim.x entries
+    unsigned* ticket;   // zero before the launch, reset by the last block
+};
+
+template <class Fin>
+__device__ void block_reduce_finish(double v, const ReduceSlot& rs, Fin fin) {
+    __shared__ double warp_part[32];
+    __shared__ bool is_last;
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) warp_part[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        double t = lane < (int)(blockDim.x >> 5) ? warp_part[lane] : 0.0;
+        t = warp_sum(t);
+        if (lane == 0) {
+            rs.partials[blockIdx.x] = t;
+            __threadfence();
+            unsigned done = atomicAdd(rs.ticket, 1u);
+            is_last = (done == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        // fixed-order second stage: thread k sums partials k, k+blockDim, ...
+        double t = 0.0;
+        for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x)
+            t += ((volatile double*)rs.partials)[k];
+        t = warp_sum(t);
+        if (lane == 0) warp_part[wid] = t;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += warp_part[w];
+            *rs.ticket = 0u;
+            fin(tot);
+        }
+    }
+}
+
+// ------------------------------------------------------------ epilogues --
+template <typename TY>
+struct EpiStore {
+    TY* y;
+    template <typename A>
+    __device__ void operator()(long i, A s, double&) const { y[i] = (TY)s; }
+};
+
+template <typename TB, typename TY>
+struct EpiResidual {
+    const TB* b;
+    TY* r;
+    template <typename A>
+    __device__ void operator()(long i, A s, double&) const { r[i] = (TY)((A)b[i] - s); }
+};
+
+template <typename TY>
+struct EpiAppend {
+    TY* y;
+    template <typename A>
+    __device__ void operator()(long i, A s, double&) const { y[i] = (TY)((A)y[i] + s); }
+};
+
+// Jacobi / L1-Jacobi: xn = xo + dinv (b - A xo); dinv already holds w/d_i.
+template <typename TX, typename TB, typename TY>
+struct EpiJacobi {
+    const TX* xo;
+    const TB* b;
+    const TX* dinv;
+    TY* xn;
+    template <typename A>
+    __device__ void operator()(long i, A s, double&) const {
+        xn[i] = (TY)((A)xo[i] + (A)dinv[i] * ((A)b[i] - s));
+    }
+};
+
+// y = A p and accumulate p.y (the CG denominator)
+struct EpiStoreDot {
+    const double* p;
+    double* y;
+    __device__ void operator()(long i, double s, double& red) const {
+        y[i] = s;
+        red += p[i] * s;
+    }
+};
+
+struct NoFinish {
+    __device__ void operator()(double) const {}
+};
+
+// ------------------------------------------------------------- kernels --
+template <int G, typename TV, typename TX, class Epi>
+__global__ void __launch_bounds__(kRowBlock)
+k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
+           const TV* __restrict__ cv, const TX* __restrict__ x, Epi epi) {
+    using Acc = typename AccOf<TV>::type;
+    constexpr int RPW = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / G, gl = lane & (G - 1);
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    double red = 0.0;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        const bool valid = row < n;
+        int s = 0, e = 0;
+        if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); }
+        Acc sum = 0;
+        int j = s + gl;
+        for (; j + G < e; j += 2 * G) {
+            const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + G);
+            const TV v0 = __ldg(cv + j), v1 = __ldg(cv + j + G);
+            sum += (Acc)v0 * (Acc)__ldg(x + c0);
+            sum += (Acc)v1 * (Acc)__ldg(x + c1);
+        }
+        if (j < e) sum += (Acc)__ldg(cv + j) * (Acc)__ldg(x + __ldg(ci + j));
+        sum = group_sum<G>(sum);
+        if (valid && gl == 0) epi(row, sum, red);
+    }
+    (void)red;
+}
+
+template <int G, class Fin>
+__global__ void __launch_bounds__(kRowBlock)
+k_csr_rows_dot(long n, const int* __restrict__ rp, const int* __restrict__ ci,
+               const double* __restrict__ cv, const double* __restrict__ x, EpiStoreDot epi,
+               ReduceSlot rs, Fin fin) {
+    constexpr int RPW = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / G, gl = lane & (G - 1);
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    double red = 0.0;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        const bool valid = row < n;
+        int s = 0, e = 0;
+        if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); }
+        double sum = 0;
+        for (int j = s + gl; j < e; j += G) sum += __ldg(cv + j) * __ldg(x + __ldg(ci + j));
+        sum = group_sum<G>(sum);
+        if (valid && gl == 0) epi(row, sum, red);
+    }
+    block_reduce_finish(red, rs, fin);
+}
+
+// Lanes per row from the mean row length (a power of two in 2..32).
+inline int pick_group(long n, long long nnz) {
+    double mean = n > 0 ? (double)nnz / (double)n : 1.0;
+    if (mean <= 3) return 2;
+    if (mean <= 6) return 4;
+    if (mean <= 14) return 8;
+    if (mean <= 40) return 16;
+    return 32;
+}
+
+inline unsigned row_grid(long n, int G) {
+    long warps = (n * G + 31) / 32;
+    long blocks = (warps * 32 + kRowBlock - 1) / kRowBlock;
+    long cap = (long)sm_count() * 16;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return (unsigned)blocks;
+}
+
+template <typename TV, typename TX, class Epi>
+void launch_rows(const int* rp, const int* ci, const TV* cv, long n, long long nnz, const TX* x,
+                 Epi epi, int G = 0, cudaStream_t st = nullptr) {
+    if (n <= 0) return;
+    if (!st) st = stream();
+    if (G <= 0) G = pick_group(n, nnz);
+    const unsigned grid = row_grid(n, G);
+    switch (G) {
+        case 2: k_csr_rows<2><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
+        case 4: k_csr_rows<4><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
+        case 8: k_csr_rows<8><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
+        case 16: k_csr_rows<16><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
+        default: k_csr_rows<32><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
+    }
+    RB_CHECK_LAUNCH();
+}
+
+}  // namespace rb

@@ -1,0 +1,333 @@
+"""GPU parity: every CUDA path against the oracle on the same seeded inputs.
+
+Integer and pattern results (stencil patterns, strength patterns, C/F
+splittings, P and A_l patterns) must be bit-exact.  FP64 setup values are
+compared exactly too (the setup kernels keep the reference's accumulation
+order without FMA); solve-phase values within 1e-12 relative, residual
+histories within 1e-10 relative.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.conftest import golden_csr
+
+pytestmark = pytest.mark.gpu
+
+rb = pytest.importorskip("raptor_b200")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    rb.init(0)
+
+
+def to_rb(A):
+    n, m, _ = A.shape
+    rp, ci, cv = A.arrays()
+    return rb.ParCSRMatrix.from_arrays(n, m, rp, ci, cv)
+
+
+def rb_tuple(M):
+    n, m, _ = M.info()
+    return (n, m) + M.arrays()
+
+
+def oc_tuple(M):
+    n, m, _ = M.shape
+    return (n, m) + M.arrays()
+
+
+def canon(t):
+    n, m, rp, ci, cv = t
+    ci = ci.copy()
+    cv = cv.copy()
+    for i in range(n):
+        s, e = rp[i], rp[i + 1]
+        o = np.argsort(ci[s:e], kind="stable")
+        ci[s:e] = ci[s:e][o]
+        cv[s:e] = cv[s:e][o]
+    return n, m, rp, ci, cv
+
+
+def assert_csr_equal(got, ref, rtol=0.0, exact_order=False):
+    if not exact_order:
+        got, ref = canon(got), canon(ref)
+    assert got[0] == ref[0] and got[1] == ref[1]
+    np.testing.assert_array_equal(got[2], ref[2])
+    np.testing.assert_array_equal(got[3], ref[3])
+    if rtol == 0.0:
+        np.testing.assert_array_equal(got[4], ref[4])
+    else:
+        np.testing.assert_allclose(got[4], ref[4], rtol=rtol, atol=0)
+
+
+AN = (0.001, math.pi / 8.0)
+
+
+def aniso(n):
+    return O.stencil_grid(O.diffusion_stencil_2d(*AN), [n, n])
+
+
+def lap27(n):
+    return O.stencil_grid(O.laplace_stencil_27pt(), [n, n, n])
+
+
+def aniso7(n, cz=0.01):
+    st = np.zeros(27)
+    st[13] = 2 + 2 + 2 * cz
+    st[12] = st[14] = -1.0
+    st[10] = st[16] = -1.0
+    st[4] = st[22] = -cz
+    return O.stencil_grid(st, [n, n, n])
+
+
+# ---------------------------------------------------------------- gallery --
+@pytest.mark.parametrize("kind,n", [("aniso", 25), ("aniso", 100), ("aniso", 37), ("lap27", 10),
+                                    ("lap27", 17), ("aniso7", 12)])
+def test_stencil_generator_bit_exact(kind, n):
+    if kind == "aniso":
+        st = rb.diffusion_stencil_2d(*AN)
+        np.testing.assert_array_equal(st, O.diffusion_stencil_2d(*AN))
+        got = rb.par_stencil_grid(st, [n, n])
+        ref = aniso(n)
+    elif kind == "lap27":
+        got = rb.par_stencil_grid(rb.laplace_stencil_27pt(), [n, n, n])
+        ref = lap27(n)
+    else:
+        ref = aniso7(n)
+        st = np.zeros(27)
+        st[13] = 2 + 2 + 2 * 0.01
+        st[12] = st[14] = st[10] = st[16] = -1.0
+        st[4] = st[22] = -0.01
+        got = rb.par_stencil_grid(st, [n, n, n])
+    assert_csr_equal(rb_tuple(got), oc_tuple(ref), exact_order=True)
+
+
+def test_stencil_against_golden(golden):
+    got = rb.par_stencil_grid(rb.laplace_stencil_27pt(), [10, 10, 10])
+    assert_csr_equal(rb_tuple(got), golden_csr(golden, "laplacian27"))
+
+
+# ------------------------------------------------------------ SpMV family --
+@pytest.mark.parametrize("name", ["aniso", "laplacian27", "random"])
+def test_spmv_golden(golden, name):
+    A = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, name))
+    n, m, _ = A.info()
+    x = rb.ParVector(m, values=np.arange(m, dtype=np.float64))
+    b = rb.ParVector(n)
+    A.mult(x, b)
+    np.testing.assert_allclose(b.numpy(), golden[name + "_inc_b"], rtol=1e-12, atol=1e-9)
+    xt = rb.ParVector(n, values=np.arange(n, dtype=np.float64))
+    bt = rb.ParVector(m)
+    A.mult_T(xt, bt)
+    np.testing.assert_allclose(bt.numpy(), golden[name + "_inc_b_T"], rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("prob", ["aniso64", "lap27_24"])
+def test_spmv_family_vs_oracle(prob):
+    Ao = aniso(64) if prob == "aniso64" else lap27(24)
+    A = to_rb(Ao)
+    n = Ao.shape[0]
+    rng = np.random.default_rng(7)
+    xh = rng.uniform(-1, 1, n)
+    bh = rng.uniform(-1, 1, n)
+    x = rb.ParVector(n, values=xh)
+    b = rb.ParVector(n, values=bh)
+    y = rb.ParVector(n)
+    A.mult(x, y)
+    np.testing.assert_allclose(y.numpy(), O.spmv(Ao, xh), rtol=1e-12, atol=1e-13)
+    r = rb.ParVector(n)
+    A.residual(x, b, r)
+    np.testing.assert_allclose(r.numpy(), O.residual(Ao, xh, bh), rtol=1e-12, atol=1e-13)
+    A.mult_T(x, y)
+    np.testing.assert_allclose(y.numpy(), O.spmv_T(Ao, xh), rtol=1e-12, atol=1e-13)
+    y.set_values(bh)
+    A.mult_append(x, y)
+    np.testing.assert_allclose(y.numpy(), bh + O.spmv(Ao, xh), rtol=1e-12, atol=1e-13)
+    # vector ops (par_vector.cpp:88-121)
+    assert abs(x.inner_product(b) - float(xh @ bh)) <= 1e-12 * n
+    assert abs(x.norm(2) - float(np.linalg.norm(xh))) <= 1e-12 * math.sqrt(n)
+
+
+def test_dot_is_deterministic():
+    n = 1 << 20
+    v = rb.ParVector(n, values=np.random.default_rng(1).standard_normal(n))
+    d = [v.inner_product(v) for _ in range(5)]
+    assert len(set(d)) == 1
+
+
+# ----------------------------------------------------------------- setup --
+@pytest.mark.parametrize("prob", ["aniso64", "lap27_16", "aniso7_14"])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_strength_bit_exact(prob, kind):
+    Ao = {"aniso64": aniso(64), "lap27_16": lap27(16), "aniso7_14": aniso7(14)}[prob]
+    Ao = O.sort_diag_first(Ao)
+    A = to_rb(Ao)
+    S = A.strength(kind, 0.25)
+    ref = O.classical_strength(Ao, 0.25) if kind == 0 else O.symmetric_strength(Ao, 0.25)
+    assert_csr_equal(rb_tuple(S), oc_tuple(ref), exact_order=True)
+
+
+@pytest.mark.parametrize("lvl", [0, 1])
+def test_pmis_golden(golden, lvl):
+    S = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, "rss_S%d" % lvl)).sort_diag_first()
+    st = rb.split_pmis(S, golden["weights"])
+    np.testing.assert_array_equal(st, golden["rss_cf%d_pmis" % lvl])
+
+
+@pytest.mark.parametrize("prob", ["aniso100", "lap27_20"])
+def test_pmis_vs_oracle(prob):
+    Ao = O.sort_diag_first(aniso(100) if prob == "aniso100" else lap27(20))
+    So = O.classical_strength(Ao, 0.25)
+    w = O.rand_weights(Ao.shape[0])
+    S = to_rb(So)
+    np.testing.assert_array_equal(rb.split_pmis(S, w), O.split_pmis(So, w))
+
+
+@pytest.mark.parametrize("prob", ["aniso", "laplacian"])
+@pytest.mark.parametrize("kind,fix", [(1, "P_mod_class"), (2, "P_extend")])
+def test_interpolation_golden(golden, prob, kind, fix):
+    A = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, prob)).sort_diag_first()
+    S = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, prob + "_S")).sort_diag_first()
+    P = rb.interpolation(A, S, golden[prob + "_split"], kind, 0.0)
+    ref = canon(golden_csr(golden, prob + "_" + fix))
+    got = canon(rb_tuple(P))
+    np.testing.assert_array_equal(got[2], ref[2])
+    np.testing.assert_array_equal(got[3], ref[3])
+    np.testing.assert_allclose(got[4], ref[4], atol=1e-6)
+
+
+@pytest.mark.parametrize("prob", ["aniso100", "lap27_16"])
+@pytest.mark.parametrize("kind,filt", [(1, 0.0), (2, 0.0), (2, 0.3)])
+def test_interpolation_bit_exact(prob, kind, filt):
+    Ao = O.sort_diag_first(aniso(100) if prob == "aniso100" else lap27(16))
+    So = O.classical_strength(Ao, 0.25)
+    st = O.split_pmis(So, O.rand_weights(Ao.shape[0]))
+    ref = O.interpolation(Ao, So, st, "extended" if kind == 2 else "mod_classical", filt)
+    P = rb.interpolation(to_rb(Ao), to_rb(So), st, kind, filt)
+    assert_csr_equal(rb_tuple(P), oc_tuple(ref))
+
+
+@pytest.mark.parametrize("lvl", [0, 1])
+def test_rap_golden(golden, lvl):
+    A = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, "rss_A%d" % lvl))
+    P = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, "rss_P%d" % lvl))
+    Ac = rb.rap(A, P)
+    ref = canon(golden_csr(golden, "rss_A%d" % (lvl + 1)))
+    got = canon(rb_tuple(Ac))
+    np.testing.assert_array_equal(got[2], ref[2])
+    np.testing.assert_array_equal(got[3], ref[3])
+    np.testing.assert_allclose(got[4], ref[4], atol=1e-6)
+
+
+@pytest.mark.parametrize("prob", ["aniso100", "lap27_16"])
+def test_rap_bit_exact(prob):
+    Ao = O.sort_diag_first(aniso(100) if prob == "aniso100" else lap27(16))
+    So = O.classical_strength(Ao, 0.25)
+    st = O.split_pmis(So, O.rand_weights(Ao.shape[0]))
+    Po = O.interpolation(Ao, So, st, "extended", 0.3)
+    ref = O.rap(Ao, Po)
+    got = rb.rap(to_rb(Ao), to_rb(Po))
+    assert_csr_equal(rb_tuple(got), oc_tuple(ref), exact_order=True)
+
+
+# -------------------------------------------------------------- hierarchy --
+def hierarchy_pair(Ao, interp, relax, **kw):
+    A = to_rb(Ao)
+    ml = rb.ParRugeStubenSolver(0.25, rb.PMIS, {"mod_classical": rb.ModClassical,
+                                                "extended": rb.Extended}[interp], rb.Classical,
+                                {"jacobi": rb.Jacobi, "l1_jacobi": rb.L1Jacobi,
+                                 "sor": rb.SOR, "ssor": rb.SSOR}[relax])
+    for k, v in kw.items():
+        setattr(ml, k, v)
+    ml.setup(A)
+    om = O.Hierarchy(Ao, interp=interp, relax={"sor": "mc_sor", "ssor": "mc_ssor"}.get(relax, relax),
+                     **{k: v for k, v in kw.items() if k in ("relax_weight", "jacobi_compat", "solve_tol",
+                                                            "num_smooth_sweeps", "max_coarse")})
+    return A, ml, om
+
+
+@pytest.mark.parametrize("prob,interp", [("aniso100", "mod_classical"), ("aniso100", "extended"),
+                                         ("lap27_20", "extended"), ("lap27_20", "mod_classical")])
+def test_hierarchy_bit_exact(prob, interp):
+    Ao = aniso(100) if prob == "aniso100" else lap27(20)
+    A, ml, om = hierarchy_pair(Ao, interp, "jacobi")
+    assert ml.num_levels == om.num_levels
+    for l in range(ml.num_levels):
+        assert_csr_equal(rb_tuple(ml.level_matrix(l, "A")), oc_tuple(om.A(l)), exact_order=True)
+        if l < ml.num_levels - 1:
+            assert_csr_equal(rb_tuple(ml.level_matrix(l, "P")), oc_tuple(om.P(l)))
+
+
+@pytest.mark.parametrize("compat", [1, 0])
+def test_solve_history_jacobi(compat):
+    # 100^2 aniso, RS/PMIS/ModClassical, Jacobi w=2/3, solve to 1e-8
+    Ao = aniso(100)
+    A, ml, om = hierarchy_pair(Ao, "mod_classical", "jacobi", relax_weight=2.0 / 3.0,
+                               jacobi_compat=compat, solve_tol=1e-8)
+    n = Ao.shape[0]
+    bh = O.spmv(Ao, np.ones(n))
+    x = rb.ParVector(n)
+    b = rb.ParVector(n, values=bh)
+    it = ml.solve(x, b)
+    xo, ito, ho = om.solve(np.zeros(n), bh)
+    assert it == ito
+    np.testing.assert_allclose(ml.get_residuals(), ho, rtol=1e-10)
+    np.testing.assert_allclose(x.numpy(), xo, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("prob,interp,relax", [("aniso100", "mod_classical", "jacobi"),
+                                               ("lap27_20", "extended", "l1_jacobi"),
+                                               ("lap27_20", "extended", "jacobi")])
+def test_pcg_reference_history(prob, interp, relax):
+    Ao = aniso(100) if prob == "aniso100" else lap27(20)
+    kw = {"relax_weight": 2.0 / 3.0} if relax == "jacobi" else {}
+    A, ml, om = hierarchy_pair(Ao, interp, relax, **kw)
+    n = Ao.shape[0]
+    bh = O.spmv(Ao, np.ones(n))
+    x = rb.ParVector(n)
+    b = rb.ParVector(n, values=bh)
+    res = []
+    rb.PCG(A, ml, x, b, res, tol=1e-8)
+    xo, ho, _ = O.pcg(Ao, om, np.zeros(n), bh, tol=1e-8)
+    assert len(res) == len(ho)
+    np.testing.assert_allclose(res, ho, rtol=1e-10)
+    np.testing.assert_allclose(x.numpy(), xo, rtol=1e-9, atol=1e-12)
+
+
+def test_cg_and_bicgstab_golden(golden):
+    A = rb.par_stencil_grid(rb.diffusion_stencil_2d(*AN), [50, 50])
+    n = A.global_num_rows
+    x = rb.ParVector(n)
+    b = rb.ParVector(n)
+    x.set_const_value(1.0)
+    A.mult(x, b)
+    bnorm = b.norm(2)
+    x.set_const_value(0.0)
+    res = []
+    rb.CG(A, x, b, res)
+    ref = golden["cg_res"]
+    m = min(len(res), len(ref))
+    np.testing.assert_allclose(np.array(res[:m]) * bnorm, ref[:m], atol=1e-6)
+    x.set_const_value(0.0)
+    res = []
+    rb.BiCGStab(A, x, b, res)
+    np.testing.assert_allclose(res[:25], golden["bicgstab_res"][:25], rtol=1e-6)
+
+
+def test_pre_bicgstab_vs_oracle():
+    Ao = aniso(64)
+    A, ml, om = hierarchy_pair(Ao, "mod_classical", "jacobi", relax_weight=2.0 / 3.0)
+    n = Ao.shape[0]
+    bh = O.spmv(Ao, np.ones(n))
+    x = rb.ParVector(n)
+    b = rb.ParVector(n, values=bh)
+    res = []
+    rb.Pre_BiCGStab(A, x, b, ml, res, tol=1e-8)
+    _, ho = O.bicgstab(Ao, np.zeros(n), bh, tol=1e-8, ml=om)
+    m = min(len(res), len(ho), 8)
+    np.testing.assert_allclose(res[:m], ho[:m], rtol=1e-8)
+    assert np.linalg.norm(O.residual(Ao, x.numpy(), bh)) <= 1e-7 * np.linalg.norm(bh)
