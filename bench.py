@@ -1,0 +1,441 @@
+"""Benchmark: AMG-preconditioned CG to 1e-8 relative residual on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--size 192] [--impl b200|reference]
+
+A step is one complete AMG-PCG solve (x0 = 0, stop at ||b - A x|| / ||b|| <
+1e-8) of the 3D 27-point Laplacian (laplace_stencil_27pt through
+par_stencil_grid) on a size^3 grid with b uniform in [-1, 1] from a fixed
+seed; Ruge-Stuben AMG with classical strength 0.25, PMIS, extended+i
+interpolation (filter 0.3) and L1-Jacobi.  The hierarchy and V-cycle run in
+FP32, the outer CG (residual, dots, A p) and the coarse LU in FP64.  The same
+solve with an all-FP64 hierarchy is timed too (`fp64_form`), giving the
+FP32/FP64 speed-up at the same verified accuracy.
+
+Inputs stay resident in HBM during the device-timed steps (the FP64 matrix
+alone is larger than L2, so no flush is needed); `e2e` times the public API
+with host buffers: pinned b uploaded and x downloaded every step.
+
+Under torchrun each rank solves its own copy (replicas; the solve does not
+shard), timings are the max over ranks.  `--impl reference` times the CPU
+restatement of the reference's algorithm (the reference's own AMG path needs
+MPI and cannot be built here) on a bounded sample on rank 0.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 20261203
+METRIC = "AMG-PCG time to 1e-8 rel-res"
+TOL = 1e-8
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--size", type=int, default=192)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--cpu-sample", type=int, default=96)
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    def __init__(self, world, local):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+            torch.cuda.set_device(local)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.td = td
+            self.torch = torch
+
+    def barrier(self):
+        if self.world > 1:
+            self.td.barrier()
+
+    def max(self, v):
+        if self.world == 1:
+            return v
+        t = self.torch.tensor([float(v)], device="cuda")
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.td.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:  # noqa: BLE001
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:  # noqa: BLE001
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ b200 ----
+def a_bytes(ml, l, vbytes):
+    """Bytes of one pass over A_l in its stored format: CSR z(v+4) + (n+1)4,
+    or the sliced diagonals nd * 32 ceil(n/32) v (no indices)."""
+    n, z, _ = ml.level_info(l)
+    nd = ml.level_storage(l)
+    if nd:
+        return nd * 32 * ((n + 31) // 32) * vbytes
+    return z * (vbytes + 4) + (n + 1) * 4
+
+
+def cycle_bytes(ml, vbytes):
+    """Algorithmic bytes of one V-cycle (1 pre- and 1 post-sweep, zero guess).
+
+    Per level l with n rows, p = nnz(P_l), v = value bytes, i = 4: B_A = one
+    pass over A_l in its stored format (a_bytes), B_P = B_R = p(v+i) +
+    (rows+1)i.  Pre-smooth from a zero guess reads b and the inverse diagonal
+    and writes x (3nv); residual B_A + 3nv; restriction B_R + n v + n_c v;
+    prolongation B_P + (2n + n_c) v; post-smooth B_A + 4nv (x, b, D^-1 in, x
+    out).  Coarsest level: the dense LU (2 n_c^2 8 bytes)."""
+    L = ml.num_levels
+    tot = 0.0
+    per = []
+    for l in range(L):
+        n, z, p = ml.level_info(l)
+        if l == L - 1:
+            b = 2.0 * n * n * 8
+        else:
+            nc = ml.level_info(l + 1)[0]
+            BA = a_bytes(ml, l, vbytes)
+            BP = p * (vbytes + 4) + (n + 1) * 4
+            BR = p * (vbytes + 4) + (nc + 1) * 4
+            b = (3 * n * vbytes) + (BA + 3 * n * vbytes) + (BR + n * vbytes + nc * vbytes) + \
+                (BP + (2 * n + nc) * vbytes) + (BA + 4 * n * vbytes)
+        per.append(b)
+        tot += b
+    return tot, per
+
+
+def run_b200(args, rank, world, local):
+    import raptor_b200 as rb
+
+    dist = Dist(world, local)
+    rb.init(local)
+    S = args.size
+    A = rb.par_stencil_grid(rb.laplace_stencil_27pt(), [S, S, S])
+    n = A.global_num_rows
+    nnz = A.local_nnz
+    bh = np.random.default_rng(SEED).uniform(-1.0, 1.0, n)
+    b = rb.ParVector(n, values=bh)
+    x = rb.ParVector(n)
+    bnorm = float(np.linalg.norm(bh))
+
+    def make(prec):
+        ml = rb.ParRugeStubenSolver(0.25, rb.PMIS, rb.Extended, rb.Classical, rb.L1Jacobi)
+        ml.precision = prec
+        ml.setup(A)
+        return ml
+
+    def solve(ml):
+        x.set_const_value(0.0)
+        res = []
+        rc = rb.PCG(A, ml, x, b, res, tol=TOL, max_iter=500, mode=rb.PCG_TRUE_RESIDUAL)
+        return rc, len(res) - 1
+
+    def timed(ml, steps, warmup):
+        for _ in range(warmup):
+            solve(ml)
+        rb.lib().rb_synchronize()
+        dist.barrier()
+        c0 = rb.launch_count()
+        t0 = time.perf_counter()
+        iters = []
+        for _ in range(steps):
+            rc, it = solve(ml)
+            iters.append(it)
+        rb.lib().rb_synchronize()
+        el = time.perf_counter() - t0
+        launches = rb.launch_count() - c0
+        dist.barrier()
+        return dist.max(el) / steps, iters, launches
+
+    def true_relres():
+        r = rb.ParVector(n)
+        A.residual(x, b, r)
+        return r.norm(2) / bnorm
+
+    ml32 = make(rb.FP32)
+    setup32 = ml32.setup_seconds
+    clocks = ClockSampler(local)
+    clocks.start()
+    t32, iters32, launches = timed(ml32, args.steps, args.warmup)
+    clk = clocks.stop()
+    rel32 = true_relres()
+    xs32 = x.numpy()
+
+    # per-level cycle profile and the dominant kernel
+    prof = ml32.cycle_profile()
+    cyc_ms = float(prof.sum())
+    cbytes, _ = cycle_bytes(ml32, 4)
+    # dominant kernel: the finest-level row kernel of the cycle (the
+    # post-smoothing sweep; the residual is the same kernel with one vector less)
+    op_ms = {}
+    for op, name in ((0, "residual_A0_fp32"), (3, "jacobi_A0_fp32"), (4, "spmv_dot_A0_fp64"),
+                     (1, "restrict_R0_fp32"), (2, "prolong_P0_fp32")):
+        op_ms[name] = ml32.time_operator(0, op, reps=20)
+    n0, z0, p0 = ml32.level_info(0)
+    n1 = ml32.level_info(1)[0]
+    BA0 = a_bytes(ml32, 0, 4)
+    alg = {
+        "residual_A0_fp32": BA0 + 3 * n0 * 4,
+        "jacobi_A0_fp32": BA0 + 4 * n0 * 4,
+        "spmv_dot_A0_fp64": BA0 + 2 * n0 * 8,
+        "restrict_R0_fp32": p0 * 8 + (n1 + 1) * 4 + n0 * 4 + n1 * 4,
+        "prolong_P0_fp32": p0 * 8 + (n0 + 1) * 4 + (2 * n0 + n1) * 4,
+    }
+    peak, peak_kind = peaks()
+    dom = "jacobi_A0_fp32"
+    achieved = alg[dom] / (op_ms[dom] * 1e-3) / 1e9
+
+    # FP64 form
+    fp64 = None
+    if not args.no_fp64:
+        ml64 = make(rb.FP64)
+        t64, iters64, _ = timed(ml64, max(2, args.steps // 2), 2)
+        rel64 = true_relres()
+        xs64 = x.numpy()
+        fp64 = {"seconds": t64, "iters": iters64[-1], "final_rel_res": rel64,
+                "setup_s": ml64.setup_seconds,
+                "speedup_fp32_over_fp64": t64 / t32,
+                "x_rel_diff_fp32_vs_fp64": float(np.linalg.norm(xs32 - xs64) / np.linalg.norm(xs64))}
+        ml = ml64
+    else:
+        ml = ml32
+
+    # end to end through the public API with host buffers
+    import ctypes as C
+    try:
+        import torch
+        hb = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        hx = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        hb.numpy()[:] = bh
+        hbp, hxp = hb.data_ptr(), hx.data_ptr()
+        pinned = True
+    except Exception:  # noqa: BLE001
+        hbn = np.ascontiguousarray(bh)
+        hxn = np.empty(n)
+        hbp, hxp = hbn.ctypes.data, hxn.ctypes.data
+        pinned = False
+    L = rb.lib()
+    Dp = C.POINTER(C.c_double)
+    ml_e2e = ml32
+    e2e_t = []
+    for s in range(args.warmup + args.steps):
+        dist.barrier()
+        t0 = time.perf_counter()
+        L.rb_vec_upload.argtypes = [C.c_void_p, C.c_void_p]
+        L.rb_vec_download.argtypes = [C.c_void_p, C.c_void_p]
+        assert L.rb_vec_upload(b.h, C.c_void_p(hbp)) == 0
+        x.set_const_value(0.0)
+        res = []
+        rb.PCG(A, ml_e2e, x, b, res, tol=TOL, max_iter=500, mode=rb.PCG_TRUE_RESIDUAL)
+        assert L.rb_vec_download(x.h, C.c_void_p(hxp)) == 0
+        el = time.perf_counter() - t0
+        if s >= args.warmup:
+            e2e_t.append(dist.max(el))
+    # restore numpy-typed signatures
+    from raptor_b200 import _capi
+    L.rb_vec_upload.argtypes = _capi.SIGNATURES["rb_vec_upload"][1]
+    L.rb_vec_download.argtypes = _capi.SIGNATURES["rb_vec_download"][1]
+    e2e = sum(e2e_t) / len(e2e_t)
+
+    out = {
+        "metric": METRIC, "value": t32, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t32 * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32-vcycle/fp64-outer",
+        "data": "synthetic (27-point Laplacian stencil, b ~ U[-1,1] seed %d)" % SEED,
+        "config": {
+            "workload": "laplacian27 %d^3 AMG-PCG to 1e-8 (RS PMIS, extended+i, L1-Jacobi)" % S,
+            "rows": n, "nnz": nnz, "levels": None,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (A0 FP64 = %.2f GB)" % (nnz * 12 / 1e9),
+        },
+        "iters": iters32[-1], "final_rel_res": rel32, "setup_s": setup32,
+        "vcycle": {"ms": cyc_ms, "alg_bytes": cbytes, "gbs": cbytes / (cyc_ms * 1e-3) / 1e9,
+                   "frac_of_%s_peak" % peak_kind: cbytes / (cyc_ms * 1e-3) / 1e9 / peak},
+        "fp64_form": fp64,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic_for(dom),
+                     "peak_source": peak_kind, "ops_ms": op_ms, "alg_bytes": alg,
+                     "a0_storage": ("sliced-diagonals nd=%d" % ml32.level_storage(0))
+                     if ml32.level_storage(0) else "csr"},
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": n * 8,
+                "d2h_bytes_per_step": n * 8, "pinned": pinned},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    out["config"]["levels"] = ml.num_levels
+    if rank == 0 and args.cpu_sample > 0:
+        out["cpu_baseline"] = cpu_baseline(args.cpu_sample, S, iters32[-1])
+    dist.close()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def traffic_for(kernel):
+    """DRAM bytes per launch from the committed ncu summary, when present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(kernel)
+    except Exception:  # noqa: BLE001
+        return None
+
+
+# ------------------------------------------------------------- CPU legs ----
+class CpuSample:
+    """The oracle's AMG-PCG with the same options on an m^3 grid, stopped on
+    the same true relative residual (1 core, FP64); setup is not timed."""
+
+    def __init__(self, m):
+        from oracle import oracle as O
+        self.O = O
+        self.A = O.stencil_grid(O.laplace_stencil_27pt(), [m, m, m])
+        self.n = self.A.shape[0]
+        self.b = np.random.default_rng(SEED).uniform(-1.0, 1.0, self.n)
+        self.ml = O.Hierarchy(self.A, interp="extended", relax="l1_jacobi")
+
+    def solve(self):
+        t0 = time.perf_counter()
+        _, hist, _ = self.O.pcg(self.A, self.ml, np.zeros(self.n), self.b, tol=TOL, max_iter=500,
+                                mode=1)
+        return time.perf_counter() - t0, len(hist) - 1
+
+
+def cpu_sample_solve(m):
+    cs = CpuSample(m)
+    el, it = cs.solve()
+    return el, it, cs.n
+
+
+def cpu_baseline(m, S, iters_full):
+    el, it, n = cpu_sample_solve(m)
+    scale = (S ** 3) / n
+    return {"value": el * scale, "unit": "s", "cores": 1, "kind": "port",
+            "sample": "oracle AMG-PCG solve phase on %d^3 (%d rows, %d iterations, %.2f s on 1 "
+                      "core), scaled by rows to %d^3" % (m, n, it, el, S)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    S = args.size
+    m = args.cpu_sample
+    cs = CpuSample(m)
+    n = cs.n
+    times = []
+    for s in range(args.warmup + args.steps):
+        el, it = cs.solve()
+        if s >= args.warmup:
+            times.append(el * (S ** 3) / n)
+    v = sum(times) / len(times)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp64", "data": "synthetic (27-point Laplacian, b ~ U[-1,1] seed %d)" % SEED,
+        "config": {"workload": "laplacian27 %d^3 AMG-PCG to 1e-8 (RS PMIS, extended+i, "
+                               "L1-Jacobi)" % S, "parallelism": "single"},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "port",
+                         "sample": "CPU restatement of the reference algorithm (the reference "
+                                   "needs MPI), solve phase on %d^3 per step, scaled by rows to "
+                                   "%d^3" % (m, S)},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_b200(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

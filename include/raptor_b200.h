@@ -152,6 +152,8 @@ typedef struct rb_amg_opts {
     int precision;            /* RB_PREC_FP64 / RB_PREC_FP32 */
     int jacobi_compat;        /* 1: Jacobi leaves x unchanged, as par_relax.cpp:127,146 does */
     int seed_offset;          /* first_local_row in srand(2448422 + first_local_row) */
+    int fuse_coarse;          /* 1: levels below 1e5 rows run as one persistent launch (default 0) */
+    int use_graphs;           /* 1: replay cycles / Krylov iterations from CUDA graphs */
 } rb_amg_opts;
 
 void rb_amg_default_opts(rb_amg_opts* opts);
@@ -173,11 +175,35 @@ int rb_amg_cycle(rb_amg ml, rb_vec x, rb_vec b);
  * ||r_k||/||b|| for k = 0..iters (up to cap entries). */
 int rb_amg_solve(rb_amg ml, rb_vec x, rb_vec b, int* iters, double* hist, int cap);
 
+/* Time one V-cycle operation by operation (track_times / print_solve_times,
+ * par_multilevel.hpp:343-456, 578-619).  ms receives 8 values per level:
+ * [pre-smooth, residual, restriction, prolongation, post-smooth, coarse
+ * solve, 0, 0] in milliseconds; n_out = 8 * num_levels. */
+int rb_amg_cycle_profile(rb_amg ml, double* ms, int cap, int* n_out);
+/* Average milliseconds per launch of one cycle operator over reps launches:
+ * op 0 residual with A_l, 1 restriction with R_l, 2 prolongation with P_l,
+ * 3 Jacobi sweep with A_l (all in the cycle precision), 4 the outer FP64
+ * A p fused with p.Ap on the finest level. */
+int rb_amg_time_operator(rb_amg ml, int level, int op, int reps, double* ms_per_launch);
+/* Wall time of the last rb_amg_setup (seconds) and the autotuner's choices
+ * for level l: lanes per row of A_l (0 when A_l is stored by diagonals),
+ * P_l and R_l. */
+int rb_amg_setup_seconds(rb_amg ml, double* seconds);
+int rb_amg_level_lanes(rb_amg ml, int level, int* lanes_A, int* lanes_P, int* lanes_R);
+/* Storage of A_l in the cycle: *ndiag = number of stored diagonals when the
+ * autotuner picked the sliced-diagonal layout, 0 for CSR. */
+int rb_amg_level_storage(rb_amg ml, int level, int* ndiag);
+/* Kernels this library has launched so far (graph replays count their
+ * kernel nodes). */
+int rb_launch_count(int64_t* count);
+
 /* ------------------------------------------------------------------ Krylov */
 #define RB_PCG_REFERENCE 0 /* par_cg.cpp:121-263 exactly: stop on r.z < tol*sqrt(b.Mb) */
 #define RB_PCG_TRUE_RESIDUAL 1 /* stop on ||b - A x|| / ||b|| < tol */
 
-/* PCG (krylov/par_cg.cpp:121-263).  hist receives the reference's history
+/* PCG (krylov/par_cg.cpp:121-263).  When A is the matrix ml was set up with,
+ * A p reads the hierarchy's copies of it (changing A's values after setup
+ * needs a new setup).  hist receives the reference's history
  * (sqrt(r.z) then r.z/b.Mb) in RB_PCG_REFERENCE mode, ||r||/||b|| otherwise;
  * n_hist receives the entry count. */
 int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, int mode,

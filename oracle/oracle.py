@@ -96,6 +96,8 @@ def lib():
         L.oc_ml_solve.argtypes = [_P, _D, _D, _D, C.c_int]
         L.oc_pcg.restype = C.c_int
         L.oc_pcg.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+        L.oc_pcg_mode.restype = C.c_int
+        L.oc_pcg_mode.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, C.c_int, _D, C.c_int]
         L.oc_cg.restype = C.c_int
         L.oc_cg.argtypes = [_P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
         L.oc_bicgstab.restype = C.c_int
@@ -325,11 +327,14 @@ class Hierarchy:
         return x, it, hist[: min(it + 1, cap)]
 
 
-def pcg(A, ml, x, b, tol=1e-5, max_iter=-1, cap=10000):
+def pcg(A, ml, x, b, tol=1e-5, max_iter=-1, cap=10000, mode=0):
+    """mode 0: the reference's PCG; mode 1: stop on the true relative residual."""
     x = np.ascontiguousarray(x, np.float64).copy()
     hist = np.zeros(cap)
-    nh = lib().oc_pcg(A.ptr, ml.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter,
-                      hist, cap)
+    if max_iter <= 0:
+        max_iter = int(1.3 * A.shape[0]) + 2
+    nh = lib().oc_pcg_mode(A.ptr, ml.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter,
+                           mode, hist, cap)
     return x, hist[: min(abs(nh), cap)], nh
 
 

@@ -1339,8 +1339,20 @@ int oc_ml_solve(oc_ml* ml, double* x, const double* b, double* hist, int cap) {
 /* PCG, krylov/par_cg.cpp:121-263.  Returns the number of history entries
  * (res[0] = sqrt(r.z), then r.z / b.Mb per iteration); stops on
  * next_inner < tol*sqrt(b.Mb); restarts every 8 iterations. */
+int oc_pcg_mode(const oc_csr* A, oc_ml* ml, double* x, const double* b, double tol,
+                int max_iter, int mode, double* hist, int cap);
+
 int oc_pcg(const oc_csr* A, oc_ml* ml, double* x, const double* b, double tol, int max_iter,
            double* hist, int cap) {
+    return oc_pcg_mode(A, ml, x, b, tol, max_iter, 0, hist, cap);
+}
+
+/* mode 0: the reference's iteration exactly.  mode 1 (not in the reference):
+ * the same recurrence stopped when ||r|| <= tol ||b|| with the true residual
+ * confirmed at exit, residual replacement every 10 iterations and no p
+ * restart; history entries ||r||/||b||. */
+int oc_pcg_mode(const oc_csr* A, oc_ml* ml, double* x, const double* b, double tol,
+                int max_iter, int mode, double* hist, int cap) {
     int n = A->n_rows;
     if (max_iter <= 0) max_iter = (int)(1.3 * n) + 2;
     double* r = (double*)calloc((size_t)n + 1, sizeof(double));
@@ -1348,6 +1360,44 @@ int oc_pcg(const oc_csr* A, oc_ml* ml, double* x, const double* b, double tol, i
     double* p = (double*)calloc((size_t)n + 1, sizeof(double));
     double* Ap = (double*)calloc((size_t)n + 1, sizeof(double));
     int nh = 0;
+    if (mode == 1) {
+        double bn = sqrt(vdot(b, b, n));
+        if (bn == 0.0) bn = 1.0;
+        oc_residual(A, x, b, r);
+        memset(z, 0, sizeof(double) * n);
+        cycle(ml, z, r, 0);
+        memcpy(p, z, sizeof(double) * n);
+        double rz = vdot(r, z, n);
+        double rn = sqrt(vdot(r, r, n));
+        if (nh < cap) hist[nh] = rn / bn;
+        nh++;
+        int it = 0;
+        while (rn > tol * bn && it < max_iter) {
+            it++;
+            oc_spmv(A, p, Ap);
+            double pAp = vdot(Ap, p, n);
+            double alpha = rz / pAp;
+            vaxpy(x, p, alpha, n);
+            if (it % 10 == 0) oc_residual(A, x, b, r);
+            else vaxpy(r, Ap, -alpha, n);
+            rn = sqrt(vdot(r, r, n));
+            if (rn <= tol * bn) {
+                oc_residual(A, x, b, r);
+                rn = sqrt(vdot(r, r, n));
+            }
+            if (nh < cap) hist[nh] = rn / bn;
+            nh++;
+            if (rn <= tol * bn) break;
+            memset(z, 0, sizeof(double) * n);
+            cycle(ml, z, r, 0);
+            double next = vdot(r, z, n);
+            double beta = next / rz;
+            for (int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+            rz = next;
+        }
+        free(r); free(z); free(p); free(Ap);
+        return nh;
+    }
     memset(z, 0, sizeof(double) * n);
     cycle(ml, z, b, 0);
     double b_inner = vdot(b, z, n);

@@ -150,6 +150,8 @@ void oc_ml_cycle(oc_ml* ml, double* x, const double* b);
 int oc_ml_solve(oc_ml* ml, double* x, const double* b, double* hist, int cap);
 int oc_pcg(const oc_csr* A, oc_ml* ml, double* x, const double* b, double tol,
            int max_iter, double* hist, int cap);
+int oc_pcg_mode(const oc_csr* A, oc_ml* ml, double* x, const double* b, double tol,
+                int max_iter, int mode, double* hist, int cap);
 int oc_cg(const oc_csr* A, double* x, const double* b, double tol, int max_iter,
           double* hist, int cap);
 int oc_bicgstab(const oc_csr* A, double* x, const double* b, double tol,

@@ -262,6 +262,9 @@ class ParMultilevel:
 
     _FIELDS = ("strong_threshold", "relax_weight", "num_smooth_sweeps", "max_coarse",
                "max_levels", "max_iterations", "solve_tol", "interp_filter")
+    _EXTRA = ("precision", "jacobi_compat", "seed_offset", "relax_type", "strength_type",
+              "interp_type", "fuse_coarse", "use_graphs", "prolong_weight",
+              "prolong_smooth_steps", "solver")
 
     def __init__(self, strong_threshold=0.0, strength_type=Classical, relax_type=SOR):
         self.opts = AmgOpts()
@@ -275,14 +278,12 @@ class ParMultilevel:
         self.store_residuals = True
 
     def __getattr__(self, name):
-        if name in ParMultilevel._FIELDS or name in ("precision", "jacobi_compat", "seed_offset",
-                                                     "relax_type", "strength_type", "interp_type"):
+        if name in ParMultilevel._FIELDS or name in ParMultilevel._EXTRA:
             return getattr(self.__dict__["opts"], name)
         raise AttributeError(name)
 
     def __setattr__(self, name, value):
-        if name in ParMultilevel._FIELDS or name in ("precision", "jacobi_compat", "seed_offset",
-                                                     "relax_type", "strength_type", "interp_type"):
+        if name in ParMultilevel._FIELDS or name in ParMultilevel._EXTRA:
             setattr(self.opts, name, value)
         else:
             object.__setattr__(self, name, value)
@@ -345,6 +346,36 @@ class ParMultilevel:
 
     def get_residuals(self):
         return self.residuals
+
+    def cycle_profile(self):
+        """Milliseconds per level: rows [pre, residual, restrict, prolong, post, coarse]."""
+        L = self.num_levels
+        ms = np.zeros(8 * L)
+        n = C.c_int()
+        check(lib().rb_amg_cycle_profile(self.h, _ptr(ms), 8 * L, C.byref(n)))
+        return ms.reshape(L, 8)[:, :6]
+
+    def time_operator(self, level, op, reps=20):
+        out = C.c_double()
+        check(lib().rb_amg_time_operator(self.h, int(level), int(op), int(reps), C.byref(out)))
+        return out.value
+
+    @property
+    def setup_seconds(self):
+        out = C.c_double()
+        check(lib().rb_amg_setup_seconds(self.h, C.byref(out)))
+        return out.value
+
+    def level_lanes(self, l):
+        a, p, r = C.c_int(), C.c_int(), C.c_int()
+        check(lib().rb_amg_level_lanes(self.h, l, C.byref(a), C.byref(p), C.byref(r)))
+        return a.value, p.value, r.value
+
+    def level_storage(self, l):
+        """Number of stored diagonals of A_l (sliced layout), 0 for CSR."""
+        nd = C.c_int()
+        check(lib().rb_amg_level_storage(self.h, l, C.byref(nd)))
+        return nd.value
 
     def print_hierarchy(self):
         print("Num Levels = %d" % self.num_levels)
@@ -420,6 +451,12 @@ def Pre_BiCGStab(A, x, b, ml, res, tol=1e-5, max_iter=-1):
     if rc not in (0, -5):
         check(rc)
     return rc
+
+
+def launch_count():
+    out = C.c_int64()
+    check(lib().rb_launch_count(C.byref(out)))
+    return out.value
 
 
 def init(device=0):

@@ -40,6 +40,7 @@ class AmgOpts(C.Structure):
         ("relax_weight", C.c_double), ("solve_tol", C.c_double), ("interp_filter", C.c_double),
         ("prolong_weight", C.c_double), ("prolong_smooth_steps", C.c_int),
         ("precision", C.c_int), ("jacobi_compat", C.c_int), ("seed_offset", C.c_int),
+        ("fuse_coarse", C.c_int), ("use_graphs", C.c_int),
     ]
 
 
@@ -97,6 +98,12 @@ SIGNATURES = {
     "rb_amg_level_states": (C.c_int, [_P, C.c_int, _I]),
     "rb_amg_cycle": (C.c_int, [_P, _P, _P]),
     "rb_amg_solve": (C.c_int, [_P, _P, _P, C.POINTER(C.c_int), _P, C.c_int]),
+    "rb_amg_cycle_profile": (C.c_int, [_P, _P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_amg_time_operator": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "rb_amg_setup_seconds": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "rb_amg_level_lanes": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "rb_amg_level_storage": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rb_pcg": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
     "rb_cg": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
     "rb_bicgstab": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),

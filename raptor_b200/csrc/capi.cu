@@ -484,6 +484,8 @@ void rb_amg_default_opts(rb_amg_opts* o) {
     o->precision = RB_PREC_FP64;
     o->jacobi_compat = 0;
     o->seed_offset = 0;
+    o->fuse_coarse = 0;
+    o->use_graphs = 1;
 }
 
 int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_amg* out) {
@@ -586,6 +588,76 @@ int rb_amg_solve(rb_amg ml, rb_vec x, rb_vec b, int* iters, double* hist, int ca
         int rc = ml->h.solve(x->v.get(), b->v.get(), hist ? hist : h.data(), hist ? cap : 0, &it);
         if (iters) *iters = it;
         return rc;
+    });
+}
+
+int rb_amg_cycle_profile(rb_amg ml, double* ms, int cap, int* n_out) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(ms);
+        std::vector<double> v = ml->h.profile_cycle();
+        const int m = std::min<int>(cap, (int)v.size());
+        for (int i = 0; i < m; i++) ms[i] = v[i];
+        if (n_out) *n_out = (int)v.size();
+        return RB_OK;
+    });
+}
+
+int rb_amg_time_operator(rb_amg ml, int level, int op, int reps, double* ms_per_launch) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(ms_per_launch);
+        RB_REQUIRE(op >= 0 && op <= 4, "unknown operator");
+        *ms_per_launch = ml->h.time_operator(level, op, reps);
+        return RB_OK;
+    });
+}
+
+int rb_amg_setup_seconds(rb_amg ml, double* seconds) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(seconds);
+        *seconds = ml->h.setup_seconds;
+        return RB_OK;
+    });
+}
+
+int rb_amg_level_lanes(rb_amg ml, int level, int* lanes_A, int* lanes_P, int* lanes_R) {
+    return guarded([&]() -> int {
+        NEED(ml);
+        RB_REQUIRE(level >= 0 && level < ml->h.num_levels(), "level out of range");
+        int a = 0, p = 0, r = 0;
+        if (ml->h.opts.precision == RB_PREC_FP32) {
+            const auto& V = ml->h.lv32[level];
+            a = V.dia ? 0 : V.gA; p = V.gP; r = V.gR;
+        } else {
+            const auto& V = ml->h.lv64[level];
+            a = V.dia ? 0 : V.gA; p = V.gP; r = V.gR;
+        }
+        if (lanes_A) *lanes_A = a;
+        if (lanes_P) *lanes_P = p;
+        if (lanes_R) *lanes_R = r;
+        return RB_OK;
+    });
+}
+
+int rb_amg_level_storage(rb_amg ml, int level, int* ndiag) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(ndiag);
+        RB_REQUIRE(level >= 0 && level < ml->h.num_levels(), "level out of range");
+        if (ml->h.opts.precision == RB_PREC_FP32) {
+            const auto& V = ml->h.lv32[level];
+            *ndiag = V.dia ? V.off.nd : 0;
+        } else {
+            const auto& V = ml->h.lv64[level];
+            *ndiag = V.dia ? V.off.nd : 0;
+        }
+        return RB_OK;
+    });
+}
+
+int rb_launch_count(int64_t* count) {
+    return guarded([&]() -> int {
+        NEED(count);
+        *count = launch_counter();
+        return RB_OK;
     });
 }
 

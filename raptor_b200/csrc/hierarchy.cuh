@@ -8,6 +8,8 @@
 #include <vector>
 
 #include "blas1.cuh"
+#include "coarse_cycle.cuh"
+#include "dia.cuh"
 #include "rb_internal.cuh"
 
 namespace rb {
@@ -31,7 +33,17 @@ struct Level {
     std::vector<int> colour_ptr;
     DevArray<T> x, b, r, xt;
     int gA = 0, gP = 0, gR = 0;        // lanes per row picked by the autotuner
+    bool dia = false;                  // A_l by diagonals (the autotuner's pick)
+    DiaOff off{};
+    DevArray<T> Adia;
     void alloc_vectors();
+
+    // y-epilogue over the rows of A_l times x, in whichever format was picked
+    template <typename TX, class Epi>
+    void apply_A(const TX* xin, Epi epi) const {
+        if (dia) launch_dia(off, Adia.get(), n, xin, epi);
+        else launch_rows(A.rowptr, A.cols, A.vals, n, A.nnz, xin, epi, gA);
+    }
 };
 
 struct Hierarchy {
@@ -48,8 +60,26 @@ struct Hierarchy {
     KScal* host_scal = nullptr;
     int gA0 = 0;
     bool use_graphs = true;
+    // fused bottom of the cycle (levels fuse_from .. L-1 in one launch)
+    int fuse_from = -1;
+    int fuse_grid = 0;
+    DevArray<LevelDesc<double>> fdesc64;
+    DevArray<LevelDesc<float>> fdesc32;
+    DevArray<BarrierState> barrier;
+    int* host_barrier_error = nullptr;
+    template <typename T>
+    void build_fused(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc);
+    template <typename T>
+    void launch_fused(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc);
     std::map<std::string, cudaGraphExec_t> graphs;
     std::map<std::string, long long> graph_kernels;
+    // the matrix handed to setup: PCG on it reads the hierarchy's copies of
+    // A_0 (the same values, stored by diagonals / in the cycle precision)
+    const rb_csr_s* src_A = nullptr;
+    bool is_finest(const rb_csr_s& A) const {
+        return &A == master[0].A.get() ||
+               (&A == src_A && A.nnz == master[0].A->nnz && A.n_rows == master[0].A->n_rows);
+    }
     double setup_seconds = 0;
     int last_iters = 0;
 
@@ -73,7 +103,18 @@ struct Hierarchy {
     double norm64(const double* v, long n);
     KScal read_scal();
 
+    // profiling (multilevel/par_multilevel.hpp:343-456 keeps per-level
+    // solve_times; here CUDA events bracket each operation of one cycle)
+    std::vector<std::pair<int, cudaEvent_t>>* prof = nullptr;
+    void mark(int slot);
+    std::vector<double> profile_cycle();
+    double time_operator(int level, int op, int reps);
+
     int solve(double* x, const double* b, double* hist, int cap, int* iters);
+    // outer A p fused with p.Ap on the finest level: from the FP64 operator,
+    // or from the cycle-precision copy of A_0 with FP64 accumulation
+    template <class Fin>
+    void outer_apply(const rb_csr_s& A, bool lowprec, const double* p, double* Ap, Fin fin);
     int pcg(const rb_csr_s& A, double* x, const double* b, double tol, int max_iter, int mode,
             double* hist, int cap, int* n_hist);
     size_t device_bytes() const;

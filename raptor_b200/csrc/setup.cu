@@ -373,18 +373,11 @@ __global__ void k_ext_bound(int n, const int* __restrict__ srp, const int* __res
     ub[i] = b;
 }
 
-// Insertion-ordered unique pattern (par_interpolation.cpp:574-690).
-__global__ void k_ext_pattern(int n, const int* __restrict__ srp, const int* __restrict__ sci,
-                              const int* __restrict__ st, const int* __restrict__ uoff,
-                              int* list, int* cnt) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int o = uoff[i];
-    if (st[i] != kUnselected) {
-        if (st[i] == kSelected) { list[o] = i; cnt[i] = 1; }
-        else cnt[i] = 0;
-        return;
-    }
+// Insertion-ordered unique pattern (par_interpolation.cpp:574-690) of
+// the rows [r0, r0 + n), built in a scratch list to count it.
+__device__ __forceinline__ int ext_build_pattern(int i, const int* __restrict__ srp,
+                                                 const int* __restrict__ sci,
+                                                 const int* __restrict__ st, int* list, int o) {
     int m = o;
     for (int j = srp[i] + 1; j < srp[i + 1]; j++) {
         int c = sci[j];
@@ -397,7 +390,21 @@ __global__ void k_ext_pattern(int n, const int* __restrict__ srp, const int* __r
             }
         }
     }
-    cnt[i] = m - o;
+    return m - o;
+}
+
+__global__ void k_ext_pattern(int n, int r0, const int* __restrict__ srp,
+                              const int* __restrict__ sci, const int* __restrict__ st,
+                              const int* __restrict__ uoff, int* list, int* cnt) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = r0 + t;
+    const int o = uoff[t];
+    if (st[i] != kUnselected) {
+        cnt[i] = st[i] == kSelected ? 1 : 0;
+        return;
+    }
+    cnt[i] = ext_build_pattern(i, srp, sci, st, list, o);
 }
 
 // Values (par_interpolation.cpp:692-944) and filter_interp (:175-278).
@@ -406,14 +413,15 @@ __global__ void k_ext_pattern(int n, const int* __restrict__ srp, const int* __r
 __global__ void k_ext_fill(int n, const int* __restrict__ arp, const int* __restrict__ aci,
                            const double* __restrict__ acv, const int* __restrict__ srp,
                            const int* __restrict__ sci, const int* __restrict__ st,
-                           const int* __restrict__ uoff, const int* __restrict__ list,
                            const int* __restrict__ prp, int* pcols, double* pvals, double filter,
                            int* kept) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int p0 = prp[i], p1 = prp[i + 1];
-    const int o = uoff[i];
-    for (int t = p0; t < p1; t++) { pcols[t] = list[o + (t - p0)]; pvals[t] = 0.0; }
+    // rebuild the insertion-ordered pattern in place (its size is p1 - p0)
+    if (st[i] == kSelected) pcols[p0] = i;
+    else if (st[i] == kUnselected) ext_build_pattern(i, srp, sci, st, pcols, p0);
+    for (int t = p0; t < p1; t++) pvals[t] = 0.0;
     if (st[i] == kSelected) { pvals[p0] = 1.0; }
     if (st[i] == kUnselected) {
         int start = arp[i], end = arp[i + 1];
@@ -547,23 +555,46 @@ rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* st, int
         RB_CHECK_LAUNCH();
         return P;
     }
-    // Extended+i
-    DevArray<int> ub((size_t)n + 1), uoff((size_t)n + 1);
+    // Extended+i: count each row's pattern in chunks whose dedup scratch
+    // (bounded by the row bounds) fits an int32-indexed buffer
+    DevArray<int> ub((size_t)n + 1);
     if (n) k_ext_bound<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), st, ub.get());
     RB_CHECK_LAUNCH();
-    long long ubt = exclusive_scan(ub.get(), uoff.get(), n);
-    DevArray<int> list((size_t)std::max(ubt, 1LL));
-    if (n) k_ext_pattern<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), st, uoff.get(),
-                                                  list.get(), cnt.get());
-    RB_CHECK_LAUNCH();
+    std::vector<int> ubh((size_t)n);
+    ub.download(ubh.data(), n);
+    RB_CUDA(cudaStreamSynchronize(stream()));
+    const long long kChunk = 1LL << 28;   // 1 GiB of int scratch per chunk
+    long long maxchunk = 0;
+    {
+        long long acc = 0;
+        for (int i = 0; i < n; i++) {
+            if (acc + ubh[i] > kChunk && acc > 0) { maxchunk = std::max(maxchunk, acc); acc = 0; }
+            acc += ubh[i];
+        }
+        maxchunk = std::max(maxchunk, acc);
+    }
+    DevArray<int> list((size_t)std::max(maxchunk, 1LL)), uoff((size_t)n + 1);
+    for (int r0 = 0; r0 < n;) {
+        long long acc = 0;
+        int r1 = r0;
+        while (r1 < n && (acc + ubh[r1] <= kChunk || r1 == r0)) acc += ubh[r1++];
+        const int cn = r1 - r0;
+        exclusive_scan(ub.get() + r0, uoff.get(), cn);
+        k_ext_pattern<<<grid_for(cn, 256), 256, 0, stream()>>>(cn, r0, S.rowptr.get(), S.cols.get(),
+                                                               st, uoff.get(), list.get(), cnt.get());
+        RB_CHECK_LAUNCH();
+        r0 = r1;
+    }
+    list.release();
+    uoff.release();
+    ub.release();
     long long nnz0 = exclusive_scan(cnt.get(), prp.get(), n);
     pcols.alloc((size_t)std::max(nnz0, 1LL));
     pvals.alloc((size_t)std::max(nnz0, 1LL));
     if (n) k_ext_fill<<<g, 256, 0, stream()>>>(
         n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(), st,
-        uoff.get(), list.get(), prp.get(), pcols.get(), pvals.get(), filter, kept.get());
+        prp.get(), pcols.get(), pvals.get(), filter, kept.get());
     RB_CHECK_LAUNCH();
-    list.release();
     DevArray<int> frp((size_t)n + 1);
     long long nnz = exclusive_scan(kept.get(), frp.get(), n);
     rb_csr_s* P = new_csr(n, nc, nnz);

@@ -110,6 +110,8 @@ struct EpiStoreDot {
     }
 };
 
+unsigned row_grid_fwd(long n, int G);
+
 struct NoFinish {
     __device__ void operator()(double) const {}
 };
@@ -133,23 +135,29 @@ k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
         if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); }
         Acc sum = 0;
         int j = s + gl;
-        for (; j + G < e; j += 2 * G) {
+        // four independent index/value loads ahead of their gathers
+        for (; j + 3 * G < e; j += 4 * G) {
             const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + G);
+            const int c2 = __ldg(ci + j + 2 * G), c3 = __ldg(ci + j + 3 * G);
             const TV v0 = __ldg(cv + j), v1 = __ldg(cv + j + G);
-            sum += (Acc)v0 * (Acc)__ldg(x + c0);
-            sum += (Acc)v1 * (Acc)__ldg(x + c1);
+            const TV v2 = __ldg(cv + j + 2 * G), v3 = __ldg(cv + j + 3 * G);
+            const TX x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+            sum += (Acc)v0 * (Acc)x0;
+            sum += (Acc)v1 * (Acc)x1;
+            sum += (Acc)v2 * (Acc)x2;
+            sum += (Acc)v3 * (Acc)x3;
         }
-        if (j < e) sum += (Acc)__ldg(cv + j) * (Acc)__ldg(x + __ldg(ci + j));
+        for (; j < e; j += G) sum += (Acc)__ldg(cv + j) * (Acc)__ldg(x + __ldg(ci + j));
         sum = group_sum<G>(sum);
         if (valid && gl == 0) epi(row, sum, red);
     }
     (void)red;
 }
 
-template <int G, class Fin>
+template <int G, typename TV, class Fin>
 __global__ void __launch_bounds__(kRowBlock)
 k_csr_rows_dot(long n, const int* __restrict__ rp, const int* __restrict__ ci,
-               const double* __restrict__ cv, const double* __restrict__ x, EpiStoreDot epi,
+               const TV* __restrict__ cv, const double* __restrict__ x, EpiStoreDot epi,
                ReduceSlot rs, Fin fin) {
     constexpr int RPW = 32 / G;
     const int lane = threadIdx.x & 31;
@@ -163,11 +171,44 @@ k_csr_rows_dot(long n, const int* __restrict__ rp, const int* __restrict__ ci,
         int s = 0, e = 0;
         if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); }
         double sum = 0;
-        for (int j = s + gl; j < e; j += G) sum += __ldg(cv + j) * __ldg(x + __ldg(ci + j));
+        int j = s + gl;
+        for (; j + 3 * G < e; j += 4 * G) {
+            const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + G);
+            const int c2 = __ldg(ci + j + 2 * G), c3 = __ldg(ci + j + 3 * G);
+            const TV v0 = __ldg(cv + j), v1 = __ldg(cv + j + G);
+            const TV v2 = __ldg(cv + j + 2 * G), v3 = __ldg(cv + j + 3 * G);
+            const double x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+            sum += (double)v0 * x0;
+            sum += (double)v1 * x1;
+            sum += (double)v2 * x2;
+            sum += (double)v3 * x3;
+        }
+        for (; j < e; j += G) sum += (double)__ldg(cv + j) * __ldg(x + __ldg(ci + j));
         sum = group_sum<G>(sum);
         if (valid && gl == 0) epi(row, sum, red);
     }
     block_reduce_finish(red, rs, fin);
+}
+
+ReduceSlot global_reduce_slot(int grid);
+
+// y = A x fused with x.y (deterministic), CSR with values of type TV and
+// FP64 vectors/accumulation.
+template <typename TV, class Fin>
+void launch_rows_dot(const int* rp, const int* ci, const TV* cv, long n, const double* x,
+                     double* y, int G, Fin fin) {
+    const unsigned grid = row_grid_fwd(n, G);
+    ReduceSlot rs = global_reduce_slot(grid);
+    EpiStoreDot epi{x, y};
+    switch (G) {
+        case 1: k_csr_rows_dot<1, TV><<<grid, kRowBlock, 0, stream()>>>(n, rp, ci, cv, x, epi, rs, fin); break;
+        case 2: k_csr_rows_dot<2, TV><<<grid, kRowBlock, 0, stream()>>>(n, rp, ci, cv, x, epi, rs, fin); break;
+        case 4: k_csr_rows_dot<4, TV><<<grid, kRowBlock, 0, stream()>>>(n, rp, ci, cv, x, epi, rs, fin); break;
+        case 8: k_csr_rows_dot<8, TV><<<grid, kRowBlock, 0, stream()>>>(n, rp, ci, cv, x, epi, rs, fin); break;
+        case 16: k_csr_rows_dot<16, TV><<<grid, kRowBlock, 0, stream()>>>(n, rp, ci, cv, x, epi, rs, fin); break;
+        default: k_csr_rows_dot<32, TV><<<grid, kRowBlock, 0, stream()>>>(n, rp, ci, cv, x, epi, rs, fin); break;
+    }
+    RB_CHECK_LAUNCH();
 }
 
 // Lanes per row from the mean row length (a power of two in 2..32).
@@ -189,6 +230,8 @@ inline unsigned row_grid(long n, int G) {
     return (unsigned)blocks;
 }
 
+inline unsigned row_grid_fwd(long n, int G) { return row_grid(n, G); }
+
 template <typename TV, typename TX, class Epi>
 void launch_rows(const int* rp, const int* ci, const TV* cv, long n, long long nnz, const TX* x,
                  Epi epi, int G = 0, cudaStream_t st = nullptr) {
@@ -197,6 +240,7 @@ void launch_rows(const int* rp, const int* ci, const TV* cv, long n, long long n
     if (G <= 0) G = pick_group(n, nnz);
     const unsigned grid = row_grid(n, G);
     switch (G) {
+        case 1: k_csr_rows<1><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
         case 2: k_csr_rows<2><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
         case 4: k_csr_rows<4><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
         case 8: k_csr_rows<8><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;

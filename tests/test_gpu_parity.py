@@ -246,7 +246,8 @@ def hierarchy_pair(Ao, interp, relax, **kw):
     ml.setup(A)
     om = O.Hierarchy(Ao, interp=interp, relax={"sor": "mc_sor", "ssor": "mc_ssor"}.get(relax, relax),
                      **{k: v for k, v in kw.items() if k in ("relax_weight", "jacobi_compat", "solve_tol",
-                                                            "num_smooth_sweeps", "max_coarse")})
+                                                            "num_smooth_sweeps", "max_coarse",
+                                                            "max_iterations")})
     return A, ml, om
 
 
@@ -331,3 +332,91 @@ def test_pre_bicgstab_vs_oracle():
     m = min(len(res), len(ho), 8)
     np.testing.assert_allclose(res[:m], ho[:m], rtol=1e-8)
     assert np.linalg.norm(O.residual(Ao, x.numpy(), bh)) <= 1e-7 * np.linalg.norm(bh)
+
+
+# ------------------------------------------------------- precision form --
+@pytest.mark.parametrize("prob", ["lap27_24", "aniso128"])
+def test_fp32_preconditioner_reaches_fp64_accuracy(prob):
+    Ao = lap27(24) if prob == "lap27_24" else aniso(128)
+    A = to_rb(Ao)
+    n = Ao.shape[0]
+    bh = np.random.default_rng(3).uniform(-1, 1, n)
+    b = rb.ParVector(n, values=bh)
+    xs = {}
+    iters = {}
+    for prec in (rb.FP64, rb.FP32):
+        ml = rb.ParRugeStubenSolver(0.25, rb.PMIS, rb.Extended, rb.Classical, rb.L1Jacobi)
+        ml.precision = prec
+        ml.setup(A)
+        x = rb.ParVector(n)
+        res = []
+        rb.PCG(A, ml, x, b, res, tol=1e-8, max_iter=300, mode=rb.PCG_TRUE_RESIDUAL)
+        r = rb.ParVector(n)
+        A.residual(x, b, r)
+        # the FP64 outer iteration verifies the true residual at exit
+        assert r.norm(2) <= 1e-8 * np.linalg.norm(bh)
+        xs[prec] = x.numpy()
+        iters[prec] = len(res) - 1
+    # same accuracy: both solutions agree to the level the tolerance allows
+    ref = np.linalg.solve(Ao.to_scipy().toarray(), bh) if n <= 20000 else xs[rb.FP64]
+    for prec in (rb.FP64, rb.FP32):
+        assert np.linalg.norm(xs[prec] - ref) <= 1e-5 * np.linalg.norm(ref)
+    assert iters[rb.FP32] <= iters[rb.FP64] + 3
+
+
+def test_fp32_cycle_matches_fp64_cycle_to_single_precision():
+    Ao = lap27(20)
+    A = to_rb(Ao)
+    n = Ao.shape[0]
+    bh = np.random.default_rng(5).uniform(-1, 1, n)
+    b = rb.ParVector(n, values=bh)
+    out = {}
+    for prec in (rb.FP64, rb.FP32):
+        ml = rb.ParRugeStubenSolver(0.25, rb.PMIS, rb.Extended, rb.Classical, rb.L1Jacobi)
+        ml.precision = prec
+        ml.setup(A)
+        x = rb.ParVector(n)
+        ml.cycle(x, b)
+        out[prec] = x.numpy()
+    np.testing.assert_allclose(out[rb.FP32], out[rb.FP64], rtol=0,
+                               atol=1e-5 * np.abs(out[rb.FP64]).max())
+
+
+# --------------------------------------------------- multicolour smoothers --
+def conv_factor(hist, start=5):
+    h = np.asarray(hist)
+    h = h[h > 0]
+    k = len(h) - 1
+    if k <= start:
+        return float(h[-1] / h[0]) ** (1.0 / max(k, 1))
+    return float(h[-1] / h[start]) ** (1.0 / (k - start))
+
+
+@pytest.mark.parametrize("relax", ["sor", "ssor"])
+def test_multicolour_sor_matches_oracle_restatement(relax):
+    Ao = aniso(64)
+    A, ml, om = hierarchy_pair(Ao, "mod_classical", relax, solve_tol=1e-8)
+    n = Ao.shape[0]
+    bh = O.spmv(Ao, np.ones(n))
+    x = rb.ParVector(n)
+    b = rb.ParVector(n, values=bh)
+    it = ml.solve(x, b)
+    xo, ito, ho = om.solve(np.zeros(n), bh)
+    assert it == ito
+    np.testing.assert_allclose(ml.get_residuals(), ho, rtol=1e-9)
+
+
+@pytest.mark.parametrize("prob,interp", [("aniso100", "mod_classical"), ("lap27_20", "extended")])
+def test_multicolour_sor_convergence_factor_within_5pct(prob, interp):
+    Ao = aniso(100) if prob == "aniso100" else lap27(20)
+    A, ml, _ = hierarchy_pair(Ao, interp, "sor", solve_tol=1e-10, max_iterations=60)
+    n = Ao.shape[0]
+    bh = O.spmv(Ao, np.ones(n))
+    x = rb.ParVector(n)
+    ml.solve(x, rb.ParVector(n, values=bh))
+    rho_mc = conv_factor(ml.get_residuals())
+    # the reference's sequential forward Gauss-Seidel (par_relax.cpp:29-68)
+    seq = O.Hierarchy(Ao, interp=interp, relax="sor", solve_tol=1e-10, max_iterations=60)
+    _, _, hs = seq.solve(np.zeros(n), bh)
+    rho_ref = conv_factor(hs)
+    assert abs(rho_mc - rho_ref) <= 0.05 * rho_ref, (rho_mc, rho_ref)
