@@ -193,8 +193,20 @@ def cycle_bytes(ml, vbytes):
 def run_b200(args, rank, world, local):
     import raptor_b200 as rb
 
+    import ctypes as C
+    import torch
+
     dist = Dist(world, local)
     rb.init(local)
+    # every library call is ordered on this stream; the CUDA events that time
+    # the steps are recorded on it
+    ts = torch.cuda.Stream(device=local)
+    rb.check(rb.lib().rb_set_stream(C.c_void_p(ts.cuda_stream)))
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(ts)
+        return e
     S = args.size
     A = rb.par_stencil_grid(rb.laplace_stencil_27pt(), [S, S, S])
     n = A.global_num_rows
@@ -222,13 +234,14 @@ def run_b200(args, rank, world, local):
         rb.lib().rb_synchronize()
         dist.barrier()
         c0 = rb.launch_count()
-        t0 = time.perf_counter()
+        e0 = ev()
         iters = []
         for _ in range(steps):
             rc, it = solve(ml)
             iters.append(it)
+        e1 = ev()
         rb.lib().rb_synchronize()
-        el = time.perf_counter() - t0
+        el = e0.elapsed_time(e1) * 1e-3
         launches = rb.launch_count() - c0
         dist.barrier()
         return dist.max(el) / steps, iters, launches
@@ -305,16 +318,19 @@ def run_b200(args, rank, world, local):
     ml_e2e = ml32
     e2e_t = []
     for s in range(args.warmup + args.steps):
-        dist.barrier()
-        t0 = time.perf_counter()
         L.rb_vec_upload.argtypes = [C.c_void_p, C.c_void_p]
         L.rb_vec_download.argtypes = [C.c_void_p, C.c_void_p]
+        rb.lib().rb_synchronize()
+        dist.barrier()
+        e0 = ev()
         assert L.rb_vec_upload(b.h, C.c_void_p(hbp)) == 0
         x.set_const_value(0.0)
         res = []
         rb.PCG(A, ml_e2e, x, b, res, tol=TOL, max_iter=500, mode=rb.PCG_TRUE_RESIDUAL)
         assert L.rb_vec_download(x.h, C.c_void_p(hxp)) == 0
-        el = time.perf_counter() - t0
+        e1 = ev()
+        rb.lib().rb_synchronize()
+        el = e0.elapsed_time(e1) * 1e-3
         if s >= args.warmup:
             e2e_t.append(dist.max(el))
     # restore numpy-typed signatures
