@@ -197,6 +197,21 @@ int rb_amg_level_storage(rb_amg ml, int level, int* ndiag);
  * kernel nodes). */
 int rb_launch_count(int64_t* count);
 
+/* ||b - A x||_2 into norm_out[0] without allocating device memory.  No
+ * counterpart in the reference.  For callers that must not allocate while
+ * they run: runtimes that hand the solver a fixed memory budget and forbid
+ * allocation once a solve is under way (an allocation there can fail), and
+ * real-time loops in which cudaMalloc's implicit device synchronisation
+ * would break the deadline.  Every pointer is device memory owned by the caller (CSR arrays of A
+ * with n_rows rows, x, b, and one double for the result); stream is a
+ * cudaStream_t (NULL = default stream).  Its scratch is a file-scope device
+ * array (128 KiB per device, held until exit), so n_rows is limited to
+ * 16777216 (RB_ERR_INVALID beyond).  The first call on a device resolves the
+ * array's address and must precede any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race. */
+int rb_residual_norm_noalloc(int n_rows, const int* rowptr, const int* cols, const double* vals,
+                             const double* x, const double* b, double* norm_out, void* stream);
+
 /* ------------------------------------------------------------------ Krylov */
 #define RB_PCG_REFERENCE 0 /* par_cg.cpp:121-263 exactly: stop on r.z < tol*sqrt(b.Mb) */
 #define RB_PCG_TRUE_RESIDUAL 1 /* stop on ||b - A x|| / ||b|| < tol */

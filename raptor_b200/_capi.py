@@ -103,6 +103,7 @@ SIGNATURES = {
     "rb_amg_setup_seconds": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "rb_amg_level_lanes": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "rb_amg_level_storage": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_residual_norm_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "rb_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rb_pcg": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
     "rb_cg": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
