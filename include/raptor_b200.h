@@ -113,6 +113,24 @@ int rb_split_pmis(rb_csr S, const double* weights, int* states);
  * extended_interpolation + filter_interp (:280-989, :175-278). */
 int rb_interpolation(rb_csr A, rb_csr S, const int* states, int kind, double filter,
                      rb_csr* P);
+/* mis2 (aggregation/par_mis.cpp:204-645) on a strength matrix S with its
+ * diagonal first; weights as for rb_split_pmis (NULL = the reference's glibc
+ * rand() weights); states (host, n_rows) receive 1 = root, 0 = not a root. */
+int rb_mis2(rb_csr S, const double* weights, int* states);
+/* aggregate (aggregation/par_aggregate.cpp:5-185): A and S with the
+ * diagonal first, states from rb_mis2, r the tie-break weights (NULL = 0, as
+ * the solver calls it).  aggregates (host, n_rows) receive each row's root
+ * row index (-1 = unaggregated); n_aggs the number of roots. */
+int rb_aggregate(rb_csr A, rb_csr S, const int* states, const double* r, int* aggregates,
+                 int* n_aggs);
+/* fit_candidates with one candidate (aggregation/par_candidates.cpp:6-216):
+ * T (n_rows x n_aggs, one entry B_i / R_a per aggregated row, columns = the
+ * roots in increasing order) and R (host, n_aggs) the aggregate norms. */
+int rb_fit_candidates(int n_rows, int n_aggs, const int* aggregates, const double* B, double* R,
+                      rb_csr* T);
+/* jacobi_prolongation (aggregation/par_prolongation.cpp:7-104):
+ * P = (I - omega D_abs^-1 A)^steps T with D_abs the absolute row sums. */
+int rb_jacobi_prolongation(rb_csr A, rb_csr T, double omega, int steps, rb_csr* P);
 /* C = A B (ParCSRMatrix::mult, par_matmult.cpp:73-107 -> matmult.cpp:71-137 +
  * add.cpp:39-78): rows sorted by column, |c| <= 1e-16 dropped. */
 int rb_spgemm(rb_csr A, rb_csr B, rb_csr* C);

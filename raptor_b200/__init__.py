@@ -27,6 +27,8 @@ Classical, Symmetric = 0, 1                 # strength_t
 RS, CLJP, Falgout, PMIS, HMIS = 0, 1, 2, 3, 4   # coarsen_t (PMIS is built)
 Direct, ModClassical, Extended = 0, 1, 2    # interp_t
 Jacobi, SOR, SSOR, L1Jacobi = 0, 1, 2, 3    # relax_t (+ L1-Jacobi)
+MIS = 0                                     # agg_t
+JacobiProlongation = 0                      # prolong_t
 FP64, FP32 = 0, 1                           # cycle precision
 PCG_REFERENCE, PCG_TRUE_RESIDUAL = 0, 1
 
@@ -256,6 +258,45 @@ def rap(A, P, diag_first=True):
     return ParCSRMatrix(h)
 
 
+def mis2(S, weights=None):
+    """mis2 (aggregation/par_mis.cpp:204-645): 1 = root, 0 = not a root."""
+    n = S.global_num_rows
+    st = np.zeros(max(n, 1), np.int32)
+    w = None if weights is None else np.ascontiguousarray(weights[:n], np.float64)
+    check(lib().rb_mis2(S.h, _ptr(w) if w is not None else None, st))
+    return st[:n]
+
+
+def aggregate(A, S, states, rand_vals=None):
+    """aggregate (aggregation/par_aggregate.cpp:5-185) -> (n_aggs, aggregates);
+    aggregates hold each row's root row index, -1 when unaggregated."""
+    n = S.global_num_rows
+    st = np.ascontiguousarray(states, np.int32)
+    agg = np.zeros(max(n, 1), np.int32)
+    r = None if rand_vals is None else np.ascontiguousarray(rand_vals[:n], np.float64)
+    na = C.c_int()
+    check(lib().rb_aggregate(A.h, S.h, st, _ptr(r) if r is not None else None, agg, C.byref(na)))
+    return na.value, agg[:n]
+
+
+def fit_candidates(n, n_aggs, aggregates, B):
+    """fit_candidates with one candidate (aggregation/par_candidates.cpp:6-216)
+    -> (T, R)."""
+    agg = np.ascontiguousarray(aggregates, np.int32)
+    Bv = np.ascontiguousarray(B[:n], np.float64)
+    R = np.zeros(max(n_aggs, 1), np.float64)
+    h = C.c_void_p()
+    check(lib().rb_fit_candidates(int(n), int(n_aggs), agg, Bv, R, C.byref(h)))
+    return ParCSRMatrix(h), R[:n_aggs]
+
+
+def jacobi_prolongation(A, T, omega=4.0 / 3.0, num_smooth_steps=1):
+    """jacobi_prolongation (aggregation/par_prolongation.cpp:7-104)."""
+    h = C.c_void_p()
+    check(lib().rb_jacobi_prolongation(A.h, T.h, float(omega), int(num_smooth_steps), C.byref(h)))
+    return ParCSRMatrix(h)
+
+
 # multilevel ---------------------------------------------------------------
 class ParMultilevel:
     """ParMultilevel (multilevel/par_multilevel.hpp:75-659) on the device."""
@@ -396,6 +437,23 @@ class ParRugeStubenSolver(ParMultilevel):
         if interp_type not in (ModClassical, Extended):
             raise RaptorError(-1, "interpolation must be ModClassical or Extended")
         self.opts.interp_type = interp_type
+
+
+class ParSmoothedAggregationSolver(ParMultilevel):
+    """ParSmoothedAggregationSolver
+    (aggregation/par_smoothed_aggregation_solver.hpp:13-136): symmetric
+    strength, mis2 aggregation, one all-ones candidate, Jacobi-smoothed
+    tentative prolongator, Galerkin coarse operators."""
+
+    def __init__(self, strong_threshold=0.0, agg_type=MIS, prolong_type=JacobiProlongation,
+                 strength_type=Symmetric, relax_type=SOR, prolong_smooth_steps=1,
+                 prolong_weight=4.0 / 3):
+        super().__init__(strong_threshold, strength_type, relax_type)
+        if agg_type != MIS or prolong_type != JacobiProlongation:
+            raise RaptorError(-1, "only MIS aggregation with Jacobi prolongation exists")
+        self.opts.solver = 1
+        self.opts.prolong_smooth_steps = prolong_smooth_steps
+        self.opts.prolong_weight = prolong_weight
 
 
 # Krylov -------------------------------------------------------------------

@@ -87,6 +87,10 @@ SIGNATURES = {
     "rb_strength": (C.c_int, [_P, C.c_int, C.c_double, _PP]),
     "rb_split_pmis": (C.c_int, [_P, _P, _I]),
     "rb_interpolation": (C.c_int, [_P, _P, _I, C.c_int, C.c_double, _PP]),
+    "rb_mis2": (C.c_int, [_P, _P, _I]),
+    "rb_aggregate": (C.c_int, [_P, _P, _I, _P, _I, C.POINTER(C.c_int)]),
+    "rb_fit_candidates": (C.c_int, [C.c_int, C.c_int, _I, _D, _D, _PP]),
+    "rb_jacobi_prolongation": (C.c_int, [_P, _P, C.c_double, C.c_int, _PP]),
     "rb_spgemm": (C.c_int, [_P, _P, _PP]),
     "rb_rap": (C.c_int, [_P, _P, C.c_int, _PP]),
     "rb_amg_default_opts": (None, [C.POINTER(AmgOpts)]),

@@ -445,6 +445,66 @@ int rb_interpolation(rb_csr A, rb_csr S, const int* states, int kind, double fil
     });
 }
 
+int rb_mis2(rb_csr S, const double* weights, int* states) {
+    return guarded([&]() -> int {
+        NEED(S); NEED(states);
+        const int n = S->n_rows;
+        std::vector<double> w = weights ? std::vector<double>(weights, weights + n) : rand_weights(n, 0);
+        DevArray<double> wd((size_t)std::max(n, 1));
+        wd.upload(w.data(), n);
+        DevArray<int> st((size_t)std::max(n, 1));
+        mis2(*S, wd.get(), st.get());
+        st.download(states, n);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_aggregate(rb_csr A, rb_csr S, const int* states, const double* r, int* aggregates,
+                 int* n_aggs) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(S); NEED(states); NEED(aggregates); NEED(n_aggs);
+        const int n = S->n_rows;
+        DevArray<int> st((size_t)std::max(n, 1)), agg((size_t)std::max(n, 1));
+        st.upload(states, n);
+        DevArray<double> rd;
+        if (r) {
+            rd.alloc((size_t)std::max(n, 1));
+            rd.upload(r, n);
+        }
+        *n_aggs = aggregate(*A, *S, st.get(), agg.get(), r ? rd.get() : nullptr);
+        agg.download(aggregates, n);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_fit_candidates(int n_rows, int n_aggs, const int* aggregates, const double* B, double* R,
+                      rb_csr* T) {
+    return guarded([&]() -> int {
+        NEED(aggregates); NEED(B); NEED(R); NEED(T);
+        RB_REQUIRE(n_rows >= 0 && n_aggs >= 0, "negative size");
+        ensure_device();
+        DevArray<int> agg((size_t)std::max(n_rows, 1));
+        agg.upload(aggregates, n_rows);
+        DevArray<double> Bd((size_t)std::max(n_rows, 1)), Rd((size_t)std::max(n_aggs, 1));
+        Bd.upload(B, n_rows);
+        *T = fit_candidates(n_rows, n_aggs, agg.get(), Bd.get(), Rd.get());
+        Rd.download(R, n_aggs);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_jacobi_prolongation(rb_csr A, rb_csr T, double omega, int steps, rb_csr* P) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(T); NEED(P);
+        RB_REQUIRE(steps >= 0, "steps < 0");
+        *P = jacobi_prolongation(*A, *T, omega, steps);
+        return RB_OK;
+    });
+}
+
 int rb_spgemm(rb_csr A, rb_csr B, rb_csr* C) {
     return guarded([&]() -> int {
         NEED(A); NEED(B); NEED(C);
@@ -495,7 +555,8 @@ int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_am
         rb_amg_opts o;
         if (opts) o = *opts;
         else rb_amg_default_opts(&o);
-        RB_REQUIRE(o.solver == RB_SOLVER_RS, "only the Ruge-Stuben solver is built in this library");
+        RB_REQUIRE(o.solver == RB_SOLVER_RS || o.solver == RB_SOLVER_SA, "unknown solver");
+        RB_REQUIRE(o.prolong_smooth_steps >= 0, "prolong_smooth_steps < 0");
         RB_REQUIRE(o.num_smooth_sweeps >= 0, "num_smooth_sweeps < 0");
         std::unique_ptr<rb_amg_s> ml(new rb_amg_s());
         ml->h.setup(*A, o, weights);

@@ -343,17 +343,46 @@ void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* we
     DevArray<double> wdev((size_t)std::max(Af.n_rows, 1));
     wdev.upload(w.data(), w.size());
 
+    // smoothed aggregation: near-nullspace candidate B, all ones on level 0
+    // (par_smoothed_aggregation_solver.hpp:38-47), replaced by the
+    // aggregate norms R of each level for the next one (:122)
+    const bool sa = o.solver == RB_SOLVER_SA;
+    DevArray<double> cand;
+    if (sa) {
+        std::vector<double> ones((size_t)std::max(Af.n_rows, 1), 1.0);
+        cand.alloc(ones.size());
+        cand.upload(ones.data(), ones.size());
+    }
+
     while (master.back().A->n_rows > o.max_coarse &&
            (o.max_levels == -1 || (int)master.size() < o.max_levels)) {
         MasterLevel& L = master.back();
         const rb_csr_s& A = *L.A;
         std::unique_ptr<rb_csr_s> S(strength(A, o.strength_type, o.strong_threshold));
         L.states.alloc((size_t)std::max(A.n_rows, 1));
-        split_pmis(*S, wdev.get(), L.states.get());
-        L.P.reset(interpolation(A, *S, L.states.get(), o.interp_type, o.interp_filter));
+        if (sa) {
+            // par_smoothed_aggregation_solver.hpp:51-129: mis2, aggregate,
+            // fit_candidates, jacobi_prolongation; A_c = P^T (A P)
+            sort_rows_diag_first(*S, true);   // aggregate() sorts S (par_aggregate.cpp:13-14)
+            mis2(*S, wdev.get(), L.states.get());
+            DevArray<int> agg((size_t)std::max(A.n_rows, 1));
+            const int n_aggs = aggregate(A, *S, L.states.get(), agg.get(), nullptr);
+            DevArray<double> R((size_t)std::max(n_aggs, 1));
+            std::unique_ptr<rb_csr_s> T(fit_candidates(A.n_rows, n_aggs, agg.get(), cand.get(),
+                                                       R.get()));
+            L.P.reset(jacobi_prolongation(A, *T, o.prolong_weight, o.prolong_smooth_steps));
+            cand = std::move(R);
+        } else {
+            split_pmis(*S, wdev.get(), L.states.get());
+            L.P.reset(interpolation(A, *S, L.states.get(), o.interp_type, o.interp_filter));
+        }
         S.reset();
         L.R.reset(transpose(*L.P));
-        rb_csr_s* Ac = rap(A, *L.P, L.R.get(), true);
+        // RS sorts A_c with the diagonal first (par_ruge_stuben_solver.hpp:142-143);
+        // SA leaves it sorted by column and the next level's setup (or the
+        // relaxation) moves the diagonal first, which is the same thing
+        rb_csr_s* Ac = rap(A, *L.P, L.R.get(), !sa);
+        if (sa) sort_rows_diag_first(*Ac, true);
         if (Ac->n_rows == 0 || Ac->n_rows == A.n_rows) {
             // no coarsening possible: keep this level as the coarsest
             delete Ac;

@@ -58,6 +58,15 @@ rb_csr_s* spgemm(const rb_csr_s& A, const rb_csr_s& B);
 rb_csr_s* rap(const rb_csr_s& A, const rb_csr_s& P, const rb_csr_s* R_in, bool diag_first);
 int colour_rows(const rb_csr_s& A, int* colour_dev);
 
+// Smoothed-aggregation setup components (aggregation.cu).  states, agg, r, B
+// and R are device arrays.
+void mis2(const rb_csr_s& S, const double* r_dev, int* states_dev);
+int aggregate(const rb_csr_s& A, const rb_csr_s& S, const int* states_dev, int* agg_dev,
+              const double* r_dev);
+rb_csr_s* fit_candidates(int n, int n_aggs, const int* agg_dev, const double* B_dev,
+                         double* R_dev);
+rb_csr_s* jacobi_prolongation(const rb_csr_s& A, const rb_csr_s& T, double omega, int steps);
+
 // glibc rand() weights of the reference (par_multilevel.hpp:215-225).
 std::vector<double> rand_weights(int n, int first_row);
 
