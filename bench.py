@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=96)
+    p.add_argument("--batch-size", type=int, default=160,
+                   help="grid side of the k right-hand-side workload (0 skips it)")
     return p.parse_args()
 
 
@@ -188,6 +190,57 @@ def cycle_bytes(ml, vbytes):
         per.append(b)
         tot += b
     return tot, per
+
+
+def aniso7_stencil(cz=0.01):
+    """3D 7-point anisotropic diffusion (1, 1, cz) as a 27-entry stencil."""
+    st = [0.0] * 27
+    st[13] = 4.0 + 2.0 * cz
+    st[12] = st[14] = -1.0
+    st[10] = st[16] = -1.0
+    st[4] = st[22] = -cz
+    return st
+
+
+def run_batching(rb, ev, sync, S, ks=(1, 8, 32), steps=2):
+    """k right-hand sides over one smoothed-aggregation hierarchy: the
+    7-point anisotropic diffusion (1, 1, 0.01) on S^3, FP32 V-cycle, FP64
+    outer CG, each column to 1e-8 true relative residual."""
+    A = rb.par_stencil_grid(aniso7_stencil(), [S, S, S])
+    n = A.global_num_rows
+    ml = rb.ParSmoothedAggregationSolver(0.25, relax_type=rb.L1Jacobi)
+    ml.precision = rb.FP32
+    ml.setup(A)
+    out = {"workload": "SA (symmetric strength 0.25, mis2 aggregates, Jacobi-smoothed "
+                       "prolongator, L1-Jacobi) on 7-point aniso (1, 1, 0.01) %d^3, FP32 "
+                       "V-cycle, FP64 outer CG to 1e-8 per column" % S,
+           "rows": n, "nnz": A.local_nnz, "levels": ml.num_levels,
+           "setup_s": ml.setup_seconds, "k": {}}
+    rng = np.random.default_rng(SEED + 7)
+    for k in ks:
+        Bv = rb.ParVector(n * k, values=rng.uniform(-1.0, 1.0, n * k))
+        Xv = rb.ParVector(n * k)
+        times = []
+        iters = relres = None
+        for s in range(1 + steps):
+            Xv.set_const_value(0.0)
+            sync()
+            e0 = ev()
+            rc, iters, relres = rb.PCG_block(A, ml, Xv, Bv, k, tol=TOL, max_iter=500)
+            e1 = ev()
+            sync()
+            if s >= 1:
+                times.append(e0.elapsed_time(e1))
+        ms = sum(times) / len(times)
+        out["k"][str(k)] = {"ms": ms, "ms_per_rhs": ms / k, "iters_max": int(max(iters)),
+                            "iters_min": int(min(iters)),
+                            "max_true_rel_res": float(max(relres)), "status": rc}
+        del Bv, Xv
+    k1 = out["k"].get("1")
+    for k in ks:
+        if k1 and k != 1:
+            out["k"][str(k)]["per_rhs_speedup_vs_k1"] = k1["ms"] / out["k"][str(k)]["ms_per_rhs"]
+    return out
 
 
 def run_b200(args, rank, world, local):
@@ -365,6 +418,9 @@ def run_b200(args, rank, world, local):
         "clocks": clk,
     }
     out["config"]["levels"] = ml.num_levels
+    if args.batch_size > 0:
+        out["batching"] = run_batching(rb, ev, lambda: rb.lib().rb_synchronize(),
+                                       args.batch_size)
     if rank == 0 and args.cpu_sample > 0:
         out["cpu_baseline"] = cpu_baseline(args.cpu_sample, S, iters32[-1])
     dist.close()

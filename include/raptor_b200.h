@@ -241,6 +241,20 @@ int rb_residual_norm_noalloc(int n_rows, const int* rowptr, const int* cols, con
  * n_hist receives the entry count. */
 int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, int mode,
            double* hist, int cap, int* n_hist);
+/* One V-cycle from a zero guess applied to k columns at once, X = M B
+ * (columns interleaved by row, n * k entries each; k in 2..32; Jacobi or
+ * L1-Jacobi smoothing).  No counterpart in the reference. */
+int rb_amg_cycle_block(rb_amg ml, rb_vec X, rb_vec B, int k);
+/* k right-hand sides over one hierarchy (no counterpart in the reference,
+ * which solves one at a time).  X and B are vectors of n * k entries with the
+ * columns interleaved by row: entry (i, c) at i * k + c.  Runs k independent
+ * preconditioned CG recurrences whose SpMMs read every matrix once for all
+ * columns; each column stops when its true ||b_c - A x_c|| / ||b_c|| <= tol.
+ * iters[k] and relres[k] (host) receive each column's iterations and final
+ * true relative residual.  k in 1..32; the smoother must be Jacobi or
+ * L1-Jacobi.  Columns with b_c = 0 are left as given. */
+int rb_pcg_block(rb_csr A, rb_amg ml, rb_vec X, rb_vec B, int k, double tol, int max_iter,
+                 int* iters, double* relres);
 /* CG (krylov/par_cg.cpp:8-118); hist = ||r||/||b||. */
 int rb_cg(rb_csr A, rb_vec x, rb_vec b, double tol, int max_iter, double* hist, int cap,
           int* n_hist);

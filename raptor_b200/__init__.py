@@ -388,6 +388,10 @@ class ParMultilevel:
     def get_residuals(self):
         return self.residuals
 
+    def cycle_block(self, X, B, k):
+        """X = M B for k interleaved columns (one V-cycle from a zero guess)."""
+        check(lib().rb_amg_cycle_block(self.h, X.h, B.h, int(k)))
+
     def cycle_profile(self):
         """Milliseconds per level: rows [pre, residual, restrict, prolong, post, coarse]."""
         L = self.num_levels
@@ -474,6 +478,18 @@ def PCG(A, ml, x, b, res, tol=1e-5, max_iter=-1, mode=PCG_REFERENCE):
     if rc not in (0, -5):
         check(rc)
     return rc
+
+
+def PCG_block(A, ml, X, B, k, tol=1e-8, max_iter=-1):
+    """k right-hand sides over one hierarchy: X, B are ParVectors of n * k
+    entries, columns interleaved by row.  Returns (status, iters[k], relres[k])
+    with each column's iterations and final true relative residual."""
+    iters = np.zeros(max(k, 1), np.int32)
+    relres = np.zeros(max(k, 1), np.float64)
+    rc = lib().rb_pcg_block(A.h, ml.h, X.h, B.h, int(k), float(tol), int(max_iter), iters, relres)
+    if rc not in (0, -5):
+        check(rc)
+    return rc, iters[:k], relres[:k]
 
 
 def CG(A, x, b, res, tol=1e-5, max_iter=-1):

@@ -110,6 +110,8 @@ SIGNATURES = {
     "rb_residual_norm_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "rb_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rb_pcg": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_amg_cycle_block": (C.c_int, [_P, _P, _P, C.c_int]),
+    "rb_pcg_block": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_double, C.c_int, _I, _D]),
     "rb_cg": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
     "rb_bicgstab": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
 }

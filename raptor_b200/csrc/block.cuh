@@ -1,0 +1,411 @@
+// block.cuh -- k right-hand sides at once: block-vector SpMM kernels.
+//
+// A block vector holds k columns interleaved by row: entry (i, c) at
+// i * k + c.  One pass over A then serves all k columns: the values and
+// column indices of a row are read once (a broadcast to the lanes of the
+// row's columns), and the k entries of x at each column index are one
+// contiguous run.  For a bandwidth-bound operator this divides the matrix
+// traffic per right-hand side by k.
+//
+// Lane layout of a warp: KP lanes per row cover the columns (KP = k rounded
+// up to a power of two; lanes c >= k idle), S such groups split the row's
+// nonzeros, and 32 / (KP S) rows share the warp.  (KP, S) is the tile shape
+// the autotuner picks per operator.
+#pragma once
+
+#include "dia.cuh"
+
+namespace rb {
+
+constexpr int kMaxBlockK = 32;
+
+// ----------------------------------------------------------- epilogues --
+template <typename TY>
+struct BStore {
+    TY* y;
+    template <typename A>
+    __device__ void operator()(long i, int c, int k, A s) const { y[i * k + c] = (TY)s; }
+};
+
+template <typename TB, typename TY>
+struct BResidual {
+    const TB* b;
+    TY* r;
+    template <typename A>
+    __device__ void operator()(long i, int c, int k, A s) const {
+        r[i * k + c] = (TY)((A)b[i * k + c] - s);
+    }
+};
+
+template <typename TY>
+struct BAppend {
+    TY* y;
+    template <typename A>
+    __device__ void operator()(long i, int c, int k, A s) const {
+        y[i * k + c] = (TY)((A)y[i * k + c] + s);
+    }
+};
+
+template <typename TY>
+struct BAddTo {
+    const TY* x0;
+    TY* y;
+    template <typename A>
+    __device__ void operator()(long i, int c, int k, A s) const {
+        y[i * k + c] = (TY)((A)x0[i * k + c] + s);
+    }
+};
+
+// xn = xo + dinv_i (b - A xo), dinv per row
+template <typename T>
+struct BJacobi {
+    const T* xo;
+    const T* b;
+    const T* dinv;
+    T* xn;
+    template <typename A>
+    __device__ void operator()(long i, int c, int k, A s) const {
+        const long e = i * k + c;
+        xn[e] = (T)((A)xo[e] + (A)dinv[i] * ((A)b[e] - s));
+    }
+};
+
+// ------------------------------------------------ per-column reductions --
+// Each lane carries a partial for its column c = lane % KP.  The block sums
+// them per column (warp shuffles over the row lanes, then the warps in a
+// fixed order), writes partials[block * KP + c], and the last block to
+// finish sums the block partials per column in a fixed order and calls
+// fin(c, total) for c < k.  Bit-reproducible for a given grid.
+template <int KP, class Fin>
+__device__ void block_reduce_cols(double v, int k, const ReduceSlot& rs, Fin fin) {
+    constexpr int kWarps = 256 / 32;
+    constexpr int kStrands = 256 / KP;
+    __shared__ double wpart[kWarps][KP];
+    __shared__ double spart[256];
+    __shared__ bool is_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = KP; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane < KP) wpart[wid][lane] = v;
+    __syncthreads();
+    if (threadIdx.x < KP) {
+        double t = 0.0;
+        for (int w = 0; w < kWarps; w++) t += wpart[w][threadIdx.x];
+        rs.partials[(size_t)blockIdx.x * KP + threadIdx.x] = t;
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(rs.ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    // strand q of column c sums blocks q, q + kStrands, ...
+    const int c = threadIdx.x % KP, q = threadIdx.x / KP;
+    double t = 0.0;
+    for (unsigned b = q; b < gridDim.x; b += kStrands)
+        t += ((volatile double*)rs.partials)[(size_t)b * KP + c];
+    spart[threadIdx.x] = t;
+    __syncthreads();
+    if (threadIdx.x < KP) {
+        double tot = 0.0;
+        for (int s = 0; s < kStrands; s++) tot += spart[s * KP + threadIdx.x];
+        if (threadIdx.x < k) fin(threadIdx.x, tot);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *rs.ticket = 0u;
+}
+
+// ----------------------------------------------------------- CSR SpMM --
+template <int KP, int S, typename TV, typename TX, typename Acc, class Epi>
+__global__ void __launch_bounds__(256)
+k_csr_block(long n, int k, const int* __restrict__ rp, const int* __restrict__ ci,
+            const TV* __restrict__ cv, const TX* __restrict__ X, Epi epi) {
+    constexpr int RPW = 32 / (KP * S);
+    const int lane = threadIdx.x & 31;
+    const int c = lane % KP, s = (lane / KP) % S, sub = lane / (KP * S);
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        Acc acc = 0;
+        if (row < n && c < k) {
+            const int rs = __ldg(rp + row), re = __ldg(rp + row + 1);
+            int j = rs + s;
+            for (; j + S < re; j += 2 * S) {
+                const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + S);
+                const TV v0 = __ldg(cv + j), v1 = __ldg(cv + j + S);
+                const TX x0 = __ldg(X + (long)c0 * k + c), x1 = __ldg(X + (long)c1 * k + c);
+                acc += (Acc)v0 * (Acc)x0;
+                acc += (Acc)v1 * (Acc)x1;
+            }
+            if (j < re) acc += (Acc)__ldg(cv + j) * (Acc)__ldg(X + (long)__ldg(ci + j) * k + c);
+        }
+#pragma unroll
+        for (int o = KP; o < KP * S; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (row < n && c < k && s == 0) epi(row, c, k, acc);
+    }
+}
+
+// Y = A P with the per-column dots p.y (FP64 vectors, values TV)
+template <int KP, int S, typename TV, class Fin>
+__global__ void __launch_bounds__(256)
+k_csr_block_dot(long n, int k, const int* __restrict__ rp, const int* __restrict__ ci,
+                const TV* __restrict__ cv, const double* __restrict__ P, double* __restrict__ Y,
+                ReduceSlot rsl, Fin fin) {
+    constexpr int RPW = 32 / (KP * S);
+    const int lane = threadIdx.x & 31;
+    const int c = lane % KP, s = (lane / KP) % S, sub = lane / (KP * S);
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    double red = 0.0;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        double acc = 0;
+        if (row < n && c < k) {
+            const int rs = __ldg(rp + row), re = __ldg(rp + row + 1);
+            int j = rs + s;
+            for (; j + S < re; j += 2 * S) {
+                const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + S);
+                const double x0 = __ldg(P + (long)c0 * k + c), x1 = __ldg(P + (long)c1 * k + c);
+                acc += (double)__ldg(cv + j) * x0;
+                acc += (double)__ldg(cv + j + S) * x1;
+            }
+            if (j < re) acc += (double)__ldg(cv + j) * __ldg(P + (long)__ldg(ci + j) * k + c);
+        }
+#pragma unroll
+        for (int o = KP; o < KP * S; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (row < n && c < k && s == 0) {
+            Y[row * k + c] = acc;
+            red += P[row * k + c] * acc;
+        }
+    }
+    block_reduce_cols<KP>(red, k, rsl, fin);
+}
+
+// ---------------------------------------------------- sliced DIA SpMM --
+template <int ND, int KP, typename TV, typename TX, typename Acc, class Epi>
+__global__ void __launch_bounds__(256)
+k_sdia_block(long n, int k, DiaOff off, const TV* __restrict__ sv, const TX* __restrict__ X,
+             Epi epi) {
+    constexpr int RPW = 32 / KP;
+    const int nd = ND > 0 ? ND : off.nd;
+    const int lane = threadIdx.x & 31;
+    const int c = lane % KP, sub = lane / KP;
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long i = base + sub;
+        if (i >= n || c >= k) continue;
+        const TV* a = sv + (i >> 5) * nd * 32 + (i & 31);
+        Acc acc = 0;
+        if constexpr (ND > 0) {
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+                const long j = i + off.o[d];
+                if (j >= 0 && j < n) acc += (Acc)__ldg(a + d * 32) * (Acc)__ldg(X + j * k + c);
+            }
+        } else {
+            for (int d = 0; d < nd; d++) {
+                const long j = i + off.o[d];
+                if (j >= 0 && j < n) acc += (Acc)__ldg(a + d * 32) * (Acc)__ldg(X + j * k + c);
+            }
+        }
+        epi(i, c, k, acc);
+    }
+}
+
+template <int ND, int KP, typename TV, class Fin>
+__global__ void __launch_bounds__(256)
+k_sdia_block_dot(long n, int k, DiaOff off, const TV* __restrict__ sv,
+                 const double* __restrict__ P, double* __restrict__ Y, ReduceSlot rsl, Fin fin) {
+    constexpr int RPW = 32 / KP;
+    const int nd = ND > 0 ? ND : off.nd;
+    const int lane = threadIdx.x & 31;
+    const int c = lane % KP, sub = lane / KP;
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    double red = 0.0;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long i = base + sub;
+        if (i >= n || c >= k) continue;
+        const TV* a = sv + (i >> 5) * nd * 32 + (i & 31);
+        double acc = 0;
+        for (int d = 0; d < (ND > 0 ? ND : nd); d++) {
+            const long j = i + off.o[d];
+            if (j >= 0 && j < n) acc += (double)__ldg(a + d * 32) * __ldg(P + j * k + c);
+        }
+        Y[i * k + c] = acc;
+        red += P[i * k + c] * acc;
+    }
+    block_reduce_cols<KP>(red, k, rsl, fin);
+}
+
+// ------------------------------------------------------- block BLAS-1 --
+// x = dinv .* b per column (first Jacobi sweep from a zero guess)
+template <typename T>
+__global__ void k_scale_first_block(long n, int k, const T* __restrict__ b,
+                                    const T* __restrict__ dinv, T* __restrict__ x) {
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n * k) x[e] = b[e] * dinv[e / k];
+}
+
+// Per-column dot a.b over n rows of k columns (FP64), through fin(c, t).
+template <int KP, class Fin>
+__global__ void __launch_bounds__(256)
+k_block_dot(long n, int k, const double* __restrict__ a, const double* __restrict__ b,
+            ReduceSlot rsl, Fin fin) {
+    constexpr int RPW = 32 / KP;
+    const int lane = threadIdx.x & 31;
+    const int c = lane % KP, sub = lane / KP;
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    double t = 0.0;
+    if (c < k)
+        for (long i = gwarp * RPW + sub; i < n; i += nwarps * RPW) t += a[i * k + c] * b[i * k + c];
+    block_reduce_cols<KP>(t, k, rsl, fin);
+}
+
+// Coarsest level, k right-hand sides: one CTA per column.
+template <typename T>
+__global__ void k_lu_solve_block(int n, int k, const double* __restrict__ lu,
+                                 const int* __restrict__ piv, const T* __restrict__ b,
+                                 T* __restrict__ x) {
+    extern __shared__ double y[];
+    const int c = blockIdx.x;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)b[(long)i * k + c];
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int q = 0; q < n; q++) {
+            const int p = piv[q];
+            if (p != q) { double t = y[q]; y[q] = y[p]; y[p] = t; }
+        }
+    __syncthreads();
+    for (int j = 0; j < n; j++) {
+        const double yj = y[j];
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) y[i] -= lu[i + (size_t)j * n] * yj;
+        __syncthreads();
+    }
+    for (int j = n - 1; j >= 0; j--) {
+        if (threadIdx.x == 0) y[j] /= lu[j + (size_t)j * n];
+        __syncthreads();
+        const double yj = y[j];
+        for (int i = threadIdx.x; i < j; i += blockDim.x) y[i] -= lu[i + (size_t)j * n] * yj;
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x[(long)i * k + c] = (T)y[i];
+}
+
+// ------------------------------------------------------------ launchers --
+inline int pow2_at_least(int k) {
+    int p = 1;
+    while (p < k) p <<= 1;
+    return p;
+}
+
+inline unsigned block_grid(long n, int KP, int S) {
+    const long rows_per_warp = 32 / (KP * S);
+    long warps = (n + rows_per_warp - 1) / rows_per_warp;
+    long blocks = (warps * 32 + 255) / 256;
+    long cap = std::min<long>((long)sm_count() * 16, 65536 / kMaxBlockK);
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return (unsigned)blocks;
+}
+
+#define RB_BLOCK_KP_SWITCH(KP, ...)                     \
+    switch (KP) {                                       \
+        case 2: { constexpr int kKP = 2; __VA_ARGS__; } break;   \
+        case 4: { constexpr int kKP = 4; __VA_ARGS__; } break;   \
+        case 8: { constexpr int kKP = 8; __VA_ARGS__; } break;   \
+        case 16: { constexpr int kKP = 16; __VA_ARGS__; } break; \
+        default: { constexpr int kKP = 32; __VA_ARGS__; } break; \
+    }
+
+// CSR SpMM with tile shape (KP from k, S rows splits).
+template <typename TV, typename TX, class Epi>
+void launch_csr_block(const int* rp, const int* ci, const TV* cv, long n, int k, const TX* X,
+                      Epi epi, int S) {
+    if (n <= 0) return;
+    using Acc = typename AccOf<TV>::type;
+    const int KP = pow2_at_least(k);
+    if (KP * S > 32) S = 32 / KP;
+    const unsigned g = block_grid(n, KP, S);
+    RB_BLOCK_KP_SWITCH(KP, {
+        if constexpr (kKP <= 8) {
+            if (S >= 4) k_csr_block<kKP, 4, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+            else if (S == 2) k_csr_block<kKP, 2, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+            else k_csr_block<kKP, 1, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+        } else if constexpr (kKP == 16) {
+            if (S >= 2) k_csr_block<16, 2, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+            else k_csr_block<16, 1, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+        } else {
+            k_csr_block<32, 1, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+        }
+    });
+    RB_CHECK_LAUNCH();
+}
+
+template <typename TV, class Fin>
+void launch_csr_block_dot(const int* rp, const int* ci, const TV* cv, long n, int k,
+                          const double* P, double* Y, int S, Fin fin) {
+    const int KP = pow2_at_least(k);
+    if (KP * S > 32) S = 32 / KP;
+    const unsigned g = block_grid(n, KP, S);
+    ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+    RB_BLOCK_KP_SWITCH(KP, {
+        if constexpr (kKP <= 8) {
+            if (S >= 4) k_csr_block_dot<kKP, 4, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+            else if (S == 2) k_csr_block_dot<kKP, 2, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+            else k_csr_block_dot<kKP, 1, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+        } else if constexpr (kKP == 16) {
+            if (S >= 2) k_csr_block_dot<16, 2, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+            else k_csr_block_dot<16, 1, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+        } else {
+            k_csr_block_dot<32, 1, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+        }
+    });
+    RB_CHECK_LAUNCH();
+}
+
+template <typename TV, typename TX, class Epi>
+void launch_dia_block(const DiaOff& off, const TV* sv, long n, int k, const TX* X, Epi epi) {
+    if (n <= 0) return;
+    using Acc = typename AccOf<TV>::type;
+    const int KP = pow2_at_least(k);
+    const unsigned g = block_grid(n, KP, 1);
+    RB_BLOCK_KP_SWITCH(KP, {
+        switch (off.nd) {
+            case 7: k_sdia_block<7, kKP, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, off, sv, X, epi); break;
+            case 27: k_sdia_block<27, kKP, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, off, sv, X, epi); break;
+            default: k_sdia_block<0, kKP, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, off, sv, X, epi); break;
+        }
+    });
+    RB_CHECK_LAUNCH();
+}
+
+template <typename TV, class Fin>
+void launch_dia_block_dot(const DiaOff& off, const TV* sv, long n, int k, const double* P,
+                          double* Y, Fin fin) {
+    const int KP = pow2_at_least(k);
+    const unsigned g = block_grid(n, KP, 1);
+    ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+    RB_BLOCK_KP_SWITCH(KP, {
+        switch (off.nd) {
+            case 7: k_sdia_block_dot<7, kKP, TV><<<g, 256, 0, stream()>>>(n, k, off, sv, P, Y, rs, fin); break;
+            case 27: k_sdia_block_dot<27, kKP, TV><<<g, 256, 0, stream()>>>(n, k, off, sv, P, Y, rs, fin); break;
+            default: k_sdia_block_dot<0, kKP, TV><<<g, 256, 0, stream()>>>(n, k, off, sv, P, Y, rs, fin); break;
+        }
+    });
+    RB_CHECK_LAUNCH();
+}
+
+template <class Fin>
+void launch_block_dot(long n, int k, const double* a, const double* b, Fin fin) {
+    const int KP = pow2_at_least(k);
+    const unsigned g = block_grid(n, KP, 1);
+    ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+    RB_BLOCK_KP_SWITCH(KP, { k_block_dot<kKP><<<g, 256, 0, stream()>>>(n, k, a, b, rs, fin); });
+    RB_CHECK_LAUNCH();
+}
+
+}  // namespace rb

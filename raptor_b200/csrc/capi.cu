@@ -738,6 +738,44 @@ int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, in
     });
 }
 
+int rb_amg_cycle_block(rb_amg ml, rb_vec X, rb_vec B, int k) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(X); NEED(B);
+        const long long n = ml->h.master[0].A->n_rows;
+        RB_REQUIRE(k >= 2 && k <= 32, "block cycle: k must be in 2..32");
+        RB_REQUIRE((long long)X->n == n * k && (long long)B->n == n * k,
+                   "block cycle: X and B must hold n * k entries");
+        RB_REQUIRE(ml->h.opts.relax_type == RB_RELAX_JACOBI ||
+                       ml->h.opts.relax_type == RB_RELAX_L1JACOBI,
+                   "block cycle: the smoother must be Jacobi or L1-Jacobi");
+        ml->h.cycle_block(X->v.get(), B->v.get(), k);
+        return RB_OK;
+    });
+}
+
+int rb_pcg_block(rb_csr A, rb_amg ml, rb_vec X, rb_vec B, int k, double tol, int max_iter,
+                 int* iters, double* relres) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(ml); NEED(X); NEED(B); NEED(iters); NEED(relres);
+        RB_REQUIRE(k >= 1 && k <= 32, "block PCG: k must be in 1..32");
+        RB_REQUIRE((long long)X->n == (long long)A->n_cols * k &&
+                       (long long)B->n == (long long)A->n_rows * k,
+                   "block PCG: X and B must hold n * k entries");
+        if (k == 1) {
+            // one column: the single-vector PCG in true-residual mode
+            const long mi = max_iter > 0 ? max_iter : (long)(1.3 * A->n_rows) + 2;
+            std::vector<double> h((size_t)mi + 2);
+            int nh = 0;
+            int rc = ml->h.pcg(*A, X->v.get(), B->v.get(), tol, max_iter, RB_PCG_TRUE_RESIDUAL,
+                               h.data(), (int)h.size(), &nh);
+            iters[0] = std::max(nh - 1, 0);
+            relres[0] = nh > 0 ? h[std::min(nh, (int)h.size()) - 1] : 0.0;
+            return rc;
+        }
+        return ml->h.pcg_block(*A, X->v.get(), B->v.get(), k, tol, max_iter, iters, relres);
+    });
+}
+
 int rb_cg(rb_csr A, rb_vec x, rb_vec b, double tol, int max_iter, double* hist, int cap,
           int* n_hist) {
     return guarded([&]() -> int {

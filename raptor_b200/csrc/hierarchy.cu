@@ -101,12 +101,6 @@ void Level<T>::alloc_vectors() {
 // When RAPTOR_B200_TUNE_CACHE names a file, decisions are read from it and
 // new ones appended, so later runs (a profiled run in particular, whose
 // timings are distorted) reuse the choices of an undisturbed one.
-namespace {
-struct TuneCache {
-    std::map<std::string, int> m;
-    bool loaded = false;
-    std::string path;
-};
 TuneCache& tune_cache() {
     static TuneCache c;
     if (!c.loaded) {
@@ -140,25 +134,6 @@ std::string tune_key(const char* op, long n, long long nnz, int vbytes) {
     char b[128];
     snprintf(b, sizeof(b), "%s:%ld:%lld:%d", op, n, nnz, vbytes);
     return b;
-}
-}  // namespace
-
-// Milliseconds of 3 back-to-back launches of fn after one warm-up launch.
-template <class F>
-static float time_launch(F&& fn) {
-    cudaEvent_t e0, e1;
-    RB_CUDA(cudaEventCreate(&e0));
-    RB_CUDA(cudaEventCreate(&e1));
-    fn();
-    RB_CUDA(cudaEventRecord(e0, stream()));
-    for (int rep = 0; rep < 3; rep++) fn();
-    RB_CUDA(cudaEventRecord(e1, stream()));
-    RB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    RB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return ms;
 }
 
 // Time the row kernel for each group width and keep the fastest.

@@ -14,6 +14,37 @@
 
 namespace rb {
 
+// Autotuner decisions keyed by operator, size and value width (persisted
+// when RAPTOR_B200_TUNE_CACHE names a file).
+struct TuneCache {
+    std::map<std::string, int> m;
+    bool loaded = false;
+    std::string path;
+};
+TuneCache& tune_cache();
+void tune_save();
+std::string tune_key(const char* op, long n, long long nnz, int vbytes);
+
+// Milliseconds of 3 back-to-back launches of fn after one warm-up launch.
+template <class F>
+float time_launch(F&& fn) {
+    cudaEvent_t e0, e1;
+    RB_CUDA(cudaEventCreate(&e0));
+    RB_CUDA(cudaEventCreate(&e1));
+    fn();
+    RB_CUDA(cudaEventRecord(e0, stream()));
+    for (int rep = 0; rep < 3; rep++) fn();
+    RB_CUDA(cudaEventRecord(e1, stream()));
+    RB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    RB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ms;
+}
+
+struct BlockState;   // k right-hand-side buffers and tile shapes (block.cu)
+
 // FP64 result of setup for one level (multilevel/par_level.hpp:15-43).
 struct MasterLevel {
     std::unique_ptr<rb_csr_s> A;   // diagonal first
@@ -118,6 +149,14 @@ struct Hierarchy {
     int pcg(const rb_csr_s& A, double* x, const double* b, double tol, int max_iter, int mode,
             double* hist, int cap, int* n_hist);
     size_t device_bytes() const;
+
+    // k right-hand sides at once (block.cu): X and B are n x k blocks, entry
+    // (i, c) at i * k + c; per-column CG scalars, one shared hierarchy.
+    std::shared_ptr<BlockState> blk;
+    BlockState& block_state(int k);
+    void cycle_block(double* Z, const double* B, int k);
+    int pcg_block(const rb_csr_s& A, double* X, const double* B, int k, double tol, int max_iter,
+                  int* iters, double* relres);
 };
 
 int krylov_cg(const rb_csr_s& A, double* x, const double* b, double tol, int max_iter,
