@@ -34,6 +34,7 @@ typedef enum rb_status {
 typedef struct rb_csr_s* rb_csr;   /* device CSR matrix, FP64 values, int32 indices */
 typedef struct rb_vec_s* rb_vec;   /* device FP64 vector */
 typedef struct rb_amg_s* rb_amg;   /* AMG hierarchy (ParMultilevel) */
+typedef struct rb_batch_s* rb_batch; /* independent systems solved together */
 
 /* Description of the last failure on this thread ("" when none). */
 const char* rb_last_error(void);
@@ -241,6 +242,29 @@ int rb_residual_norm_noalloc(int n_rows, const int* rowptr, const int* cols, con
  * n_hist receives the entry count. */
 int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, int mode,
            double* hist, int cap, int* n_hist);
+/* ------------------------------------------------- batches of systems */
+/* An uneven batch of independent systems (no counterpart in the reference).
+ * Each matrix gets the hierarchy rb_amg_setup would build for it alone; the
+ * levels are packed block-diagonally so one V-cycle of the batch is one
+ * launch per operation for all systems, and rb_batch_pcg replays a whole
+ * iteration of all systems from one CUDA graph, with per-system CG scalars
+ * and stopping tests.  Vectors of a batch are the systems' vectors
+ * concatenated in order (rb_batch_offsets gives the first row of each). */
+int rb_batch_setup(int n_sys, const rb_csr* mats, const rb_amg_opts* opts, rb_batch* out);
+int rb_batch_destroy(rb_batch B);
+/* number of systems, total rows, levels of the packed hierarchy */
+int rb_batch_info(rb_batch B, int* n_sys, int64_t* total_rows, int* levels);
+/* offsets[n_sys + 1] (first row of each system, then the total) and the
+ * levels of each system's own hierarchy (levels[n_sys]); either may be NULL */
+int rb_batch_offsets(rb_batch B, int64_t* offsets, int* levels);
+/* x = M b: one V-cycle of every system from a zero guess */
+int rb_batch_cycle(rb_batch B, rb_vec x, rb_vec b);
+/* Preconditioned CG per system in true-residual mode; iters[n_sys] and
+ * relres[n_sys] receive each system's iterations and final true relative
+ * residual.  RB_ERR_NOT_CONVERGED if any system did not reach tol. */
+int rb_batch_pcg(rb_batch B, rb_vec x, rb_vec b, double tol, int max_iter, int* iters,
+                 double* relres);
+
 /* One V-cycle from a zero guess applied to k columns at once, X = M B
  * (columns interleaved by row, n * k entries each; k in 2..32; Jacobi or
  * L1-Jacobi smoothing).  No counterpart in the reference. */

@@ -460,6 +460,51 @@ class ParSmoothedAggregationSolver(ParMultilevel):
         self.opts.prolong_weight = prolong_weight
 
 
+class Batch:
+    """An uneven batch of independent systems solved together: each matrix
+    gets the hierarchy a standalone setup would build, and every V-cycle
+    operation runs once for all systems (rb_batch_* in the C ABI).  Vectors
+    are the systems' vectors concatenated (`offsets`)."""
+
+    def __init__(self, matrices, ml=None):
+        self.matrices = list(matrices)
+        opts = ml.opts if ml is not None else None
+        if opts is None:
+            opts = AmgOpts()
+            lib().rb_amg_default_opts(C.byref(opts))
+        arr = (C.c_void_p * len(self.matrices))(*[m.h.value for m in self.matrices])
+        h = C.c_void_p()
+        check(lib().rb_batch_setup(len(self.matrices), arr, C.byref(opts), C.byref(h)))
+        self.h = h
+        n = len(self.matrices)
+        self.offsets = np.zeros(n + 1, np.int64)
+        self.levels = np.zeros(n, np.int32)
+        check(lib().rb_batch_offsets(self.h, self.offsets.ctypes.data, self.levels.ctypes.data))
+        self.n_sys = n
+        self.total_rows = int(self.offsets[-1])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().rb_batch_destroy(self.h)
+            except Exception:  # noqa: BLE001 - interpreter shutdown
+                pass
+            self.h = None
+
+    def cycle(self, x, b):
+        check(lib().rb_batch_cycle(self.h, x.h, b.h))
+
+    def pcg(self, x, b, tol=1e-8, max_iter=-1):
+        """Per-system PCG to tol (true relative residual); returns
+        (status, iters[n_sys], relres[n_sys])."""
+        iters = np.zeros(self.n_sys, np.int32)
+        relres = np.zeros(self.n_sys, np.float64)
+        rc = lib().rb_batch_pcg(self.h, x.h, b.h, float(tol), int(max_iter), iters, relres)
+        if rc not in (0, -5):
+            check(rc)
+        return rc, iters, relres
+
+
 # Krylov -------------------------------------------------------------------
 def _hist_call(fn, cap):
     hist = np.zeros(cap)

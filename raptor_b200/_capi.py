@@ -110,6 +110,12 @@ SIGNATURES = {
     "rb_residual_norm_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "rb_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rb_pcg": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_batch_setup": (C.c_int, [C.c_int, _P, _P, _PP]),
+    "rb_batch_destroy": (C.c_int, [_P]),
+    "rb_batch_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+    "rb_batch_offsets": (C.c_int, [_P, _P, _P]),
+    "rb_batch_cycle": (C.c_int, [_P, _P, _P]),
+    "rb_batch_pcg": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _I, _D]),
     "rb_amg_cycle_block": (C.c_int, [_P, _P, _P, C.c_int]),
     "rb_pcg_block": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_double, C.c_int, _I, _D]),
     "rb_cg": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),

@@ -738,6 +738,71 @@ int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, in
     });
 }
 
+int rb_batch_setup(int n_sys, const rb_csr* mats, const rb_amg_opts* opts, rb_batch* out) {
+    return guarded([&]() -> int {
+        NEED(mats); NEED(out);
+        RB_REQUIRE(n_sys >= 1, "batch: no systems");
+        for (int s = 0; s < n_sys; s++) RB_REQUIRE(mats[s] != nullptr, "batch: NULL matrix");
+        rb_amg_opts o;
+        if (opts) o = *opts;
+        else rb_amg_default_opts(&o);
+        RB_REQUIRE(o.solver == RB_SOLVER_RS || o.solver == RB_SOLVER_SA, "unknown solver");
+        std::vector<const rb_csr_s*> m(mats, mats + n_sys);
+        *out = batch_setup(n_sys, m.data(), o);
+        return RB_OK;
+    });
+}
+
+int rb_batch_destroy(rb_batch B) {
+    return guarded([&]() -> int {
+        batch_destroy(B);
+        return RB_OK;
+    });
+}
+
+int rb_batch_info(rb_batch B, int* n_sys, int64_t* total_rows, int* levels) {
+    return guarded([&]() -> int {
+        NEED(B);
+        const int n = batch_num_systems(B);
+        if (n_sys) *n_sys = n;
+        if (total_rows) *total_rows = batch_offset(B, n);
+        if (levels) *levels = batch_packed_levels(B);
+        return RB_OK;
+    });
+}
+
+int rb_batch_offsets(rb_batch B, int64_t* offsets, int* levels) {
+    return guarded([&]() -> int {
+        NEED(B);
+        const int n = batch_num_systems(B);
+        for (int s = 0; s <= n; s++)
+            if (offsets) offsets[s] = batch_offset(B, s);
+        for (int s = 0; s < n; s++)
+            if (levels) levels[s] = batch_levels(B, s);
+        return RB_OK;
+    });
+}
+
+int rb_batch_cycle(rb_batch B, rb_vec x, rb_vec b) {
+    return guarded([&]() -> int {
+        NEED(B); NEED(x); NEED(b);
+        const long long N = batch_offset(B, batch_num_systems(B));
+        RB_REQUIRE(x->n == N && b->n == N, "batch cycle: vector sizes do not match");
+        batch_cycle(B, x->v.get(), b->v.get());
+        return RB_OK;
+    });
+}
+
+int rb_batch_pcg(rb_batch B, rb_vec x, rb_vec b, double tol, int max_iter, int* iters,
+                 double* relres) {
+    return guarded([&]() -> int {
+        NEED(B); NEED(x); NEED(b); NEED(iters); NEED(relres);
+        const long long N = batch_offset(B, batch_num_systems(B));
+        RB_REQUIRE(x->n == N && b->n == N, "batch PCG: vector sizes do not match");
+        return batch_pcg(B, x->v.get(), b->v.get(), tol, max_iter, iters, relres);
+    });
+}
+
 int rb_amg_cycle_block(rb_amg ml, rb_vec X, rb_vec B, int k) {
     return guarded([&]() -> int {
         NEED(ml); NEED(X); NEED(B);

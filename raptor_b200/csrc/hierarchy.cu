@@ -291,7 +291,8 @@ static void build_dia(Level<T>& V, const rb_csr_s& M, const DiaOff& off) {
 }
 
 // ------------------------------------------------------------------ setup --
-void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* weights_host) {
+void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* weights_host,
+                      bool cycle_data) {
     opts = o;
     use_graphs = o.use_graphs != 0;
     src_A = &Af;
@@ -370,7 +371,7 @@ void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* we
     }
     RB_CUDA(cudaStreamSynchronize(stream()));
     setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    build_cycle_data();
+    if (cycle_data) build_cycle_data();
 }
 
 template <typename T>
@@ -622,15 +623,6 @@ void Hierarchy::smooth(Level<T>& V, T*& cur, T*& other, const T* b, bool x_zero)
     }
 }
 
-// y = x + P xc written to a second buffer (prolongation that also moves the
-// iterate to the buffer the post-smoother should start from)
-template <typename TY>
-struct EpiAddTo {
-    const TY* x0;
-    TY* y;
-    template <typename A>
-    __device__ void operator()(long i, A s, double&) const { y[i] = (TY)((A)x0[i] + s); }
-};
 
 template <typename T>
 void Hierarchy::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool x_zero) {
@@ -1233,5 +1225,7 @@ int krylov_bicgstab(const rb_csr_s& A, Hierarchy* ml, double* x, const double* b
 
 template void Hierarchy::build_levels<double>(std::vector<Level<double>>&);
 template void Hierarchy::build_levels<float>(std::vector<Level<float>>&);
+template void Hierarchy::smooth<double>(Level<double>&, double*&, double*&, const double*, bool);
+template void Hierarchy::smooth<float>(Level<float>&, float*&, float*&, const float*, bool);
 
 }  // namespace rb

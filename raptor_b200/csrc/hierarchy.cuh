@@ -115,7 +115,9 @@ struct Hierarchy {
     int last_iters = 0;
 
     ~Hierarchy();
-    void setup(const rb_csr_s& A, const rb_amg_opts& o, const double* weights_host);
+    // cycle_data = false builds the FP64 levels only (a member of a batch)
+    void setup(const rb_csr_s& A, const rb_amg_opts& o, const double* weights_host,
+               bool cycle_data = true);
     void build_cycle_data();
     template <typename T>
     void build_levels(std::vector<Level<T>>& lv);

@@ -10,6 +10,8 @@ struct rb_csr_s {
     rb::DevArray<double> vals;
 };
 
+struct rb_batch_s;
+
 struct rb_vec_s {
     int n = 0;
     rb::DevArray<double> v;
@@ -66,6 +68,17 @@ int aggregate(const rb_csr_s& A, const rb_csr_s& S, const int* states_dev, int* 
 rb_csr_s* fit_candidates(int n, int n_aggs, const int* agg_dev, const double* B_dev,
                          double* R_dev);
 rb_csr_s* jacobi_prolongation(const rb_csr_s& A, const rb_csr_s& T, double omega, int steps);
+
+// Batches of independent systems (batch.cu).
+rb_batch_s* batch_setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o);
+void batch_destroy(rb_batch_s* B);
+int batch_num_systems(const rb_batch_s* B);
+long long batch_offset(const rb_batch_s* B, int s);
+int batch_levels(const rb_batch_s* B, int s);
+int batch_packed_levels(const rb_batch_s* B);
+void batch_cycle(rb_batch_s* B, double* x, const double* b);
+int batch_pcg(rb_batch_s* B, double* x, const double* b, double tol, int max_iter, int* iters,
+              double* relres);
 
 // glibc rand() weights of the reference (par_multilevel.hpp:215-225).
 std::vector<double> rand_weights(int n, int first_row);

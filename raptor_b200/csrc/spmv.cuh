@@ -87,6 +87,16 @@ struct EpiAppend {
     __device__ void operator()(long i, A s, double&) const { y[i] = (TY)((A)y[i] + s); }
 };
 
+// y = x + P xc written to a second buffer (prolongation that also moves the
+// iterate to the buffer the post-smoother should start from)
+template <typename TY>
+struct EpiAddTo {
+    const TY* x0;
+    TY* y;
+    template <typename A>
+    __device__ void operator()(long i, A s, double&) const { y[i] = (TY)((A)x0[i] + s); }
+};
+
 // Jacobi / L1-Jacobi: xn = xo + dinv (b - A xo); dinv already holds w/d_i.
 template <typename TX, typename TB, typename TY>
 struct EpiJacobi {
