@@ -68,8 +68,8 @@ int rb_csr_transpose(rb_csr A, rb_csr* out);
 int rb_vec_create(int n, rb_vec* out);
 int rb_vec_destroy(rb_vec v);
 int rb_vec_size(rb_vec v, int* n);
-int rb_vec_upload(rb_vec v, const double* host);
-int rb_vec_download(rb_vec v, double* host);
+int rb_vec_upload(rb_vec v, const double* host);   /* host or device source */
+int rb_vec_download(rb_vec v, double* host);       /* host or device destination */
 int rb_vec_set(rb_vec v, double value);          /* ParVector::set_const_value */
 int rb_vec_device_ptr(rb_vec v, double** ptr);
 int rb_vec_copy(rb_vec dst, rb_vec src);         /* ParVector::copy */
@@ -242,6 +242,29 @@ int rb_residual_norm_noalloc(int n_rows, const int* rowptr, const int* cols, con
  * n_hist receives the entry count. */
 int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, int mode,
            double* hist, int cap, int* n_hist);
+/* --------------------------------------------------- differentiation */
+/* Finite-volume assembly of -div(k grad u) on an nx x ny grid of unit cells
+ * (cell c = y nx + x), homogeneous Dirichlet walls: face transmissibility
+ * 2 k_i k_j / (k_i + k_j) between cells, 2 k_i to a wall; rows sorted by
+ * column.  k is a device array of nx ny conductivities.  No counterpart in
+ * the reference. */
+int rb_fv_assemble(int nx, int ny, const double* k, rb_csr* A);
+/* Backward of rb_fv_assemble: gk (device, nx ny) = dL/dk from gA (device,
+ * one entry per stored entry of A) = dL/dA. */
+int rb_fv_backward(int nx, int ny, const double* k, rb_csr A, const double* gA, double* gk);
+/* SDDMM on A's pattern: out_j = scale lambda_i x_col(j) for every stored
+ * entry j of row i (device arrays).  With scale = -1, lambda the adjoint
+ * and x the primal solution this is dL/dA for x = A^-1 b. */
+int rb_sddmm(rb_csr A, const double* lambda, const double* x, double scale, double* out);
+/* A^T lambda = g through the hierarchy ml built for A: PCG when A is
+ * symmetric (the transposed V-cycle is then the V-cycle itself), else
+ * BiCGStab with the transposed cycle (A_l^T on every level, the same P and
+ * R and smoother diagonals, Jacobi or L1-Jacobi smoothing).  lambda starts
+ * from zero; iters and relres (may be NULL) receive the iterations and the
+ * final true relative residual ||g - A^T lambda|| / ||g||. */
+int rb_adjoint_solve(rb_csr A, rb_amg ml, rb_vec lambda, rb_vec g, double tol, int max_iter,
+                     int* iters, double* relres);
+
 /* ------------------------------------------------- batches of systems */
 /* An uneven batch of independent systems (no counterpart in the reference).
  * Each matrix gets the hierarchy rb_amg_setup would build for it alone; the

@@ -584,3 +584,6 @@ def init(device=0):
 
 def version():
     return lib().rb_version().decode()
+
+
+from . import autograd  # noqa: E402,F401  (torch is imported only when used)

@@ -110,6 +110,10 @@ SIGNATURES = {
     "rb_residual_norm_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "rb_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rb_pcg": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_fv_assemble": (C.c_int, [C.c_int, C.c_int, _P, _PP]),
+    "rb_fv_backward": (C.c_int, [C.c_int, C.c_int, _P, _P, _P, _P]),
+    "rb_sddmm": (C.c_int, [_P, _P, _P, C.c_double, _P]),
+    "rb_adjoint_solve": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "rb_batch_setup": (C.c_int, [C.c_int, _P, _P, _PP]),
     "rb_batch_destroy": (C.c_int, [_P]),
     "rb_batch_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int)]),

@@ -208,10 +208,13 @@ int rb_vec_size(rb_vec v, int* n) {
     });
 }
 
+// host or device source/destination (unified addressing decides the copy)
 int rb_vec_upload(rb_vec v, const double* host) {
     return guarded([&]() -> int {
         NEED(v); NEED(host);
-        v->v.upload(host, v->n);
+        if (v->n)
+            RB_CUDA(cudaMemcpyAsync(v->v.get(), host, sizeof(double) * v->n, cudaMemcpyDefault,
+                                    stream()));
         RB_CUDA(cudaStreamSynchronize(stream()));
         return RB_OK;
     });
@@ -220,7 +223,9 @@ int rb_vec_upload(rb_vec v, const double* host) {
 int rb_vec_download(rb_vec v, double* host) {
     return guarded([&]() -> int {
         NEED(v); NEED(host);
-        v->v.download(host, v->n);
+        if (v->n)
+            RB_CUDA(cudaMemcpyAsync(host, v->v.get(), sizeof(double) * v->n, cudaMemcpyDefault,
+                                    stream()));
         RB_CUDA(cudaStreamSynchronize(stream()));
         return RB_OK;
     });
@@ -592,19 +597,6 @@ int rb_amg_level_info(rb_amg ml, int level, int* n_rows, int64_t* nnz_A, int64_t
     });
 }
 
-static rb_csr_s* clone_csr(const rb_csr_s& M) {
-    rb_csr_s* C = new_csr(M.n_rows, M.n_cols, M.nnz);
-    RB_CUDA(cudaMemcpyAsync(C->rowptr.get(), M.rowptr.get(), sizeof(int) * ((size_t)M.n_rows + 1),
-                            cudaMemcpyDeviceToDevice, stream()));
-    if (M.nnz) {
-        RB_CUDA(cudaMemcpyAsync(C->cols.get(), M.cols.get(), sizeof(int) * M.nnz,
-                                cudaMemcpyDeviceToDevice, stream()));
-        RB_CUDA(cudaMemcpyAsync(C->vals.get(), M.vals.get(), sizeof(double) * M.nnz,
-                                cudaMemcpyDeviceToDevice, stream()));
-    }
-    return C;
-}
-
 int rb_amg_level_matrix(rb_amg ml, int level, int which, rb_csr* out) {
     return guarded([&]() -> int {
         NEED(ml); NEED(out);
@@ -735,6 +727,41 @@ int rb_pcg(rb_csr A, rb_amg ml, rb_vec x, rb_vec b, double tol, int max_iter, in
                            hist ? cap : 0, &nh);
         if (n_hist) *n_hist = nh;
         return rc;
+    });
+}
+
+int rb_fv_assemble(int nx, int ny, const double* k, rb_csr* A) {
+    return guarded([&]() -> int {
+        NEED(k); NEED(A);
+        ensure_device();
+        *A = fv_assemble(nx, ny, k);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_fv_backward(int nx, int ny, const double* k, rb_csr A, const double* gA, double* gk) {
+    return guarded([&]() -> int {
+        NEED(k); NEED(A); NEED(gA); NEED(gk);
+        fv_backward(nx, ny, k, *A, gA, gk);
+        return RB_OK;
+    });
+}
+
+int rb_sddmm(rb_csr A, const double* lambda, const double* x, double scale, double* out) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(lambda); NEED(x); NEED(out);
+        sddmm(*A, lambda, x, scale, out);
+        return RB_OK;
+    });
+}
+
+int rb_adjoint_solve(rb_csr A, rb_amg ml, rb_vec lambda, rb_vec g, double tol, int max_iter,
+                     int* iters, double* relres) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(ml); NEED(lambda); NEED(g);
+        RB_REQUIRE(lambda->n == A->n_rows && g->n == A->n_rows, "adjoint: sizes do not match");
+        return adjoint_solve(*A, ml->h, lambda->v.get(), g->v.get(), tol, max_iter, iters, relres);
     });
 }
 

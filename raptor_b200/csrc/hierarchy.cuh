@@ -154,6 +154,13 @@ struct Hierarchy {
 
     // k right-hand sides at once (block.cu): X and B are n x k blocks, entry
     // (i, c) at i * k + c; per-column CG scalars, one shared hierarchy.
+    // adjoint solves (adjoint.cu): symmetry of the last operator checked, and
+    // for a nonsymmetric one the hierarchy of the transposed cycle
+    const rb_csr_s* adj_A = nullptr;
+    bool adj_sym = false;
+    std::unique_ptr<Hierarchy> adj;
+    std::unique_ptr<rb_csr_s> adj_AT;
+
     std::shared_ptr<BlockState> blk;
     BlockState& block_state(int k);
     void cycle_block(double* Z, const double* B, int k);
@@ -165,6 +172,9 @@ int krylov_cg(const rb_csr_s& A, double* x, const double* b, double tol, int max
               double* hist, int cap, int* n_hist);
 int krylov_bicgstab(const rb_csr_s& A, Hierarchy* ml, double* x, const double* b, double tol,
                     int max_iter, double* hist, int cap, int* n_hist);
+// A^T lambda = g through the hierarchy built for A (adjoint.cu)
+int adjoint_solve(const rb_csr_s& A, Hierarchy& H, double* lambda, const double* g, double tol,
+                  int max_iter, int* iters, double* relres);
 
 }  // namespace rb
 

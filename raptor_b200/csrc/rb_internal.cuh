@@ -37,6 +37,7 @@ inline CsrView<double> view(const rb_csr_s& A) {
 }
 
 rb_csr_s* new_csr(int n_rows, int n_cols, long long nnz);
+rb_csr_s* clone_csr(const rb_csr_s& M);
 // Sort every row by column and move the diagonal to the front.
 void sort_rows_diag_first(rb_csr_s& A, bool diag_first);
 // Transpose; rows of the result list source rows in increasing order.
@@ -79,6 +80,13 @@ int batch_packed_levels(const rb_batch_s* B);
 void batch_cycle(rb_batch_s* B, double* x, const double* b);
 int batch_pcg(rb_batch_s* B, double* x, const double* b, double tol, int max_iter, int* iters,
               double* relres);
+
+// Differentiation form (adjoint.cu).
+rb_csr_s* fv_assemble(int nx, int ny, const double* k_dev);
+void fv_backward(int nx, int ny, const double* k_dev, const rb_csr_s& A, const double* gA,
+                 double* gk);
+void sddmm(const rb_csr_s& A, const double* lambda, const double* x, double scale, double* out);
+bool is_symmetric(const rb_csr_s& A, double tol);
 
 // glibc rand() weights of the reference (par_multilevel.hpp:215-225).
 std::vector<double> rand_weights(int n, int first_row);

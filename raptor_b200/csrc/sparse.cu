@@ -127,6 +127,20 @@ void sort_rows_diag_first(rb_csr_s& A, bool diag_first) {
     RB_CHECK_LAUNCH();
 }
 
+// Deep copy on the device.
+rb_csr_s* clone_csr(const rb_csr_s& M) {
+    rb_csr_s* C = new_csr(M.n_rows, M.n_cols, M.nnz);
+    RB_CUDA(cudaMemcpyAsync(C->rowptr.get(), M.rowptr.get(), sizeof(int) * ((size_t)M.n_rows + 1),
+                            cudaMemcpyDeviceToDevice, stream()));
+    if (M.nnz) {
+        RB_CUDA(cudaMemcpyAsync(C->cols.get(), M.cols.get(), sizeof(int) * M.nnz,
+                                cudaMemcpyDeviceToDevice, stream()));
+        RB_CUDA(cudaMemcpyAsync(C->vals.get(), M.vals.get(), sizeof(double) * M.nnz,
+                                cudaMemcpyDeviceToDevice, stream()));
+    }
+    return C;
+}
+
 // ------------------------------------------------------------ transpose --
 __global__ void k_count_cols(long long nnz, const int* __restrict__ cols, int* cnt) {
     long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
