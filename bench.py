@@ -53,6 +53,8 @@ def parse():
                    help="grid side of the k right-hand-side workload (0 skips it)")
     p.add_argument("--systems", type=int, default=64,
                    help="independent systems of the uneven batch (0 skips it)")
+    p.add_argument("--diff-size", type=int, default=512,
+                   help="grid side of the differentiation workload (0 skips it)")
     return p.parse_args()
 
 
@@ -314,6 +316,50 @@ def run_uneven_batch(rb, ev, sync, count=64, steps=2):
             "max_true_rel_res": float(max(relres))}
 
 
+def run_differentiation(rb, ev, sync, side=512, steps=3):
+    """Forward and backward of x = A(k)^-1 b through the torch.autograd
+    harness: 5-point finite-volume diffusion with harmonic-mean faces on a
+    side^2 grid, k = exp(g) with g a Gaussian random field (correlation
+    length 32 cells, unit variance), L = 0.5 ||x - x_t||^2; FP32 V-cycle,
+    FP64 outer PCG and adjoint PCG to 1e-8."""
+    import torch
+    from raptor_b200 import autograd as AG
+
+    n = side * side
+    g = torch.tensor(AG.grf(side, side, 32.0, seed=SEED), dtype=torch.float64, device="cuda")
+    rng = np.random.default_rng(SEED + 5)
+    b = torch.tensor(rng.uniform(-1.0, 1.0, n), dtype=torch.float64, device="cuda")
+    xt = torch.tensor(rng.uniform(0.0, 1.0, n), dtype=torch.float64, device="cuda")
+    fwd, bwd = [], []
+    for s in range(1 + steps):
+        gg = g.clone().requires_grad_(True)
+        bb = b.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x = AG.DiffusionSolve.apply(torch.exp(gg), bb, side, side, TOL, 500, rb.FP32)
+        loss = 0.5 * ((x - xt) ** 2).sum()
+        e1.record()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        sync()
+        if s >= 1:
+            fwd.append(e0.elapsed_time(e1))
+            bwd.append(e1.elapsed_time(e2))
+    return {"workload": "FV diffusion %d^2, harmonic-mean faces, k = exp(GRF, corr 32, var 1); "
+                        "L = 0.5||x - x_t||^2; forward AMG-PCG + adjoint AMG-PCG, SDDMM, assembly "
+                        "backward (RS PMIS extended+i, L1-Jacobi, FP32 V-cycle, FP64 outer, 1e-8)"
+                        % side,
+            "rows": n, "forward_ms": sum(fwd) / len(fwd), "backward_ms": sum(bwd) / len(bwd),
+            "forward_includes": "assembly, AMG setup, PCG",
+            "backward_includes": "adjoint PCG, SDDMM, assembly backward",
+            "grad_g_norm": float(gg.grad.norm()), "grad_b_norm": float(bb.grad.norm())}
+
+
 def run_b200(args, rank, world, local):
     import raptor_b200 as rb
 
@@ -495,6 +541,9 @@ def run_b200(args, rank, world, local):
     if args.systems > 0:
         out["uneven_batch"] = run_uneven_batch(rb, ev, lambda: rb.lib().rb_synchronize(),
                                                args.systems)
+    if args.diff_size > 0:
+        out["differentiation"] = run_differentiation(rb, ev, lambda: rb.lib().rb_synchronize(),
+                                                     args.diff_size)
     if rank == 0 and args.cpu_sample > 0:
         out["cpu_baseline"] = cpu_baseline(args.cpu_sample, S, iters32[-1])
     dist.close()
