@@ -202,7 +202,9 @@ int rb_amg_cycle_profile(rb_amg ml, double* ms, int cap, int* n_out);
 /* Average milliseconds per launch of one cycle operator over reps launches:
  * op 0 residual with A_l, 1 restriction with R_l, 2 prolongation with P_l,
  * 3 Jacobi sweep with A_l (all in the cycle precision), 4 the outer FP64
- * A p fused with p.Ap on the finest level. */
+ * A p fused with p.Ap on the finest level, 5 one whole preconditioner
+ * V-cycle z = M r from a zero guess replayed from its CUDA graph (level is
+ * ignored). */
 int rb_amg_time_operator(rb_amg ml, int level, int op, int reps, double* ms_per_launch);
 /* Wall time of the last rb_amg_setup (seconds) and the autotuner's choices
  * for level l: lanes per row of A_l (0 when A_l is stored by diagonals),

@@ -326,7 +326,7 @@ template <typename TV, typename TX, class Epi>
 void launch_csr_block(const int* rp, const int* ci, const TV* cv, long n, int k, const TX* X,
                       Epi epi, int S) {
     if (n <= 0) return;
-    using Acc = typename AccOf<TV>::type;
+    using Acc = AccOf2<TV, TX>;
     const int KP = pow2_at_least(k);
     if (KP * S > 32) S = 32 / KP;
     const unsigned g = block_grid(n, KP, S);
@@ -370,7 +370,7 @@ void launch_csr_block_dot(const int* rp, const int* ci, const TV* cv, long n, in
 template <typename TV, typename TX, class Epi>
 void launch_dia_block(const DiaOff& off, const TV* sv, long n, int k, const TX* X, Epi epi) {
     if (n <= 0) return;
-    using Acc = typename AccOf<TV>::type;
+    using Acc = AccOf2<TV, TX>;
     const int KP = pow2_at_least(k);
     const unsigned g = block_grid(n, KP, 1);
     RB_BLOCK_KP_SWITCH(KP, {

@@ -658,7 +658,7 @@ int rb_amg_cycle_profile(rb_amg ml, double* ms, int cap, int* n_out) {
 int rb_amg_time_operator(rb_amg ml, int level, int op, int reps, double* ms_per_launch) {
     return guarded([&]() -> int {
         NEED(ml); NEED(ms_per_launch);
-        RB_REQUIRE(op >= 0 && op <= 4, "unknown operator");
+        RB_REQUIRE(op >= 0 && op <= 5, "unknown operator");
         *ms_per_launch = ml->h.time_operator(level, op, reps);
         return RB_OK;
     });

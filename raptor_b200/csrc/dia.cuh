@@ -89,7 +89,7 @@ inline unsigned dia_grid(long n) {
 template <typename TV, typename TX, class Epi>
 void launch_dia(const DiaOff& off, const TV* sv, long n, const TX* x, Epi epi) {
     if (n <= 0) return;
-    using Acc = typename AccOf<TV>::type;
+    using Acc = AccOf2<TV, TX>;
     const unsigned g = dia_grid(n);
     switch (off.nd) {
         case 5: k_sdia_rows<5, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;

@@ -81,6 +81,12 @@ k_mc_sweep(int nrows, const int* __restrict__ rows, const int* __restrict__ rp,
     }
 }
 
+// flag[0] = 1 if some value does not survive a round trip through FP32
+__global__ void k_fp32_exact(long long nnz, const double* __restrict__ v, int* flag) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < nnz && (double)(float)v[j] != v[j]) *flag = 1;
+}
+
 // --------------------------------------------------------------- helpers --
 template <typename T>
 static void launch_vec(void (*k)(long, T*, T), long n, T* x, T v) {
@@ -468,6 +474,13 @@ void Hierarchy::build_cycle_data() {
     if (opts.precision == RB_PREC_FP32) {
         build_levels(lv32);
         build_fused(lv32, fdesc32);
+        const rb_csr_s& A0 = *master[0].A;
+        DevArray<int> flag(1);
+        flag.zero();
+        if (A0.nnz)
+            k_fp32_exact<<<grid_for(A0.nnz, 256), 256, 0, stream()>>>(A0.nnz, A0.vals.get(), flag.get());
+        RB_CHECK_LAUNCH();
+        a0_fp32_exact = read_scalar(flag.get()) == 0;
     } else {
         build_levels(lv64);
         build_fused(lv64, fdesc64);
@@ -766,6 +779,26 @@ static double time_op_impl(Hierarchy& H, std::vector<Level<T>>& lv, int l, int o
 
 double Hierarchy::time_operator(int level, int op, int reps) {
     RB_REQUIRE(reps > 0, "reps must be positive");
+    if (op == 5) {
+        // one preconditioner application z = M r from a zero guess, replayed
+        // from its CUDA graph as the Krylov loops run it
+        const int n = master[0].A->n_rows;
+        launch_vec<double>(k_fill<double>, n, kr.get(), 1.0);
+        auto launch = [&]() { cycle(kz.get(), kr.get(), true); };
+        launch();
+        cudaEvent_t e0, e1;
+        RB_CUDA(cudaEventCreate(&e0));
+        RB_CUDA(cudaEventCreate(&e1));
+        RB_CUDA(cudaEventRecord(e0, stream()));
+        for (int r = 0; r < reps; r++) launch();
+        RB_CUDA(cudaEventRecord(e1, stream()));
+        RB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        RB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return ms / reps;
+    }
     if (op == 4) {
         const rb_csr_s& A = *master[0].A;
         KScal* S = scal.get();
@@ -863,6 +896,42 @@ void Hierarchy::cycle(double* x, const double* b, bool x_zero) {
     run_graph(pkey(x_zero ? "cyc0" : "cyc", x, b), [&] { cycle64(x, b, x_zero); });
 }
 
+// ------------------------------------------------ FP32-form PCG fusions --
+// x += alpha p ; r -= alpha Ap ; rr = r.r, and the FP32 copy of r that the
+// V-cycle takes as its right-hand side (saves the separate conversion pass)
+template <class Fin>
+__global__ void __launch_bounds__(256)
+k_cg_update_f32(long n, double* __restrict__ x, double* __restrict__ r,
+                const double* __restrict__ p, const double* __restrict__ Ap,
+                const KScal* __restrict__ s, float* __restrict__ r32, ReduceSlot rs, Fin fin) {
+    const double alpha = s->alpha;
+    double t = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        x[i] += p[i] * alpha;
+        const double ri = r[i] + Ap[i] * (-1.0 * alpha);
+        r[i] = ri;
+        r32[i] = (float)ri;
+        t += ri * ri;
+    }
+    block_reduce_finish(t, rs, fin);
+}
+
+// z = (double) x32 fused with r.z (the V-cycle's output conversion)
+template <class Fin>
+__global__ void __launch_bounds__(256)
+k_convert_dot(long n, const float* __restrict__ x32, const double* __restrict__ r,
+              double* __restrict__ z, ReduceSlot rs, Fin fin) {
+    double t = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        const double zi = (double)x32[i];
+        z[i] = zi;
+        t += r[i] * zi;
+    }
+    block_reduce_finish(t, rs, fin);
+}
+
 // ------------------------------------------------------------ reductions --
 namespace {
 struct FinPAp {
@@ -958,6 +1027,23 @@ void Hierarchy::outer_apply(const rb_csr_s& A, bool lowprec, const double* p, do
     launch_rows_dot(A.rowptr.get(), A.cols.get(), A.vals.get(), n, p, Ap, G, fin);
 }
 
+// r = b - A x in FP64 for the outer iteration: from the hierarchy's copy of
+// A_0 when it holds A's exact values in a cheaper format (the FP32 copy of
+// an FP32-exact matrix, or the FP64 sliced diagonals), else from A's CSR.
+void Hierarchy::true_residual(const rb_csr_s& A, const double* x, const double* b, double* r) {
+    if (is_finest(A)) {
+        if (opts.precision == RB_PREC_FP32 && a0_fp32_exact) {
+            lv32[0].apply_A(x, EpiResidual<double, double>{b, r});
+            return;
+        }
+        if (opts.precision == RB_PREC_FP64 && lv64[0].dia) {
+            lv64[0].apply_A(x, EpiResidual<double, double>{b, r});
+            return;
+        }
+    }
+    residual64(view(A), x, b, r);
+}
+
 // -------------------------------------------------------------------- PCG --
 // PCG (krylov/par_cg.cpp:121-263).  The iteration body is one CUDA graph:
 // Ap = A p fused with p.Ap (alpha computed on the device), x += alpha p with
@@ -982,16 +1068,18 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
         nh++;
     };
     RB_CUDA(cudaMemsetAsync(S, 0, sizeof(KScal), stream()));
-    // b.Mb (par_cg.cpp:150-161)
-    cycle(z, b, true);
-    dot_into(b, z, n, &S->tmp);
-    const double b_inner = read_scal().tmp;
-    const double norm_b = std::sqrt(b_inner);
+    // b.Mb (par_cg.cpp:150-161), the reference mode's stopping scale
+    double b_inner = 1.0, tol_ref = tol;
+    if (mode == RB_PCG_REFERENCE) {
+        cycle(z, b, true);
+        dot_into(b, z, n, &S->tmp);
+        b_inner = read_scal().tmp;
+        const double norm_b = std::sqrt(b_inner);
+        if (norm_b > 1e-16) tol_ref = tol * norm_b;
+    }
     const double bb = norm64(b, n);
-    double tol_ref = tol;
-    if (norm_b > 1e-16) tol_ref = tol * norm_b;
     // r0 = b - A x0 ; z = M r ; p = z ; rz = r.z
-    residual64(Av, x, b, r);
+    true_residual(A, x, b, r);
     cycle(z, r, true);
     RB_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
     dot_into(r, z, n, &S->rz);
@@ -1004,22 +1092,40 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
         return RB_OK;
     }
     const unsigned rg = red_grid(n);
+    const bool fp32 = opts.precision == RB_PREC_FP32;
     auto body = [&](bool full_r) {
         // Ap = A p ; p.Ap ; alpha = rz / pAp.  In the FP32 form A p reads
         // the FP32 copy of A_0 with FP64 accumulation; the FP64 residual
         // replacement below keeps the recurrence tied to the FP64 operator.
         outer_apply(A, lowprec, p, Ap, FinPAp{S});
         // x += alpha p ; r -= alpha Ap (or r = b - A x every 8th iteration)
-        k_cg_update<<<rg, 256, 0, stream()>>>(n, x, r, p, Ap, S, full_r ? 0 : 1,
-                                              global_reduce_slot(rg), FinSetRR{S});
+        if (fp32 && !full_r) {
+            // the update also writes the cycle's FP32 right-hand side
+            k_cg_update_f32<<<rg, 256, 0, stream()>>>(n, x, r, p, Ap, S, lv32[0].b.get(),
+                                                      global_reduce_slot(rg), FinSetRR{S});
+        } else {
+            k_cg_update<<<rg, 256, 0, stream()>>>(n, x, r, p, Ap, S, full_r ? 0 : 1,
+                                                  global_reduce_slot(rg), FinSetRR{S});
+        }
         RB_CHECK_LAUNCH();
         if (full_r) {
-            residual64(Av, x, b, r);
+            true_residual(A, x, b, r);
             dot_into(r, r, n, &S->rr);
         }
         // z = M r ; rz_new = r.z ; beta
-        cycle64(z, r, true);
-        k_dot_fin<<<rg, 256, 0, stream()>>>(r, z, n, global_reduce_slot(rg), FinRZ{S});
+        if (fp32) {
+            Level<float>& V = lv32[0];
+            if (full_r) {
+                k_convert<float, double><<<grid_for(n, 256), 256, 0, stream()>>>(n, r, V.b.get());
+                RB_CHECK_LAUNCH();
+            }
+            cycle_level(lv32, 0, V.x.get(), V.b.get(), true);
+            k_convert_dot<<<rg, 256, 0, stream()>>>(n, V.x.get(), r, z, global_reduce_slot(rg),
+                                                    FinRZ{S});
+        } else {
+            cycle64(z, r, true);
+            k_dot_fin<<<rg, 256, 0, stream()>>>(r, z, n, global_reduce_slot(rg), FinRZ{S});
+        }
         RB_CHECK_LAUNCH();
     };
     int iter = 0;
@@ -1042,7 +1148,7 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
             done = std::sqrt(hs.rr) <= tol * bb;
             if (done) {
                 // confirm with the true residual
-                residual64(Av, x, b, r);
+                true_residual(A, x, b, r);
                 dot_into(r, r, n, &S->rr);
                 double tr = std::sqrt(read_scal().rr);
                 if (nh - 1 < cap) hist[nh - 1] = tr / (bb > 0 ? bb : 1.0);

@@ -111,6 +111,11 @@ struct Hierarchy {
         return &A == master[0].A.get() ||
                (&A == src_A && A.nnz == master[0].A->nnz && A.n_rows == master[0].A->n_rows);
     }
+    // every value of A_0 is exactly representable in FP32: the FP32 copy of
+    // A_0 (FP64 accumulation) then is the operator itself, and residuals of
+    // the outer iteration read it instead of the FP64 CSR matrix
+    bool a0_fp32_exact = false;
+    void true_residual(const rb_csr_s& A, const double* x, const double* b, double* r);
     double setup_seconds = 0;
     int last_iters = 0;
 

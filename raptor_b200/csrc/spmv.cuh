@@ -10,6 +10,8 @@
 // goes through the read-only path, and partial sums meet in a shuffle tree.
 #pragma once
 
+#include <type_traits>
+
 #include "rb_common.cuh"
 
 namespace rb {
@@ -18,6 +20,10 @@ constexpr int kRowBlock = 256;
 
 template <typename T> struct AccOf { using type = T; };
 template <> struct AccOf<float> { using type = float; };
+// Accumulator of a row product: the wider of the value and vector types
+// (FP32 values against FP64 vectors accumulate in FP64).
+template <typename TV, typename TX>
+using AccOf2 = typename std::conditional<(sizeof(TX) > sizeof(TV)), TX, TV>::type;
 
 // Block-level tree reduction followed by a fixed-order reduction of the block
 // partials by the last block to finish; the result is bit-reproducible for a
@@ -131,7 +137,7 @@ template <int G, typename TV, typename TX, class Epi>
 __global__ void __launch_bounds__(kRowBlock)
 k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
            const TV* __restrict__ cv, const TX* __restrict__ x, Epi epi) {
-    using Acc = typename AccOf<TV>::type;
+    using Acc = AccOf2<TV, TX>;
     constexpr int RPW = 32 / G;
     const int lane = threadIdx.x & 31;
     const int sub = lane / G, gl = lane & (G - 1);
