@@ -75,7 +75,11 @@ def dist_env():
 
 
 class Dist:
-    def __init__(self, world, local):
+    """Replica bookkeeping across ranks: a barrier and the max of a scalar.
+    NCCL on GPUs (one rank per GPU), gloo on CPU; rendezvous from the
+    torchrun environment (MASTER_ADDR / MASTER_PORT)."""
+
+    def __init__(self, world, local, backend=None):
         self.world = world
         self.pg = None
         if world > 1:
@@ -83,8 +87,12 @@ class Dist:
 
             import torch
             import torch.distributed as td
-            torch.cuda.set_device(local)
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            self.device = "cuda" if backend == "nccl" else "cpu"
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.td = td
             self.torch = torch
 
@@ -95,7 +103,7 @@ class Dist:
     def max(self, v):
         if self.world == 1:
             return v
-        t = self.torch.tensor([float(v)], device="cuda")
+        t = self.torch.tensor([float(v)], device=self.device)
         self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
         return float(t.item())
 
