@@ -256,6 +256,11 @@ def spgemm(A, B):
     return CSR(lib().oc_spgemm(A.ptr, B.ptr))
 
 
+def spgemm_T(P, B):
+    """P^T B with P's columns walked in increasing row order (matmult.cpp:139-204)."""
+    return CSR(lib().oc_spgemm_T(P.ptr, B.ptr))
+
+
 def rap(A, P, diag_first=True):
     return CSR(lib().oc_rap(A.ptr, P.ptr, 1 if diag_first else 0))
 
