@@ -18,6 +18,17 @@ namespace rb {
 
 constexpr int kRowBlock = 256;
 
+// Register budget of the CSR row kernels (minimum resident blocks per SM;
+// 0 leaves the choice to the compiler).
+#ifndef RB_ROWS_MINB
+#define RB_ROWS_MINB 0
+#endif
+#if RB_ROWS_MINB > 0
+#define RB_ROWS_BOUNDS __launch_bounds__(kRowBlock, RB_ROWS_MINB)
+#else
+#define RB_ROWS_BOUNDS __launch_bounds__(kRowBlock)
+#endif
+
 template <typename T> struct AccOf { using type = T; };
 template <> struct AccOf<float> { using type = float; };
 // Accumulator of a row product: the wider of the value and vector types
@@ -134,7 +145,7 @@ struct NoFinish {
 
 // ------------------------------------------------------------- kernels --
 template <int G, typename TV, typename TX, class Epi>
-__global__ void __launch_bounds__(kRowBlock)
+__global__ void RB_ROWS_BOUNDS
 k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
            const TV* __restrict__ cv, const TX* __restrict__ x, Epi epi) {
     using Acc = AccOf2<TV, TX>;
@@ -171,7 +182,7 @@ k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
 }
 
 template <int G, typename TV, class Fin>
-__global__ void __launch_bounds__(kRowBlock)
+__global__ void RB_ROWS_BOUNDS
 k_csr_rows_dot(long n, const int* __restrict__ rp, const int* __restrict__ ci,
                const TV* __restrict__ cv, const double* __restrict__ x, EpiStoreDot epi,
                ReduceSlot rs, Fin fin) {

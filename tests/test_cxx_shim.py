@@ -45,6 +45,7 @@ def test_shim_solves_on_the_gpu(tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     fields = r.stdout.split()
     relres = float(fields[fields.index("relres") + 1])
-    assert relres < 1e-6   # the reference's r.z criterion at tol 1e-8
+    # the reference's PCG stops on r.z < tol sqrt(b.Mb), not on ||r|| / ||b||
+    assert relres < 1e-4
     last = float(fields[fields.index("last") + 1])
     assert last <= 1e-8
