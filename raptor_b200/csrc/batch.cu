@@ -90,6 +90,25 @@ __global__ void k_lu_solve_batch(const int* __restrict__ row0, const int* __rest
     for (int i = threadIdx.x; i < n; i += blockDim.x) x[r0 + i] = (T)y[i];
 }
 
+// x = inv b for each listed system's coarsest level (one CTA per system;
+// inverses column-major)
+template <typename T>
+__global__ void k_coarse_mv_batch(const int* __restrict__ row0, const int* __restrict__ nrow,
+                                  const long long* __restrict__ ioff, const double* __restrict__ inv_all,
+                                  const T* __restrict__ b, T* __restrict__ x) {
+    extern __shared__ double bs[];
+    const int n = nrow[blockIdx.x];
+    const long r0 = row0[blockIdx.x];
+    const double* inv = inv_all + ioff[blockIdx.x];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) bs[i] = (double)b[r0 + i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < n; j++) s += inv[(size_t)j * n + i] * bs[j];
+        x[r0 + i] = (T)s;
+    }
+}
+
 // Segmented dot: one CTA per chunk writes its partial; then one thread per
 // system sums that system's chunks in order.  Deterministic.
 __global__ void __launch_bounds__(256)
@@ -185,7 +204,7 @@ struct Batch {
     std::vector<std::vector<long long>> off;      // off[l][s], n_sys + 1 entries
     Hierarchy cat;                                // packed levels
     // coarsest-level LUs
-    DevArray<double> lu;
+    DevArray<double> lu, inv;   // inv: coarse inverses when every coarsest level is small
     DevArray<int> piv;
     struct CoarseTab {
         int count = 0, max_n = 0;
@@ -219,8 +238,12 @@ struct Batch {
     void coarse_solve(int l, const T* b, T* x) {
         CoarseTab& t = coarse[l];
         if (!t.count) return;
-        k_lu_solve_batch<T><<<t.count, 256, sizeof(double) * std::max(t.max_n, 1), stream()>>>(
-            t.row0.get(), t.n.get(), t.luo.get(), t.pivo.get(), lu.get(), piv.get(), b, x);
+        if (inv.get())
+            k_coarse_mv_batch<T><<<t.count, 256, sizeof(double) * std::max(t.max_n, 1), stream()>>>(
+                t.row0.get(), t.n.get(), t.luo.get(), inv.get(), b, x);
+        else
+            k_lu_solve_batch<T><<<t.count, 256, sizeof(double) * std::max(t.max_n, 1), stream()>>>(
+                t.row0.get(), t.n.get(), t.luo.get(), t.pivo.get(), lu.get(), piv.get(), b, x);
         RB_CHECK_LAUNCH();
     }
 
@@ -337,6 +360,19 @@ void Batch::setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o) {
         RB_CHECK_LAUNCH();
         k_lu_factor<<<1, 256, 0, stream()>>>(nc, lu.get() + luo[s], piv.get() + pivo[s], info.get());
         RB_CHECK_LAUNCH();
+    }
+    int nc_max = 0;
+    for (int s = 0; s < n; s++) nc_max = std::max(nc_max, sys[s]->master[depth[s] - 1].A->n_rows);
+    if (nc_max <= kCoarseInvMax) {
+        inv.alloc((size_t)std::max(lu_tot, 1LL));
+        for (int s = 0; s < n; s++) {
+            const int nc = sys[s]->master[depth[s] - 1].A->n_rows;
+            if (!nc) continue;
+            k_lu_invert<<<1, 256, sizeof(double) * nc, stream()>>>(nc, lu.get() + luo[s],
+                                                                  piv.get() + pivo[s],
+                                                                  inv.get() + luo[s]);
+            RB_CHECK_LAUNCH();
+        }
     }
     coarse.clear();
     coarse.resize(Lmax);

@@ -194,4 +194,55 @@ __global__ void k_lu_solve(int n, const double* __restrict__ lu, const int* __re
     for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (T)y[i];
 }
 
+// Coarse levels of up to kCoarseInvMax rows are solved by one dense product
+// with the inverse of the factored matrix (built once at setup from the LU,
+// column by column): a coarse solve then needs one read of the inverse and
+// no sequential substitution steps.
+constexpr int kCoarseInvMax = 512;
+
+// inv (column-major, n x n) = the inverse of the matrix factored in lu/piv.
+static __global__ void k_lu_invert(int n, const double* __restrict__ lu, const int* __restrict__ piv,
+                                   double* __restrict__ inv) {
+    extern __shared__ double y[];
+    for (int c = 0; c < n; c++) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (i == c) ? 1.0 : 0.0;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int k = 0; k < n; k++) {
+                const int p = piv[k];
+                if (p != k) { double t = y[k]; y[k] = y[p]; y[p] = t; }
+            }
+        __syncthreads();
+        for (int j = 0; j < n; j++) {
+            const double yj = y[j];
+            for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) y[i] -= lu[i + (size_t)j * n] * yj;
+            __syncthreads();
+        }
+        for (int j = n - 1; j >= 0; j--) {
+            if (threadIdx.x == 0) y[j] /= lu[j + (size_t)j * n];
+            __syncthreads();
+            const double yj = y[j];
+            for (int i = threadIdx.x; i < j; i += blockDim.x) y[i] -= lu[i + (size_t)j * n] * yj;
+            __syncthreads();
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) inv[(size_t)c * n + i] = y[i];
+        __syncthreads();
+    }
+}
+
+// x = inv b for column blockIdx.x of k interleaved columns (k = 1: a vector)
+template <typename T>
+__global__ void k_coarse_mv(int n, const double* __restrict__ inv, int k, const T* __restrict__ b,
+                            T* __restrict__ x) {
+    extern __shared__ double bs[];
+    const int c = blockIdx.x;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) bs[i] = (double)b[(long)i * k + c];
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < n; j++) s += inv[(size_t)j * n + i] * bs[j];
+        x[(long)i * k + c] = (T)s;
+    }
+}
+
 }  // namespace rb

@@ -206,7 +206,10 @@ void block_cycle_level(Hierarchy& H, std::vector<Level<T>>& lv, std::vector<BLev
                        T* X, const T* B, bool x_zero, int k) {
     const int L = (int)lv.size();
     if (l == L - 1) {
-        if (H.coarse_n)
+        if (H.coarse_n && H.cinv.get())
+            k_coarse_mv<T><<<k, 256, sizeof(double) * H.coarse_n, stream()>>>(H.coarse_n,
+                                                                              H.cinv.get(), k, B, X);
+        else if (H.coarse_n)
             k_lu_solve_block<T><<<k, 256, sizeof(double) * H.coarse_n, stream()>>>(
                 H.coarse_n, k, H.lu.get(), H.piv.get(), B, X);
         RB_CHECK_LAUNCH();

@@ -471,6 +471,13 @@ void Hierarchy::build_cycle_data() {
         k_lu_factor<<<1, 256, 0, stream()>>>(coarse_n, lu.get(), piv.get(), info.get());
         RB_CHECK_LAUNCH();
     }
+    cinv.release();
+    if (coarse_n > 0 && coarse_n <= kCoarseInvMax) {
+        cinv.alloc((size_t)coarse_n * coarse_n);
+        k_lu_invert<<<1, 256, sizeof(double) * coarse_n, stream()>>>(coarse_n, lu.get(), piv.get(),
+                                                                       cinv.get());
+        RB_CHECK_LAUNCH();
+    }
     if (opts.precision == RB_PREC_FP32) {
         build_levels(lv32);
         build_fused(lv32, fdesc32);
@@ -643,7 +650,10 @@ void Hierarchy::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, 
     const int L = (int)lv.size();
     if (l == L - 1) {
         mark(l * kProfSlots + 6);
-        if (coarse_n)
+        if (coarse_n && cinv.get())
+            k_coarse_mv<T><<<1, 256, sizeof(double) * coarse_n, stream()>>>(coarse_n, cinv.get(), 1,
+                                                                            b, x);
+        else if (coarse_n)
             k_lu_solve<T><<<1, 256, sizeof(double) * coarse_n, stream()>>>(coarse_n, lu.get(),
                                                                           piv.get(), b, x);
         RB_CHECK_LAUNCH();

@@ -84,6 +84,7 @@ struct Hierarchy {
     std::vector<Level<float>> lv32;
     int coarse_n = 0;
     DevArray<double> lu;
+    DevArray<double> cinv;   // inverse of the coarse matrix (coarse_n <= kCoarseInvMax)
     DevArray<int> piv;
     // Krylov work vectors (finest size) and device scalars
     DevArray<double> kr, kz, kp, kAp, ks, kAs, krs, kph, ksh;
