@@ -19,6 +19,26 @@ namespace rb {
 
 constexpr int kMaxBlockK = 32;
 
+// Tuning knobs of the block kernels (loads in flight against occupancy).
+// Measured on the SA 160^3 k = 8 / 32 solves: one row group per warp step
+// for the diagonal kernels (U = 4 rows: 12.6 / 10.7 ms per right-hand side,
+// U = 1: 10.4 / 7.6), 4-way unrolled CSR rows (9.7 / 7.05 against 2-way),
+// and the compiler's register choice (2 blocks per SM: 11.6 / 9.9).
+#ifndef RB_BLOCK_DIA_U
+#define RB_BLOCK_DIA_U 1
+#endif
+#ifndef RB_BLOCK_CSR_UNROLL
+#define RB_BLOCK_CSR_UNROLL 4
+#endif
+#ifndef RB_BLOCK_MINB
+#define RB_BLOCK_MINB 0
+#endif
+#if RB_BLOCK_MINB > 0
+#define RB_BLOCK_BOUNDS __launch_bounds__(256, RB_BLOCK_MINB)
+#else
+#define RB_BLOCK_BOUNDS __launch_bounds__(256)
+#endif
+
 // ----------------------------------------------------------- epilogues --
 template <typename TY>
 struct BStore {
@@ -131,6 +151,20 @@ k_csr_block(long n, int k, const int* __restrict__ rp, const int* __restrict__ c
         if (row < n && c < k) {
             const int rs = __ldg(rp + row), re = __ldg(rp + row + 1);
             int j = rs + s;
+#if RB_BLOCK_CSR_UNROLL >= 4
+            for (; j + 3 * S < re; j += 4 * S) {
+                const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + S);
+                const int c2 = __ldg(ci + j + 2 * S), c3 = __ldg(ci + j + 3 * S);
+                const TV v0 = __ldg(cv + j), v1 = __ldg(cv + j + S);
+                const TV v2 = __ldg(cv + j + 2 * S), v3 = __ldg(cv + j + 3 * S);
+                const TX x0 = __ldg(X + (long)c0 * k + c), x1 = __ldg(X + (long)c1 * k + c);
+                const TX x2 = __ldg(X + (long)c2 * k + c), x3 = __ldg(X + (long)c3 * k + c);
+                acc += (Acc)v0 * (Acc)x0;
+                acc += (Acc)v1 * (Acc)x1;
+                acc += (Acc)v2 * (Acc)x2;
+                acc += (Acc)v3 * (Acc)x3;
+            }
+#else
             for (; j + S < re; j += 2 * S) {
                 const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + S);
                 const TV v0 = __ldg(cv + j), v1 = __ldg(cv + j + S);
@@ -138,7 +172,8 @@ k_csr_block(long n, int k, const int* __restrict__ rp, const int* __restrict__ c
                 acc += (Acc)v0 * (Acc)x0;
                 acc += (Acc)v1 * (Acc)x1;
             }
-            if (j < re) acc += (Acc)__ldg(cv + j) * (Acc)__ldg(X + (long)__ldg(ci + j) * k + c);
+#endif
+            for (; j < re; j += S) acc += (Acc)__ldg(cv + j) * (Acc)__ldg(X + (long)__ldg(ci + j) * k + c);
         }
 #pragma unroll
         for (int o = KP; o < KP * S; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -164,13 +199,17 @@ k_csr_block_dot(long n, int k, const int* __restrict__ rp, const int* __restrict
         if (row < n && c < k) {
             const int rs = __ldg(rp + row), re = __ldg(rp + row + 1);
             int j = rs + s;
-            for (; j + S < re; j += 2 * S) {
+            for (; j + 3 * S < re; j += 4 * S) {
                 const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + S);
+                const int c2 = __ldg(ci + j + 2 * S), c3 = __ldg(ci + j + 3 * S);
                 const double x0 = __ldg(P + (long)c0 * k + c), x1 = __ldg(P + (long)c1 * k + c);
+                const double x2 = __ldg(P + (long)c2 * k + c), x3 = __ldg(P + (long)c3 * k + c);
                 acc += (double)__ldg(cv + j) * x0;
                 acc += (double)__ldg(cv + j + S) * x1;
+                acc += (double)__ldg(cv + j + 2 * S) * x2;
+                acc += (double)__ldg(cv + j + 3 * S) * x3;
             }
-            if (j < re) acc += (double)__ldg(cv + j) * __ldg(P + (long)__ldg(ci + j) * k + c);
+            for (; j < re; j += S) acc += (double)__ldg(cv + j) * __ldg(P + (long)__ldg(ci + j) * k + c);
         }
 #pragma unroll
         for (int o = KP; o < KP * S; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -183,59 +222,115 @@ k_csr_block_dot(long n, int k, const int* __restrict__ rp, const int* __restrict
 }
 
 // ---------------------------------------------------- sliced DIA SpMM --
+// A warp step covers U groups of 32 / KP consecutive rows; every value and
+// gathered x of the step is loaded before the first product.
+template <int ND>
+struct DiaUnroll {
+    static constexpr int U = (ND > 0 && ND <= 9) ? RB_BLOCK_DIA_U : 1;
+};
+
 template <int ND, int KP, typename TV, typename TX, typename Acc, class Epi>
-__global__ void __launch_bounds__(256)
+__global__ void RB_BLOCK_BOUNDS
 k_sdia_block(long n, int k, DiaOff off, const TV* __restrict__ sv, const TX* __restrict__ X,
              Epi epi) {
     constexpr int RPW = 32 / KP;
+    constexpr int U = DiaUnroll<ND>::U;
     const int nd = ND > 0 ? ND : off.nd;
     const int lane = threadIdx.x & 31;
     const int c = lane % KP, sub = lane / KP;
     const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
-    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
-        const long i = base + sub;
-        if (i >= n || c >= k) continue;
-        const TV* a = sv + (i >> 5) * nd * 32 + (i & 31);
-        Acc acc = 0;
+    for (long base = gwarp * RPW * U; base < n; base += nwarps * RPW * U) {
         if constexpr (ND > 0) {
+            TV av[U][ND];
+            TX xv[U][ND];
 #pragma unroll
-            for (int d = 0; d < ND; d++) {
-                const long j = i + off.o[d];
-                if (j >= 0 && j < n) acc += (Acc)__ldg(a + d * 32) * (Acc)__ldg(X + j * k + c);
+            for (int u = 0; u < U; u++) {
+                const long i = base + u * RPW + sub;
+                const bool ok = i < n && c < k;
+                const TV* a = sv + (i >> 5) * ND * 32 + (i & 31);
+#pragma unroll
+                for (int d = 0; d < ND; d++) {
+                    const long j = i + off.o[d];
+                    const bool in = ok && j >= 0 && j < n;
+                    av[u][d] = in ? __ldg(a + d * 32) : TV(0);
+                    xv[u][d] = in ? __ldg(X + j * k + c) : TX(0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const long i = base + u * RPW + sub;
+                if (i >= n || c >= k) continue;
+                Acc acc = 0;
+#pragma unroll
+                for (int d = 0; d < ND; d++) acc += (Acc)av[u][d] * (Acc)xv[u][d];
+                epi(i, c, k, acc);
             }
         } else {
+            const long i = base + sub;
+            if (i >= n || c >= k) continue;
+            const TV* a = sv + (i >> 5) * nd * 32 + (i & 31);
+            Acc acc = 0;
             for (int d = 0; d < nd; d++) {
                 const long j = i + off.o[d];
                 if (j >= 0 && j < n) acc += (Acc)__ldg(a + d * 32) * (Acc)__ldg(X + j * k + c);
             }
+            epi(i, c, k, acc);
         }
-        epi(i, c, k, acc);
     }
 }
 
 template <int ND, int KP, typename TV, class Fin>
-__global__ void __launch_bounds__(256)
+__global__ void RB_BLOCK_BOUNDS
 k_sdia_block_dot(long n, int k, DiaOff off, const TV* __restrict__ sv,
                  const double* __restrict__ P, double* __restrict__ Y, ReduceSlot rsl, Fin fin) {
     constexpr int RPW = 32 / KP;
+    constexpr int U = DiaUnroll<ND>::U;
     const int nd = ND > 0 ? ND : off.nd;
     const int lane = threadIdx.x & 31;
     const int c = lane % KP, sub = lane / KP;
     const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
     double red = 0.0;
-    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
-        const long i = base + sub;
-        if (i >= n || c >= k) continue;
-        const TV* a = sv + (i >> 5) * nd * 32 + (i & 31);
-        double acc = 0;
-        for (int d = 0; d < (ND > 0 ? ND : nd); d++) {
-            const long j = i + off.o[d];
-            if (j >= 0 && j < n) acc += (double)__ldg(a + d * 32) * __ldg(P + j * k + c);
+    for (long base = gwarp * RPW * U; base < n; base += nwarps * RPW * U) {
+        if constexpr (ND > 0) {
+            TV av[U][ND];
+            double xv[U][ND];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const long i = base + u * RPW + sub;
+                const bool ok = i < n && c < k;
+                const TV* a = sv + (i >> 5) * ND * 32 + (i & 31);
+#pragma unroll
+                for (int d = 0; d < ND; d++) {
+                    const long j = i + off.o[d];
+                    const bool in = ok && j >= 0 && j < n;
+                    av[u][d] = in ? __ldg(a + d * 32) : TV(0);
+                    xv[u][d] = in ? __ldg(P + j * k + c) : 0.0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const long i = base + u * RPW + sub;
+                if (i >= n || c >= k) continue;
+                double acc = 0;
+#pragma unroll
+                for (int d = 0; d < ND; d++) acc += (double)av[u][d] * xv[u][d];
+                Y[i * k + c] = acc;
+                red += P[i * k + c] * acc;
+            }
+        } else {
+            const long i = base + sub;
+            if (i >= n || c >= k) continue;
+            const TV* a = sv + (i >> 5) * nd * 32 + (i & 31);
+            double acc = 0;
+            for (int d = 0; d < nd; d++) {
+                const long j = i + off.o[d];
+                if (j >= 0 && j < n) acc += (double)__ldg(a + d * 32) * __ldg(P + j * k + c);
+            }
+            Y[i * k + c] = acc;
+            red += P[i * k + c] * acc;
         }
-        Y[i * k + c] = acc;
-        red += P[i * k + c] * acc;
     }
     block_reduce_cols<KP>(red, k, rsl, fin);
 }
