@@ -455,7 +455,7 @@ void Batch::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool
     T* other = V.xt.get();
     cat.smooth(V, cur, other, b, x_zero);
     V.apply_A(cur, EpiResidual<T, T>{b, V.r.get()});
-    launch_rows(V.R.rowptr, V.R.cols, V.R.vals, C.n, V.R.nnz, V.r.get(), EpiStore<T>{C.b.get()},
+    rows_op(V.R, V.R16, C.n, V.r.get(), EpiStore<T>{C.b.get()},
                 V.gR);
     cycle_level(lv, l + 1, C.x.get(), C.b.get(), true);
     const int rt = opts.relax_type;
@@ -463,9 +463,9 @@ void Batch::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool
     T* start = x;
     if (jt && (opts.num_smooth_sweeps & 1)) start = (x == V.xt.get()) ? x : V.xt.get();
     if (cur == start) {
-        launch_rows(V.P.rowptr, V.P.cols, V.P.vals, V.n, V.P.nnz, C.x.get(), EpiAppend<T>{cur}, V.gP);
+        rows_op(V.P, V.P16, V.n, C.x.get(), EpiAppend<T>{cur}, V.gP);
     } else {
-        launch_rows(V.P.rowptr, V.P.cols, V.P.vals, V.n, V.P.nnz, C.x.get(),
+        rows_op(V.P, V.P16, V.n, C.x.get(),
                     EpiAddTo<T>{cur, start}, V.gP);
         cur = start;
     }

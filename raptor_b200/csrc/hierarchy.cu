@@ -8,6 +8,7 @@
 // l1 row norms, a multicolour row ordering for the Gauss-Seidel stand-in, the
 // row-kernel width chosen by timing, and the LU of A_c^T.
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cmath>
 #include <map>
@@ -85,6 +86,30 @@ k_mc_sweep(int nrows, const int* __restrict__ rows, const int* __restrict__ rp,
 __global__ void k_fp32_exact(long long nnz, const double* __restrict__ v, int* flag) {
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j < nnz && (double)(float)v[j] != v[j]) *flag = 1;
+}
+
+// Per-row smallest column and whether every row spans fewer than 65536
+// columns (flag set otherwise).
+__global__ void k_row_span(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* base,
+                           int* flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int lo = INT_MAX, hi = INT_MIN;
+    for (int j = rp[i]; j < rp[i + 1]; j++) {
+        lo = min(lo, ci[j]);
+        hi = max(hi, ci[j]);
+    }
+    if (lo > hi) lo = hi = 0;
+    base[i] = lo;
+    if (hi - lo > 65535) *flag = 1;
+}
+
+__global__ void k_cols16(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                         const int* __restrict__ base, unsigned short* c16) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int b = base[i];
+    for (int j = rp[i]; j < rp[i + 1]; j++) c16[j] = (unsigned short)(ci[j] - b);
 }
 
 // --------------------------------------------------------------- helpers --
@@ -181,6 +206,64 @@ static int autotune_group_timed(const CsrView<T>& M, T* xin, T* yout) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return bestG;
+}
+
+// Build the 16-bit offsets of M and keep them when a timed product with
+// them beats the 32-bit one (decision cached per operator like the widths).
+template <typename T>
+static void tune_idx16(const CsrView<T>& M, Idx16& I, int G, const T* xin, T* yout,
+                       const char* op) {
+    I.on = false;
+    // RAPTOR_B200_IDX16=0 never uses 16-bit offsets, =1 uses them wherever
+    // the rows allow it (any size), unset lets the timing decide
+    const char* env = getenv("RAPTOR_B200_IDX16");
+    const int force = (env && env[0] == '0') ? 0 : (env && env[0] == '1') ? 1 : -1;
+    if (force == 0 || M.nnz == 0 || (force < 0 && M.n_rows < 4096)) return;
+    const std::string key = tune_key(op, M.n_rows, M.nnz, (int)sizeof(T));
+    auto& c = tune_cache();
+    auto it = c.m.find(key);
+    if (force < 0 && it != c.m.end() && it->second == 0) return;
+    DevArray<int> flag(1);
+    flag.zero();
+    I.base.alloc((size_t)M.n_rows);
+    k_row_span<<<grid_for(M.n_rows, 256), 256, 0, stream()>>>(M.n_rows, M.rowptr, M.cols,
+                                                              I.base.get(), flag.get());
+    RB_CHECK_LAUNCH();
+    if (read_scalar(flag.get())) {
+        I.base.release();
+        if (force < 0) {
+            c.m[key] = 0;
+            tune_save();
+        }
+        return;
+    }
+    I.c16.alloc((size_t)M.nnz);
+    k_cols16<<<grid_for(M.n_rows, 256), 256, 0, stream()>>>(M.n_rows, M.rowptr, M.cols,
+                                                            I.base.get(), I.c16.get());
+    RB_CHECK_LAUNCH();
+    bool use;
+    if (force > 0) {
+        use = true;
+    } else if (it != c.m.end()) {
+        use = it->second != 0;
+    } else {
+        const float t32 = time_launch([&] {
+            launch_rows(M.rowptr, M.cols, M.vals, M.n_rows, M.nnz, xin, EpiStore<T>{yout}, G);
+        });
+        const float t16 = time_launch([&] {
+            launch_rows16(M.rowptr, I.base.get(), I.c16.get(), M.vals, M.n_rows, M.nnz, xin,
+                          EpiStore<T>{yout}, G);
+        });
+        use = t16 < t32;
+        c.m[key] = use ? 1 : 0;
+        tune_save();
+    }
+    if (use) {
+        I.on = true;
+    } else {
+        I.base.release();
+        I.c16.release();
+    }
 }
 
 template <typename T>
@@ -448,7 +531,10 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
         if (l < L - 1) {
             V.gP = autotune_group(V.P, lv[l + 1].x.get(), V.xt.get(), "P");
             V.gR = autotune_group(V.R, V.r.get(), lv[l + 1].b.get(), "R");
+            tune_idx16(V.P, V.P16, V.gP, lv[l + 1].x.get(), V.xt.get(), "P16");
+            tune_idx16(V.R, V.R16, V.gR, V.r.get(), lv[l + 1].b.get(), "R16");
         }
+        if (!V.dia) tune_idx16(V.A, V.A16, V.gA, V.x.get(), V.r.get(), "A16");
     }
     RB_CUDA(cudaStreamSynchronize(stream()));
 }
@@ -678,7 +764,7 @@ void Hierarchy::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, 
     // r = b - A x ; b_c = R r   (par_multilevel.hpp:409-411)
     V.apply_A(cur, EpiResidual<T, T>{b, V.r.get()});
     mark(l * kProfSlots + 1);
-    launch_rows(V.R.rowptr, V.R.cols, V.R.vals, C.n, V.R.nnz, V.r.get(),
+    rows_op(V.R, V.R16, C.n, V.r.get(),
                 EpiStore<T>{C.b.get()}, V.gR);
     mark(l * kProfSlots + 2);
     cycle_level(lv, l + 1, C.x.get(), C.b.get(), true);
@@ -691,9 +777,9 @@ void Hierarchy::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, 
     if (jacobi_type && (opts.num_smooth_sweeps & 1)) start = (x == V.xt.get()) ? nullptr : V.xt.get();
     if (!start) start = x;
     if (cur == start) {
-        launch_rows(V.P.rowptr, V.P.cols, V.P.vals, V.n, V.P.nnz, C.x.get(), EpiAppend<T>{cur}, V.gP);
+        rows_op(V.P, V.P16, V.n, C.x.get(), EpiAppend<T>{cur}, V.gP);
     } else {
-        launch_rows(V.P.rowptr, V.P.cols, V.P.vals, V.n, V.P.nnz, C.x.get(),
+        rows_op(V.P, V.P16, V.n, C.x.get(),
                     EpiAddTo<T>{cur, start}, V.gP);
         cur = start;
     }
@@ -757,11 +843,11 @@ static double time_op_impl(Hierarchy& H, std::vector<Level<T>>& lv, int l, int o
                 V.apply_A(V.x.get(), EpiResidual<T, T>{V.b.get(), V.r.get()});
                 break;
             case 1:
-                launch_rows(V.R.rowptr, V.R.cols, V.R.vals, lv[l + 1].n, V.R.nnz, V.r.get(),
+                rows_op(V.R, V.R16, lv[l + 1].n, V.r.get(),
                             EpiStore<T>{lv[l + 1].b.get()}, V.gR);
                 break;
             case 2:
-                launch_rows(V.P.rowptr, V.P.cols, V.P.vals, V.n, V.P.nnz, lv[l + 1].x.get(),
+                rows_op(V.P, V.P16, V.n, lv[l + 1].x.get(),
                             EpiAppend<T>{V.x.get()}, V.gP);
                 break;
             default:

@@ -54,10 +54,27 @@ struct MasterLevel {
 };
 
 // Cycle data of one level in the cycle precision T.
+// 16-bit column offsets of a CSR operator whose rows each span fewer than
+// 65536 columns (column = base[row] + c16[j]); used when the autotuner
+// finds it faster than the 32-bit indices.
+struct Idx16 {
+    bool on = false;
+    DevArray<int> base;
+    DevArray<unsigned short> c16;
+};
+
+// rows of M times x with the epilogue, through 16- or 32-bit column indices
+template <typename T, typename TX, class Epi>
+void rows_op(const CsrView<T>& M, const Idx16& I, long n_rows, const TX* x, Epi epi, int G) {
+    if (I.on) launch_rows16(M.rowptr, I.base.get(), I.c16.get(), M.vals, n_rows, M.nnz, x, epi, G);
+    else launch_rows(M.rowptr, M.cols, M.vals, n_rows, M.nnz, x, epi, G);
+}
+
 template <typename T>
 struct Level {
     int n = 0;
     CsrView<T> A, P, R;
+    Idx16 A16, P16, R16;
     DevArray<T> Avals, Pvals, Rvals;   // value copies when T != double
     DevArray<T> dinv;                  // w / a_ii (Jacobi) or w / sum|a_ij| (L1)
     DevArray<int> colour_rows;         // rows grouped by colour (multicolour SOR)
@@ -73,7 +90,7 @@ struct Level {
     template <typename TX, class Epi>
     void apply_A(const TX* xin, Epi epi) const {
         if (dia) launch_dia(off, Adia.get(), n, xin, epi);
-        else launch_rows(A.rowptr, A.cols, A.vals, n, A.nnz, xin, epi, gA);
+        else rows_op(A, A16, n, xin, epi, gA);
     }
 };
 

@@ -181,6 +181,48 @@ k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
     (void)red;
 }
 
+// The same row kernel over 16-bit column offsets: column = base[row] +
+// c16[j].  For operators whose rows each span fewer than 65536 columns it
+// reads 2 bytes of index per nonzero instead of 4 (FP32 values: 6 bytes per
+// nonzero instead of 8).
+template <int G, typename TV, typename TX, class Epi>
+__global__ void RB_ROWS_BOUNDS
+k_csr_rows16(long n, const int* __restrict__ rp, const int* __restrict__ rbase,
+             const unsigned short* __restrict__ ci, const TV* __restrict__ cv,
+             const TX* __restrict__ x, Epi epi) {
+    using Acc = AccOf2<TV, TX>;
+    constexpr int RPW = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / G, gl = lane & (G - 1);
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    double red = 0.0;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        const bool valid = row < n;
+        int s = 0, e = 0, b0 = 0;
+        if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); b0 = __ldg(rbase + row); }
+        const TX* xb = x + b0;
+        Acc sum = 0;
+        int j = s + gl;
+        for (; j + 3 * G < e; j += 4 * G) {
+            const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + G);
+            const int c2 = __ldg(ci + j + 2 * G), c3 = __ldg(ci + j + 3 * G);
+            const TV v0 = __ldg(cv + j), v1 = __ldg(cv + j + G);
+            const TV v2 = __ldg(cv + j + 2 * G), v3 = __ldg(cv + j + 3 * G);
+            const TX x0 = __ldg(xb + c0), x1 = __ldg(xb + c1), x2 = __ldg(xb + c2), x3 = __ldg(xb + c3);
+            sum += (Acc)v0 * (Acc)x0;
+            sum += (Acc)v1 * (Acc)x1;
+            sum += (Acc)v2 * (Acc)x2;
+            sum += (Acc)v3 * (Acc)x3;
+        }
+        for (; j < e; j += G) sum += (Acc)__ldg(cv + j) * (Acc)__ldg(xb + __ldg(ci + j));
+        sum = group_sum<G>(sum);
+        if (valid && gl == 0) epi(row, sum, red);
+    }
+    (void)red;
+}
+
 template <int G, typename TV, class Fin>
 __global__ void RB_ROWS_BOUNDS
 k_csr_rows_dot(long n, const int* __restrict__ rp, const int* __restrict__ ci,
@@ -273,6 +315,24 @@ void launch_rows(const int* rp, const int* ci, const TV* cv, long n, long long n
         case 8: k_csr_rows<8><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
         case 16: k_csr_rows<16><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
         default: k_csr_rows<32><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
+    }
+    RB_CHECK_LAUNCH();
+}
+
+template <typename TV, typename TX, class Epi>
+void launch_rows16(const int* rp, const int* rbase, const unsigned short* c16, const TV* cv,
+                   long n, long long nnz, const TX* x, Epi epi, int G = 0) {
+    if (n <= 0) return;
+    if (G <= 0) G = pick_group(n, nnz);
+    const unsigned grid = row_grid(n, G);
+    cudaStream_t st = stream();
+    switch (G) {
+        case 1: k_csr_rows16<1><<<grid, kRowBlock, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+        case 2: k_csr_rows16<2><<<grid, kRowBlock, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+        case 4: k_csr_rows16<4><<<grid, kRowBlock, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+        case 8: k_csr_rows16<8><<<grid, kRowBlock, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+        case 16: k_csr_rows16<16><<<grid, kRowBlock, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+        default: k_csr_rows16<32><<<grid, kRowBlock, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
     }
     RB_CHECK_LAUNCH();
 }

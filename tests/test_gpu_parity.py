@@ -422,3 +422,28 @@ def test_multicolour_sor_convergence_factor_within_5pct(prob, interp):
     _, _, hs = seq.solve(np.zeros(n), bh)
     rho_ref = conv_factor(hs)
     assert abs(rho_mc - rho_ref) <= 0.05 * rho_ref, (rho_mc, rho_ref)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_sixteen_bit_column_offsets_change_nothing(prec, monkeypatch):
+    # the same hierarchy and solve with every eligible CSR operator of the
+    # cycle on 16-bit column offsets and with none: FP64 histories agree to
+    # rounding (summation order is unchanged), FP32 to single precision
+    Ao = lap27(20)
+    n = Ao.shape[0]
+    bh = np.random.default_rng(4).uniform(-1, 1, n)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("RAPTOR_B200_IDX16", mode)
+        A = to_rb(Ao)
+        ml = rb.ParRugeStubenSolver(0.25, rb.PMIS, rb.Extended, rb.Classical, rb.L1Jacobi)
+        ml.precision = prec
+        ml.setup(A)
+        x = rb.ParVector(n)
+        res = []
+        rb.PCG(A, ml, x, rb.ParVector(n, values=bh), res, tol=1e-10, mode=rb.PCG_TRUE_RESIDUAL)
+        out[mode] = (np.array(res), x.numpy())
+    r0, r1 = out["0"][0], out["1"][0]
+    assert len(r0) == len(r1)
+    np.testing.assert_allclose(r1, r0, rtol=1e-12 if prec == 0 else 1e-4)
+    np.testing.assert_allclose(out["1"][1], out["0"][1], rtol=1e-9, atol=1e-12)
