@@ -661,10 +661,8 @@ __device__ void spgemm_row(int lane, int row, const int* __restrict__ arp,
         m += __popc(bal);
     }
     __syncwarp();
-    if (!WRITE) {
-        if (lane == 0) cnt[row] = m;
-        return;
-    }
+    if (lane == 0 && cnt) cnt[row] = m;
+    if (!WRITE) return;
     // rank by column and write sorted
     const int out = crp[row];
     for (int a = lane; a < m; a += 32) {
@@ -674,6 +672,74 @@ __device__ void spgemm_row(int lane, int row, const int* __restrict__ arp,
         for (int b = 0; b < m; b++) r += keys[clist[b]] < c;
         cci[out + r] = c;
         ccv[out + r] = sums[sa];
+    }
+}
+
+// Structural size of a row of C (distinct columns, before the |v| <= 1e-16
+// drop) with key-only hash tables: 4 bytes a slot instead of 16, so four
+// times the warps per SM of the numeric pass.
+__device__ void spgemm_row_keys(int lane, int row, const int* __restrict__ arp,
+                                const int* __restrict__ aci, const int* __restrict__ brp,
+                                const int* __restrict__ bci, int* keys, int H, int* scnt) {
+    for (int t = lane; t < H; t += 32) keys[t] = -1;
+    __syncwarp();
+    const int as = arp[row], ae = arp[row + 1];
+    for (int j = as; j < ae; j++) {
+        const int ca = aci[j];
+        const int bs = brp[ca], be = brp[ca + 1];
+        for (int k = bs + lane; k < be; k += 32) hash_slot(keys, H, bci[k]);
+        __syncwarp();
+    }
+    int m = 0;
+    for (int base = 0; base < H; base += 32)
+        m += __popc(__ballot_sync(0xffffffffu, keys[base + lane] != -1));
+    if (lane == 0) scnt[row] = m;
+}
+
+template <int H, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+k_spgemm_keys(const int* __restrict__ rows, int nrows, const int* __restrict__ arp,
+              const int* __restrict__ aci, const int* __restrict__ brp,
+              const int* __restrict__ bci, int* scnt) {
+    extern __shared__ int kmem[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int idx = blockIdx.x * WPB + w;
+    if (idx >= nrows) return;
+    spgemm_row_keys(lane, rows[idx], arp, aci, brp, bci, kmem + (size_t)w * H, H, scnt);
+}
+
+__global__ void k_spgemm_keys_global(const int* __restrict__ rows, int nrows,
+                                     const long long* __restrict__ toff,
+                                     const int* __restrict__ tsize, const int* __restrict__ arp,
+                                     const int* __restrict__ aci, const int* __restrict__ brp,
+                                     const int* __restrict__ bci, int* gkeys, int* scnt) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nrows) return;
+    spgemm_row_keys(lane, rows[w], arp, aci, brp, bci, gkeys + toff[w], tsize[w], scnt);
+}
+
+// Bin rows by a size: <= lim0 -> bin 0, <= lim1 -> bin 1, else bin 2.
+__global__ void k_bin_rows(int n, const int* __restrict__ size, int lim0, int lim1, int* bins,
+                           int* bin_count) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int u = size[i];
+    const int bin = u <= lim0 ? 0 : (u <= lim1 ? 1 : 2);
+    const int p = atomicAdd(bin_count + bin, 1);
+    bins[(size_t)bin * n + p] = i;
+}
+
+// Move each row's first cnt[i] entries from the capacity layout (cap
+// offsets) to the final one (out offsets).
+__global__ void k_spgemm_compact(int n, const int* __restrict__ cap, const int* __restrict__ out,
+                                 const int* __restrict__ cnt, const int* __restrict__ ci,
+                                 const double* __restrict__ cv, int* oci, double* ocv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = cap[i], d = out[i];
+    for (int t = 0; t < cnt[i]; t++) {
+        oci[d + t] = ci[s + t];
+        ocv[d + t] = cv[s + t];
     }
 }
 
@@ -770,56 +836,134 @@ void spgemm_pass(const rb_csr_s& A, const rb_csr_s& B, const int* bins, const in
 }
 }  // namespace
 
+namespace {
+constexpr int kK0 = 1024, kKW0 = 16;   // key pass: 16 warps x 1024 x 4 B = 64 KB
+constexpr int kK1 = 8192, kKW1 = 4;    // key pass: 4 warps x 8192 x 4 B = 128 KB
+
+// Global tables (one per row of bin 2), sized from a per-row size.
+struct GlobalTables {
+    DevArray<long long> toff;
+    DevArray<int> tsize;
+    long long total = 0;
+};
+
+GlobalTables global_tables(const int* bins2, int count, const int* size_dev, int n) {
+    GlobalTables g;
+    if (!count) return g;
+    std::vector<int> rows(count), sz_h(n);
+    RB_CUDA(cudaMemcpyAsync(rows.data(), bins2, sizeof(int) * count, cudaMemcpyDeviceToHost,
+                            stream()));
+    RB_CUDA(cudaMemcpyAsync(sz_h.data(), size_dev, sizeof(int) * n, cudaMemcpyDeviceToHost,
+                            stream()));
+    RB_CUDA(cudaStreamSynchronize(stream()));
+    std::vector<long long> off(count);
+    std::vector<int> sz(count);
+    for (int t = 0; t < count; t++) {
+        sz[t] = next_pow2(std::max(64, 2 * sz_h[rows[t]]));
+        off[t] = g.total;
+        g.total += sz[t];
+    }
+    g.toff.alloc(count);
+    g.toff.upload(off.data(), count);
+    g.tsize.alloc(count);
+    g.tsize.upload(sz.data(), count);
+    return g;
+}
+}  // namespace
+
+// C = A B in two passes: a key-only pass counts each row's distinct
+// columns (4-byte slots, so four times the warps per SM of the numeric
+// pass), then the numeric pass -- binned by that count, so most rows get
+// small shared tables -- forms the sums in A's row order, drops
+// |v| <= 1e-16 and writes the survivors sorted; rows that lost entries to
+// the drop are compacted afterwards.
 rb_csr_s* spgemm(const rb_csr_s& A, const rb_csr_s& B) {
     RB_REQUIRE(A.n_cols == B.n_rows, "spgemm: inner dimensions differ");
     const int n = A.n_rows;
-    DevArray<int> ub((size_t)n + 1), bins((size_t)3 * n + 3), bcnt(3);
+    if (n == 0) {
+        rb_csr_s* C = new_csr(0, B.n_cols, 0);
+        RB_CUDA(cudaMemsetAsync(C->rowptr.get(), 0, sizeof(int), stream()));
+        return C;
+    }
+    // 1. structural counts
+    DevArray<int> ub((size_t)n + 1), bins((size_t)3 * n + 3), bcnt(3), scnt((size_t)n + 1);
     bcnt.zero();
-    if (n)
-        k_spgemm_bound<<<grid_for(n, 256), 256, 0, stream()>>>(n, A.rowptr.get(), A.cols.get(),
-                                                              B.rowptr.get(), ub.get(), bins.get(),
-                                                              bcnt.get(), kH0 / 2, kH1 / 2);
+    k_spgemm_bound<<<grid_for(n, 256), 256, 0, stream()>>>(n, A.rowptr.get(), A.cols.get(),
+                                                          B.rowptr.get(), ub.get(), bins.get(),
+                                                          bcnt.get(), kK0 / 2, kK1 / 2);
     RB_CHECK_LAUNCH();
     int hb[3];
     bcnt.download(hb, 3);
     RB_CUDA(cudaStreamSynchronize(stream()));
-    // global tables for the largest rows
-    DevArray<long long> toff;
-    DevArray<int> tsize, gkeys, glist;
-    DevArray<double> gsums;
-    std::vector<int> big;
+    if (hb[0]) {
+        const size_t sm = (size_t)kKW0 * kK0 * sizeof(int);
+        auto kern = k_spgemm_keys<kK0, kKW0>;
+        RB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        kern<<<grid_for(hb[0], kKW0), kKW0 * 32, sm, stream()>>>(
+            bins.get(), hb[0], A.rowptr.get(), A.cols.get(), B.rowptr.get(), B.cols.get(),
+            scnt.get());
+        RB_CHECK_LAUNCH();
+    }
+    if (hb[1]) {
+        const size_t sm = (size_t)kKW1 * kK1 * sizeof(int);
+        auto kern = k_spgemm_keys<kK1, kKW1>;
+        RB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        kern<<<grid_for(hb[1], kKW1), kKW1 * 32, sm, stream()>>>(
+            bins.get() + (size_t)n, hb[1], A.rowptr.get(), A.cols.get(), B.rowptr.get(),
+            B.cols.get(), scnt.get());
+        RB_CHECK_LAUNCH();
+    }
     if (hb[2]) {
-        std::vector<int> rows(hb[2]), ubh(n);
-        RB_CUDA(cudaMemcpyAsync(rows.data(), bins.get() + 2 * (size_t)n, sizeof(int) * hb[2],
-                                cudaMemcpyDeviceToHost, stream()));
-        RB_CUDA(cudaMemcpyAsync(ubh.data(), ub.get(), sizeof(int) * n, cudaMemcpyDeviceToHost,
-                                stream()));
+        GlobalTables g = global_tables(bins.get() + 2 * (size_t)n, hb[2], ub.get(), n);
+        DevArray<int> gkeys((size_t)g.total);
+        k_spgemm_keys_global<<<grid_for((long)hb[2] * 32, 128), 128, 0, stream()>>>(
+            bins.get() + 2 * (size_t)n, hb[2], g.toff.get(), g.tsize.get(), A.rowptr.get(),
+            A.cols.get(), B.rowptr.get(), B.cols.get(), gkeys.get(), scnt.get());
+        RB_CHECK_LAUNCH();
         RB_CUDA(cudaStreamSynchronize(stream()));
-        std::vector<long long> off(hb[2]);
-        std::vector<int> sz(hb[2]);
-        long long tot = 0;
-        for (int t = 0; t < hb[2]; t++) {
-            sz[t] = next_pow2(std::max(64, 2 * ubh[rows[t]]));
-            off[t] = tot;
-            tot += sz[t];
-        }
-        toff.alloc(hb[2]);
-        toff.upload(off.data(), hb[2]);
-        tsize.alloc(hb[2]);
-        tsize.upload(sz.data(), hb[2]);
-        gkeys.alloc((size_t)tot);
-        gsums.alloc((size_t)tot);
-        glist.alloc((size_t)tot);
+    }
+    // 2. capacity layout and numeric pass binned by the structural counts
+    DevArray<int> cap((size_t)n + 1);
+    const long long capacity = exclusive_scan(scnt.get(), cap.get(), n);
+    RB_REQUIRE(capacity <= INT_MAX, "spgemm: product has more than 2^31-1 entries");
+    DevArray<int> cols((size_t)std::max<long long>(capacity, 1));
+    DevArray<double> vals((size_t)std::max<long long>(capacity, 1));
+    bcnt.zero();
+    k_bin_rows<<<grid_for(n, 256), 256, 0, stream()>>>(n, scnt.get(), kH0 / 2, kH1 / 2,
+                                                       bins.get(), bcnt.get());
+    RB_CHECK_LAUNCH();
+    bcnt.download(hb, 3);
+    RB_CUDA(cudaStreamSynchronize(stream()));
+    GlobalTables g = global_tables(bins.get() + 2 * (size_t)n, hb[2], scnt.get(), n);
+    DevArray<int> gkeys, glist;
+    DevArray<double> gsums;
+    if (hb[2]) {
+        gkeys.alloc((size_t)g.total);
+        gsums.alloc((size_t)g.total);
+        glist.alloc((size_t)g.total);
     }
     DevArray<int> cnt((size_t)n + 1);
-    spgemm_pass<false>(A, B, bins.get(), hb, big, toff, tsize, gkeys, gsums, glist, cnt.get(),
-                       nullptr, nullptr, nullptr);
+    std::vector<int> unused;
+    spgemm_pass<true>(A, B, bins.get(), hb, unused, g.toff, g.tsize, gkeys, gsums, glist,
+                      cnt.get(), cap.get(), cols.get(), vals.get());
+    // 3. final layout: the capacity one unless the drop removed entries
     DevArray<int> crp((size_t)n + 1);
-    long long nnz = exclusive_scan(cnt.get(), crp.get(), n);
-    rb_csr_s* C = new_csr(n, B.n_cols, nnz);
-    C->rowptr = std::move(crp);
-    spgemm_pass<true>(A, B, bins.get(), hb, big, toff, tsize, gkeys, gsums, glist, nullptr,
-                      C->rowptr.get(), C->cols.get(), C->vals.get());
+    const long long nnz = exclusive_scan(cnt.get(), crp.get(), n);
+    rb_csr_s* C = new_csr(n, B.n_cols, 0);
+    C->nnz = nnz;
+    if (nnz == capacity) {
+        C->rowptr = std::move(cap);
+        C->cols = std::move(cols);
+        C->vals = std::move(vals);
+    } else {
+        C->rowptr = std::move(crp);
+        C->cols.alloc((size_t)std::max<long long>(nnz, 1));
+        C->vals.alloc((size_t)std::max<long long>(nnz, 1));
+        k_spgemm_compact<<<grid_for(n, 256), 256, 0, stream()>>>(
+            n, cap.get(), C->rowptr.get(), cnt.get(), cols.get(), vals.get(), C->cols.get(),
+            C->vals.get());
+        RB_CHECK_LAUNCH();
+    }
     return C;
 }
 
