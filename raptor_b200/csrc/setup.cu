@@ -357,6 +357,11 @@ __global__ void k_modclass_fill(int n, const int* __restrict__ arp, const int* _
 }
 
 // --- extended_interpolation, par_interpolation.cpp:280-989 ---------------
+// rows whose C set fits kExtSlots registers a lane go through the warp
+// kernels below; larger ones through the one-thread-per-row kernels
+constexpr int kExtSlots = 8;
+constexpr int kExtWarpMax = 32 * kExtSlots;
+
 // Upper bound of a row's pattern: strong C neighbours plus the strong C
 // neighbours of every strong F neighbour.
 __global__ void k_ext_bound(int n, const int* __restrict__ srp, const int* __restrict__ sci,
@@ -395,11 +400,13 @@ __device__ __forceinline__ int ext_build_pattern(int i, const int* __restrict__ 
 
 __global__ void k_ext_pattern(int n, int r0, const int* __restrict__ srp,
                               const int* __restrict__ sci, const int* __restrict__ st,
-                              const int* __restrict__ uoff, int* list, int* cnt) {
+                              const int* __restrict__ big, const int* __restrict__ uoff, int* list,
+                              int* cnt) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int i = r0 + t;
     const int o = uoff[t];
+    if (!big[i]) return;   // counted by k_ext_pattern_warp
     if (st[i] != kUnselected) {
         cnt[i] = st[i] == kSelected ? 1 : 0;
         return;
@@ -418,6 +425,7 @@ __global__ void k_ext_fill(int n, const int* __restrict__ arp, const int* __rest
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int p0 = prp[i], p1 = prp[i + 1];
+    if (p1 - p0 <= kExtWarpMax) return;   // filled by k_ext_fill_warp
     // rebuild the insertion-ordered pattern in place (its size is p1 - p0)
     if (st[i] == kSelected) pcols[p0] = i;
     else if (st[i] == kUnselected) ext_build_pattern(i, srp, sci, st, pcols, p0);
@@ -500,6 +508,244 @@ __global__ void k_ext_fill(int n, const int* __restrict__ arp, const int* __rest
     kept[i] = out - p0;
 }
 
+// ---- warp-per-row extended interpolation -------------------------------
+// The same arithmetic, in the same order, as k_ext_pattern / k_ext_fill,
+// with one warp per row.  The row's insertion-ordered C set, a hash table
+// from column to position and the weights live in the warp's shared memory.
+// Loops over a neighbour's row run one entry per lane: membership tests are
+// parallel hash probes, new C points are appended in entry order (ballot
+// prefix), the weights of one neighbour's expansion go to distinct
+// positions, and every sum whose order matters (col_sum, weak_sum, the
+// filter's row sums) is folded sequentially in the original order.  Rows
+// whose set exceeds kExtWarpMax entries take the one-thread-per-row kernels.
+constexpr int kExtHash = 2 * kExtWarpMax;   // hash slots per warp
+constexpr int kExtWarps = 8;                // warps per block
+
+struct ExtWarpMem {
+    int keys[kExtHash];
+    int pos[kExtHash];
+    int list[kExtWarpMax];
+    double vals[kExtWarpMax];
+};
+
+__device__ __forceinline__ unsigned ext_hash(int c) { return (unsigned)c * 2654435761u; }
+
+// position of column c in the set, or -1
+__device__ __forceinline__ int ext_find(const ExtWarpMem& w, int c) {
+    unsigned h = ext_hash(c) & (kExtHash - 1);
+    while (true) {
+        const int k = w.keys[h];
+        if (k == c) return w.pos[h];
+        if (k == -1) return -1;
+        h = (h + 1) & (kExtHash - 1);
+    }
+}
+
+// insert column c (not yet present) at position p; distinct keys may be
+// inserted by several lanes at once
+__device__ __forceinline__ void ext_insert(ExtWarpMem& w, int c, int p) {
+    unsigned h = ext_hash(c) & (kExtHash - 1);
+    while (true) {
+        if (atomicCAS(&w.keys[h], -1, c) == -1) {
+            w.pos[h] = p;
+            return;
+        }
+        h = (h + 1) & (kExtHash - 1);
+    }
+}
+
+// Insertion-ordered C set of row i; returns its size, or kExtWarpMax + 1
+// when it does not fit.
+__device__ int ext_build_warp(int i, const int* __restrict__ srp, const int* __restrict__ sci,
+                              const int* __restrict__ st, ExtWarpMem& w, int lane) {
+    for (int t = lane; t < kExtHash; t += 32) w.keys[t] = -1;
+    __syncwarp();
+    int m = 0;
+    for (int j = srp[i] + 1; j < srp[i + 1]; j++) {
+        const int c = sci[j];
+        const int sc = st[c];
+        if (sc == kSelected) {
+            if (ext_find(w, c) < 0) {
+                if (m >= kExtWarpMax) return kExtWarpMax + 1;
+                if (lane == 0) {
+                    w.list[m] = c;
+                    ext_insert(w, c, m);
+                }
+                m++;
+                __syncwarp();
+            }
+        } else if (sc == kUnselected) {
+            for (int base = srp[c] + 1; base < srp[c + 1]; base += 32) {
+                const int k = base + lane;
+                const int ck = k < srp[c + 1] ? sci[k] : -1;
+                const bool isnew = ck >= 0 && st[ck] == kSelected && ext_find(w, ck) < 0;
+                const unsigned b = __ballot_sync(0xffffffffu, isnew);
+                const int add = __popc(b);
+                if (m + add > kExtWarpMax) return kExtWarpMax + 1;
+                if (isnew) {
+                    const int p = m + __popc(b & ((1u << lane) - 1));
+                    w.list[p] = ck;
+                    ext_insert(w, ck, p);
+                }
+                m += add;
+                __syncwarp();
+            }
+        }
+    }
+    return m;
+}
+
+// Pattern sizes of the rows whose C set fits; a row that does not is marked
+// (big[i] = 1) for the one-thread-per-row kernel.
+__global__ void __launch_bounds__(kExtWarps * 32)
+k_ext_pattern_warp(int n, const int* __restrict__ srp, const int* __restrict__ sci,
+                   const int* __restrict__ st, int* cnt, int* big) {
+    extern __shared__ unsigned char ext_smem[];
+    ExtWarpMem& w = reinterpret_cast<ExtWarpMem*>(ext_smem)[threadIdx.x >> 5];
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= n) return;
+    if (st[i] != kUnselected) {
+        if (lane == 0) { cnt[i] = st[i] == kSelected ? 1 : 0; big[i] = 0; }
+        return;
+    }
+    const int m = ext_build_warp(i, srp, sci, st, w, lane);
+    if (lane == 0) {
+        big[i] = m > kExtWarpMax ? 1 : 0;
+        if (m <= kExtWarpMax) cnt[i] = m;
+    }
+}
+
+__global__ void __launch_bounds__(kExtWarps * 32)
+k_ext_fill_warp(int n, const int* __restrict__ arp, const int* __restrict__ aci,
+                const double* __restrict__ acv, const int* __restrict__ srp,
+                const int* __restrict__ sci, const int* __restrict__ st,
+                const int* __restrict__ prp, int* pcols, double* pvals, double filter,
+                int* kept) {
+    extern __shared__ unsigned char ext_smem[];
+    ExtWarpMem& w = reinterpret_cast<ExtWarpMem*>(ext_smem)[threadIdx.x >> 5];
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int p0 = prp[i], p1 = prp[i + 1];
+    if (p1 - p0 > kExtWarpMax) return;   // the one-thread-per-row kernel takes it
+    const int si = st[i];
+    int m = 0;
+    if (si == kSelected) {
+        if (lane == 0) { w.list[0] = i; w.vals[0] = 1.0; }
+        m = 1;
+        __syncwarp();
+    } else if (si == kUnselected) {
+        m = ext_build_warp(i, srp, sci, st, w, lane);
+        for (int t = lane; t < m; t += 32) w.vals[t] = 0.0;
+        __syncwarp();
+        int start = arp[i];
+        const int end = arp[i + 1];
+        double weak_sum = acv[start++];
+        int ctr = srp[i] + 1;
+        const int end_S = srp[i + 1];
+        for (int j = start; j < end; j++) {
+            const int col = aci[j];
+            const double val = acv[j];
+            const int idx = ext_find(w, col);
+            if (idx >= 0) {
+                if (lane == 0) w.vals[idx] = dadd(w.vals[idx], val);
+                __syncwarp();
+                if (ctr < end_S && sci[ctr] == col) ctr++;
+            } else if (ctr < end_S && sci[ctr] == col) {
+                ctr++;
+                if (st[col] != kUnselected) continue;
+                const int sk = arp[col] + 1, ek = arp[col + 1];
+                const int sign = acv[arp[col]] > 0 ? 1 : -1;
+                // col_sum: the qualifying entries of row col, summed in order
+                double col_sum = 0;
+                for (int base = sk; base < ek; base += 32) {
+                    const int k = base + lane;
+                    double vk = 0.0;
+                    bool q = false;
+                    if (k < ek) {
+                        vk = acv[k];
+                        const int ck = aci[k];
+                        q = dmul(vk, (double)sign) < 0 && (ck == i || ext_find(w, ck) >= 0);
+                    }
+                    unsigned b = __ballot_sync(0xffffffffu, q);
+                    while (b) {
+                        const int t = __ffs(b) - 1;
+                        col_sum = dadd(col_sum, __shfl_sync(0xffffffffu, vk, t));
+                        b &= b - 1;
+                    }
+                }
+                if (fabs(col_sum) < kZeroTol) {
+                    weak_sum = dadd(weak_sum, val);
+                } else {
+                    col_sum = __ddiv_rn(val, col_sum);
+                    for (int base = sk; base < ek; base += 32) {
+                        const int k = base + lane;
+                        bool self = false;
+                        double term = 0.0;
+                        if (k < ek) {
+                            const int ck = aci[k];
+                            const double vk = acv[k];
+                            if (dmul(vk, (double)sign) < 0) {
+                                term = dmul(col_sum, vk);
+                                if (ck == i) {
+                                    self = true;
+                                } else {
+                                    const int id = ext_find(w, ck);
+                                    if (id >= 0) w.vals[id] = dadd(w.vals[id], term);
+                                }
+                            }
+                        }
+                        // i occurs at most once in row col: its term joins
+                        // weak_sum at its place in the sequence
+                        const unsigned sb = __ballot_sync(0xffffffffu, self);
+                        if (sb) weak_sum = dadd(weak_sum, __shfl_sync(0xffffffffu, term, __ffs(sb) - 1));
+                    }
+                    __syncwarp();
+                }
+            } else {
+                if (st[col] != kNoNeighbors) weak_sum = dadd(weak_sum, val);
+            }
+        }
+        if (fabs(weak_sum) > kZeroTol)
+            for (int t = lane; t < m; t += 32) w.vals[t] = __ddiv_rn(w.vals[t], -weak_sum);
+        __syncwarp();
+    }
+    // filter_interp (only when 0 < filter <= 1), then the kept entries in order
+    const bool filt = filter > kZeroTol && filter <= 1;
+    double row_max = 0;
+    double scale = 1.0;
+    bool rescale = false;
+    if (filt) {
+        for (int t = lane; t < m; t += 32) row_max = fmax(row_max, fabs(w.vals[t]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) row_max = fmax(row_max, __shfl_xor_sync(0xffffffffu, row_max, o));
+        row_max = dmul(row_max, filter);
+        double row_sum = 0, remain_sum = 0;
+        for (int t = 0; t < m; t++) {
+            const double v = w.vals[t];
+            row_sum = dadd(row_sum, v);
+            if (fabs(v) >= row_max) remain_sum = dadd(remain_sum, v);
+        }
+        if (fabs(remain_sum) > kZeroTol && fabs(dsub(row_sum, remain_sum)) > kZeroTol) {
+            scale = __ddiv_rn(row_sum, remain_sum);
+            rescale = true;
+        }
+    }
+    int out = 0;
+    for (int base = 0; base < m; base += 32) {
+        const int t = base + lane;
+        const double v = t < m ? w.vals[t] : 0.0;
+        const bool keep = t < m && (!filt || fabs(v) >= row_max);
+        const unsigned b = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            const int pos = p0 + out + __popc(b & ((1u << lane) - 1));
+            pcols[pos] = w.list[t];
+            pvals[pos] = rescale ? dmul(v, scale) : v;
+        }
+        out += __popc(b);
+    }
+    if (lane == 0) kept[i] = out;
+}
+
 // Copy the first kept[i] entries of each row, mapping fine C columns to their
 // coarse index, and sort the row by column.
 __global__ void k_compact_rows(int n, const int* __restrict__ srcp, const int* __restrict__ scol,
@@ -560,9 +806,25 @@ rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* st, int
     DevArray<int> ub((size_t)n + 1);
     if (n) k_ext_bound<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), st, ub.get());
     RB_CHECK_LAUNCH();
-    std::vector<int> ubh((size_t)n);
+    DevArray<int> big((size_t)n + 1);
+    RB_CUDA(cudaFuncSetAttribute(k_ext_pattern_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kExtWarps * sizeof(ExtWarpMem))));
+    RB_CUDA(cudaFuncSetAttribute(k_ext_fill_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kExtWarps * sizeof(ExtWarpMem))));
+    if (n)
+        k_ext_pattern_warp<<<grid_for((long)n * 32, kExtWarps * 32), kExtWarps * 32,
+                             kExtWarps * sizeof(ExtWarpMem), stream()>>>(
+            n, S.rowptr.get(), S.cols.get(), st, cnt.get(), big.get());
+    RB_CHECK_LAUNCH();
+    std::vector<int> ubh((size_t)n), bigh((size_t)n);
     ub.download(ubh.data(), n);
+    big.download(bigh.data(), n);
     RB_CUDA(cudaStreamSynchronize(stream()));
+    // scratch only for the rows the warp kernel left
+    for (int i = 0; i < n; i++)
+        if (!bigh[i]) ubh[i] = 0;
+    DevArray<int> ubl((size_t)n + 1);
+    ubl.upload(ubh.data(), n);
     const long long kChunk = 1LL << 28;   // 1 GiB of int scratch per chunk
     long long maxchunk = 0;
     {
@@ -579,21 +841,30 @@ rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* st, int
         int r1 = r0;
         while (r1 < n && (acc + ubh[r1] <= kChunk || r1 == r0)) acc += ubh[r1++];
         const int cn = r1 - r0;
-        exclusive_scan(ub.get() + r0, uoff.get(), cn);
+        exclusive_scan(ubl.get() + r0, uoff.get(), cn);
         k_ext_pattern<<<grid_for(cn, 256), 256, 0, stream()>>>(cn, r0, S.rowptr.get(), S.cols.get(),
-                                                               st, uoff.get(), list.get(), cnt.get());
+                                                               st, big.get(), uoff.get(), list.get(),
+                                                               cnt.get());
         RB_CHECK_LAUNCH();
         r0 = r1;
     }
     list.release();
     uoff.release();
     ub.release();
+    ubl.release();
     long long nnz0 = exclusive_scan(cnt.get(), prp.get(), n);
     pcols.alloc((size_t)std::max(nnz0, 1LL));
     pvals.alloc((size_t)std::max(nnz0, 1LL));
-    if (n) k_ext_fill<<<g, 256, 0, stream()>>>(
-        n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(), st,
-        prp.get(), pcols.get(), pvals.get(), filter, kept.get());
+    if (n) {
+        k_ext_fill_warp<<<grid_for((long)n * 32, kExtWarps * 32), kExtWarps * 32,
+                          kExtWarps * sizeof(ExtWarpMem), stream()>>>(
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(), st,
+            prp.get(), pcols.get(), pvals.get(), filter, kept.get());
+        RB_CHECK_LAUNCH();
+        k_ext_fill<<<g, 256, 0, stream()>>>(
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(), st,
+            prp.get(), pcols.get(), pvals.get(), filter, kept.get());
+    }
     RB_CHECK_LAUNCH();
     DevArray<int> frp((size_t)n + 1);
     long long nnz = exclusive_scan(kept.get(), frp.get(), n);
