@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=96)
     p.add_argument("--batch-size", type=int, default=160,
                    help="grid side of the k right-hand-side workload (0 skips it)")
+    p.add_argument("--batch-ks", default="1,8,32",
+                   help="comma-separated right-hand-side counts of that workload")
     p.add_argument("--systems", type=int, default=64,
                    help="independent systems of the uneven batch (0 skips it)")
     p.add_argument("--diff-size", type=int, default=512,
@@ -553,7 +555,8 @@ def run_b200(args, rank, world, local):
     out["config"]["levels"] = ml.num_levels
     if args.batch_size > 0:
         out["batching"] = run_batching(rb, ev, lambda: rb.lib().rb_synchronize(),
-                                       args.batch_size)
+                                       args.batch_size,
+                                       ks=tuple(int(v) for v in args.batch_ks.split(",")))
     if args.systems > 0:
         out["uneven_batch"] = run_uneven_batch(rb, ev, lambda: rb.lib().rb_synchronize(),
                                                args.systems)

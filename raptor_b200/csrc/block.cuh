@@ -22,13 +22,13 @@ constexpr int kMaxBlockK = 32;
 // Tuning knobs of the block kernels (loads in flight against occupancy).
 // Measured on the SA 160^3 k = 8 / 32 solves: one row group per warp step
 // for the diagonal kernels (U = 4 rows: 12.6 / 10.7 ms per right-hand side,
-// U = 1: 10.4 / 7.6), 4-way unrolled CSR rows (9.7 / 7.05 against 2-way),
-// and the compiler's register choice (2 blocks per SM: 11.6 / 9.9).
+// U = 2: 9.86 / 7.96, U = 1: 9.41 / 6.78), the compiler's register choice
+// (2 blocks per SM: 11.6 / 9.9), CSR rows staged through shared memory with
+// up to 32 gathers per lane in flight (RB_BLOCK_CSR_STAGED, RB_BLOCK_STAGE_UN:
+// k = 32 7.07 -> 6.64 ms per right-hand side together with grids of resident
+// blocks only, against four index loads ahead of their gathers).
 #ifndef RB_BLOCK_DIA_U
 #define RB_BLOCK_DIA_U 1
-#endif
-#ifndef RB_BLOCK_CSR_UNROLL
-#define RB_BLOCK_CSR_UNROLL 4
 #endif
 #ifndef RB_BLOCK_MINB
 #define RB_BLOCK_MINB 0
@@ -121,9 +121,10 @@ __device__ void block_reduce_cols(double v, int k, const ReduceSlot& rs, Fin fin
     __threadfence();
     // strand q of column c sums blocks q, q + kStrands, ...
     const int c = threadIdx.x % KP, q = threadIdx.x / KP;
-    double t = 0.0;
-    for (unsigned b = q; b < gridDim.x; b += kStrands)
-        t += ((volatile double*)rs.partials)[(size_t)b * KP + c];
+    // (block b's partial of column c sits at b * KP + c: strand q reads
+    // indices (q + j kStrands) KP + c, j = 0, 1, ...)
+    const double t = sum_strided_l2(rs.partials, (unsigned)(q * KP + c), (unsigned)(kStrands * KP),
+                                    gridDim.x * (unsigned)KP);
     spart[threadIdx.x] = t;
     __syncthreads();
     if (threadIdx.x < KP) {
@@ -136,6 +137,57 @@ __device__ void block_reduce_cols(double v, int k, const ReduceSlot& rs, Fin fin
 }
 
 // ----------------------------------------------------------- CSR SpMM --
+#ifndef RB_BLOCK_CSR_STAGED
+#define RB_BLOCK_CSR_STAGED 1
+#endif
+
+#ifndef RB_BLOCK_STAGE_UN
+#define RB_BLOCK_STAGE_UN 32
+#endif
+
+#if RB_BLOCK_CSR_STAGED
+// One row's sum for lane (c, s) of its row group, G = KP S lanes.  The group
+// reads the row's column indices and values G at a time with one coalesced
+// load into the warp's staging area (scol / sval, 32 entries per warp); split
+// s then takes entries s KP .. s KP + KP - 1 of each chunk, and every lane
+// issues the gathers of X for UN of them before it uses the first, so a
+// row's gathers are in flight together instead of each waiting on its own
+// index load.  nchunks is uniform over the warp (the longest row of the
+// warp's groups): the staging area is shared by the whole warp.
+template <int KP, int S, typename TV, typename TX, typename Acc>
+__device__ __forceinline__ Acc staged_row(int rs, int re, int nchunks, const int* __restrict__ ci,
+                                          const TV* __restrict__ cv, const TX* __restrict__ X,
+                                          int k, int c, int s, int gl, int* scol, TV* sval) {
+    constexpr int G = KP * S;
+    constexpr int UN = KP >= RB_BLOCK_STAGE_UN ? RB_BLOCK_STAGE_UN : KP;
+    Acc acc = 0;
+    for (int ch = 0; ch < nchunks; ch++) {
+        const int b0 = rs + ch * G;
+        __syncwarp();
+        if (b0 + gl < re) {
+            scol[gl] = __ldg(ci + b0 + gl);
+            sval[gl] = __ldg(cv + b0 + gl);
+        }
+        __syncwarp();
+        const int cnt = min(max(re - b0 - s * KP, 0), KP);
+        const int* pc = scol + s * KP;
+        const TV* pv = sval + s * KP;
+        if (c < k) {
+            int u = 0;
+            for (; u + UN <= cnt; u += UN) {
+                TX xv[UN];
+#pragma unroll
+                for (int q = 0; q < UN; q++) xv[q] = __ldg(X + (long)pc[u + q] * k + c);
+#pragma unroll
+                for (int q = 0; q < UN; q++) acc += (Acc)pv[u + q] * (Acc)xv[q];
+            }
+            for (; u < cnt; u++) acc += (Acc)pv[u] * (Acc)__ldg(X + (long)pc[u] * k + c);
+        }
+    }
+    return acc;
+}
+#endif
+
 template <int KP, int S, typename TV, typename TX, typename Acc, class Epi>
 __global__ void __launch_bounds__(256)
 k_csr_block(long n, int k, const int* __restrict__ rp, const int* __restrict__ ci,
@@ -145,13 +197,25 @@ k_csr_block(long n, int k, const int* __restrict__ rp, const int* __restrict__ c
     const int c = lane % KP, s = (lane / KP) % S, sub = lane / (KP * S);
     const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+#if RB_BLOCK_CSR_STAGED
+    constexpr int G = KP * S;
+    __shared__ __align__(16) int scol_all[8][32];
+    __shared__ __align__(16) TV sval_all[8][32];
+    int* scol = scol_all[threadIdx.x >> 5] + sub * G;
+    TV* sval = sval_all[threadIdx.x >> 5] + sub * G;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        int rs = 0, re = 0;
+        if (row < n) { rs = __ldg(rp + row); re = __ldg(rp + row + 1); }
+        const int nch = __reduce_max_sync(0xffffffffu, (unsigned)((re - rs + G - 1) / G));
+        Acc acc = staged_row<KP, S, TV, TX, Acc>(rs, re, nch, ci, cv, X, k, c, s, lane % G, scol, sval);
+#else
     for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
         const long row = base + sub;
         Acc acc = 0;
         if (row < n && c < k) {
             const int rs = __ldg(rp + row), re = __ldg(rp + row + 1);
             int j = rs + s;
-#if RB_BLOCK_CSR_UNROLL >= 4
             for (; j + 3 * S < re; j += 4 * S) {
                 const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + S);
                 const int c2 = __ldg(ci + j + 2 * S), c3 = __ldg(ci + j + 3 * S);
@@ -164,17 +228,9 @@ k_csr_block(long n, int k, const int* __restrict__ rp, const int* __restrict__ c
                 acc += (Acc)v2 * (Acc)x2;
                 acc += (Acc)v3 * (Acc)x3;
             }
-#else
-            for (; j + S < re; j += 2 * S) {
-                const int c0 = __ldg(ci + j), c1 = __ldg(ci + j + S);
-                const TV v0 = __ldg(cv + j), v1 = __ldg(cv + j + S);
-                const TX x0 = __ldg(X + (long)c0 * k + c), x1 = __ldg(X + (long)c1 * k + c);
-                acc += (Acc)v0 * (Acc)x0;
-                acc += (Acc)v1 * (Acc)x1;
-            }
-#endif
             for (; j < re; j += S) acc += (Acc)__ldg(cv + j) * (Acc)__ldg(X + (long)__ldg(ci + j) * k + c);
         }
+#endif
 #pragma unroll
         for (int o = KP; o < KP * S; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (row < n && c < k && s == 0) epi(row, c, k, acc);
@@ -193,6 +249,20 @@ k_csr_block_dot(long n, int k, const int* __restrict__ rp, const int* __restrict
     const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
     double red = 0.0;
+#if RB_BLOCK_CSR_STAGED
+    constexpr int G = KP * S;
+    __shared__ __align__(16) int scol_all[8][32];
+    __shared__ __align__(16) TV sval_all[8][32];
+    int* scol = scol_all[threadIdx.x >> 5] + sub * G;
+    TV* sval = sval_all[threadIdx.x >> 5] + sub * G;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        int rs = 0, re = 0;
+        if (row < n) { rs = __ldg(rp + row); re = __ldg(rp + row + 1); }
+        const int nch = __reduce_max_sync(0xffffffffu, (unsigned)((re - rs + G - 1) / G));
+        double acc = staged_row<KP, S, TV, double, double>(rs, re, nch, ci, cv, P, k, c, s, lane % G,
+                                                           scol, sval);
+#else
     for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
         const long row = base + sub;
         double acc = 0;
@@ -211,6 +281,7 @@ k_csr_block_dot(long n, int k, const int* __restrict__ rp, const int* __restrict
             }
             for (; j < re; j += S) acc += (double)__ldg(cv + j) * __ldg(P + (long)__ldg(ci + j) * k + c);
         }
+#endif
 #pragma unroll
         for (int o = KP; o < KP * S; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (row < n && c < k && s == 0) {
@@ -397,11 +468,32 @@ inline int pow2_at_least(int k) {
     return p;
 }
 
+// Grid of a streaming kernel (no gathers): up to 16 blocks per SM.
 inline unsigned block_grid(long n, int KP, int S) {
     const long rows_per_warp = 32 / (KP * S);
     long warps = (n + rows_per_warp - 1) / rows_per_warp;
     long blocks = (warps * 32 + 255) / 256;
-    long cap = std::min<long>((long)sm_count() * 16, 65536 / kMaxBlockK);
+    static const int per_sm = grid_per_sm("RAPTOR_B200_GRID_BLOCK", 16);
+    long cap = std::min<long>((long)sm_count() * per_sm, 65536 / kMaxBlockK);
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return (unsigned)blocks;
+}
+
+// Grid of a gathering SpMM kernel: only as many blocks as are resident at
+// once, so that the warps in flight walk the rows as one contiguous window
+// (row = step * resident warps + warp).  The k columns of the rows a window
+// gathers from (its stencil or coarse-grid neighbours) are then read from
+// HBM once and reused from L2; with more blocks than fit, the later waves
+// revisit every neighbourhood after L2 has lost it, and a block vector of
+// hundreds of MB is read two to three times per product.
+inline unsigned block_grid_gather(const void* fn, long n, int KP, int S) {
+    static const bool wide = grid_per_sm("RAPTOR_B200_BLOCK_WIDE", 0) > 0;
+    if (wide) return block_grid(n, KP, S);
+    const long rows_per_warp = 32 / (KP * S);
+    long warps = (n + rows_per_warp - 1) / rows_per_warp;
+    long blocks = (warps * 32 + 255) / 256;
+    long cap = std::min<long>((long)sm_count() * resident_blocks_per_sm(fn, 256), 65536 / kMaxBlockK);
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     return (unsigned)blocks;
@@ -424,17 +516,20 @@ void launch_csr_block(const int* rp, const int* ci, const TV* cv, long n, int k,
     using Acc = AccOf2<TV, TX>;
     const int KP = pow2_at_least(k);
     if (KP * S > 32) S = 32 / KP;
-    const unsigned g = block_grid(n, KP, S);
+    auto go = [&](auto kern, int s) {
+        const unsigned g = block_grid_gather((const void*)kern, n, KP, s);
+        kern<<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+    };
     RB_BLOCK_KP_SWITCH(KP, {
         if constexpr (kKP <= 8) {
-            if (S >= 4) k_csr_block<kKP, 4, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
-            else if (S == 2) k_csr_block<kKP, 2, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
-            else k_csr_block<kKP, 1, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+            if (S >= 4) go(k_csr_block<kKP, 4, TV, TX, Acc, Epi>, 4);
+            else if (S == 2) go(k_csr_block<kKP, 2, TV, TX, Acc, Epi>, 2);
+            else go(k_csr_block<kKP, 1, TV, TX, Acc, Epi>, 1);
         } else if constexpr (kKP == 16) {
-            if (S >= 2) k_csr_block<16, 2, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
-            else k_csr_block<16, 1, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+            if (S >= 2) go(k_csr_block<16, 2, TV, TX, Acc, Epi>, 2);
+            else go(k_csr_block<16, 1, TV, TX, Acc, Epi>, 1);
         } else {
-            k_csr_block<32, 1, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+            go(k_csr_block<32, 1, TV, TX, Acc, Epi>, 1);
         }
     });
     RB_CHECK_LAUNCH();
@@ -445,18 +540,21 @@ void launch_csr_block_dot(const int* rp, const int* ci, const TV* cv, long n, in
                           const double* P, double* Y, int S, Fin fin) {
     const int KP = pow2_at_least(k);
     if (KP * S > 32) S = 32 / KP;
-    const unsigned g = block_grid(n, KP, S);
-    ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+    auto go = [&](auto kern, int s) {
+        const unsigned g = block_grid_gather((const void*)kern, n, KP, s);
+        ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+        kern<<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+    };
     RB_BLOCK_KP_SWITCH(KP, {
         if constexpr (kKP <= 8) {
-            if (S >= 4) k_csr_block_dot<kKP, 4, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
-            else if (S == 2) k_csr_block_dot<kKP, 2, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
-            else k_csr_block_dot<kKP, 1, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+            if (S >= 4) go(k_csr_block_dot<kKP, 4, TV, Fin>, 4);
+            else if (S == 2) go(k_csr_block_dot<kKP, 2, TV, Fin>, 2);
+            else go(k_csr_block_dot<kKP, 1, TV, Fin>, 1);
         } else if constexpr (kKP == 16) {
-            if (S >= 2) k_csr_block_dot<16, 2, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
-            else k_csr_block_dot<16, 1, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+            if (S >= 2) go(k_csr_block_dot<16, 2, TV, Fin>, 2);
+            else go(k_csr_block_dot<16, 1, TV, Fin>, 1);
         } else {
-            k_csr_block_dot<32, 1, TV><<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+            go(k_csr_block_dot<32, 1, TV, Fin>, 1);
         }
     });
     RB_CHECK_LAUNCH();
@@ -467,12 +565,15 @@ void launch_dia_block(const DiaOff& off, const TV* sv, long n, int k, const TX* 
     if (n <= 0) return;
     using Acc = AccOf2<TV, TX>;
     const int KP = pow2_at_least(k);
-    const unsigned g = block_grid(n, KP, 1);
+    auto go = [&](auto kern) {
+        const unsigned g = block_grid_gather((const void*)kern, n, KP, 1);
+        kern<<<g, 256, 0, stream()>>>(n, k, off, sv, X, epi);
+    };
     RB_BLOCK_KP_SWITCH(KP, {
         switch (off.nd) {
-            case 7: k_sdia_block<7, kKP, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, off, sv, X, epi); break;
-            case 27: k_sdia_block<27, kKP, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, off, sv, X, epi); break;
-            default: k_sdia_block<0, kKP, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, k, off, sv, X, epi); break;
+            case 7: go(k_sdia_block<7, kKP, TV, TX, Acc, Epi>); break;
+            case 27: go(k_sdia_block<27, kKP, TV, TX, Acc, Epi>); break;
+            default: go(k_sdia_block<0, kKP, TV, TX, Acc, Epi>); break;
         }
     });
     RB_CHECK_LAUNCH();
@@ -482,13 +583,16 @@ template <typename TV, class Fin>
 void launch_dia_block_dot(const DiaOff& off, const TV* sv, long n, int k, const double* P,
                           double* Y, Fin fin) {
     const int KP = pow2_at_least(k);
-    const unsigned g = block_grid(n, KP, 1);
-    ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+    auto go = [&](auto kern) {
+        const unsigned g = block_grid_gather((const void*)kern, n, KP, 1);
+        ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+        kern<<<g, 256, 0, stream()>>>(n, k, off, sv, P, Y, rs, fin);
+    };
     RB_BLOCK_KP_SWITCH(KP, {
         switch (off.nd) {
-            case 7: k_sdia_block_dot<7, kKP, TV><<<g, 256, 0, stream()>>>(n, k, off, sv, P, Y, rs, fin); break;
-            case 27: k_sdia_block_dot<27, kKP, TV><<<g, 256, 0, stream()>>>(n, k, off, sv, P, Y, rs, fin); break;
-            default: k_sdia_block_dot<0, kKP, TV><<<g, 256, 0, stream()>>>(n, k, off, sv, P, Y, rs, fin); break;
+            case 7: go(k_sdia_block_dot<7, kKP, TV, Fin>); break;
+            case 27: go(k_sdia_block_dot<27, kKP, TV, Fin>); break;
+            default: go(k_sdia_block_dot<0, kKP, TV, Fin>); break;
         }
     });
     RB_CHECK_LAUNCH();

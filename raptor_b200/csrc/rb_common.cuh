@@ -53,6 +53,12 @@ long long& launch_counter();
 cudaStream_t stream();
 void set_stream(cudaStream_t s);
 int sm_count();
+// Blocks per SM a grid-stride kernel family is capped at: the value of the
+// environment variable `env` when set to a positive integer, else `dflt`.
+int grid_per_sm(const char* env, int dflt);
+// Blocks of `threads` threads of kernel `fn` that fit on one SM at once
+// (the occupancy calculator's answer, cached per kernel).
+int resident_blocks_per_sm(const void* fn, int threads);
 
 // Owning device array (cudaMalloc'd; freed on destruction).
 template <typename T>

@@ -4,6 +4,7 @@
 
 #include <climits>
 #include <mutex>
+#include <unordered_map>
 
 #include "rb_internal.cuh"
 #include "spmv.cuh"
@@ -43,6 +44,25 @@ int sm_count() {
         RB_CUDA(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
     }
     return g_sms;
+}
+
+int resident_blocks_per_sm(const void* fn, int threads) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(fn);
+    if (it != cache.end()) return it->second;
+    int b = 0;
+    RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, threads, 0));
+    if (b < 1) b = 1;
+    cache[fn] = b;
+    return b;
+}
+
+int grid_per_sm(const char* env, int dflt) {
+    const char* v = getenv(env);
+    const int k = v ? atoi(v) : 0;
+    return k > 0 ? k : dflt;
 }
 
 rb_csr_s* new_csr(int n_rows, int n_cols, long long nnz) {
