@@ -33,10 +33,19 @@ constexpr int kMaxBlockK = 32;
 #ifndef RB_BLOCK_MINB
 #define RB_BLOCK_MINB 0
 #endif
+// Resident blocks per SM asked of the diagonal kernels with at most 9
+// diagonals (0: the compiler's choice); wider stencils keep the compiler's
+// choice.  Measured on the SA 160^3 solves, same box: 6 blocks 8.88 / 7.01
+// ms per right-hand side at k = 8 / 32, 8 blocks 9.39 / 7.05, compiler's
+// choice (4 blocks, 64 registers) 9.42 / 7.10.
+#ifndef RB_BLOCK_MINB_SMALL
+#define RB_BLOCK_MINB_SMALL 6
+#endif
 #if RB_BLOCK_MINB > 0
 #define RB_BLOCK_BOUNDS __launch_bounds__(256, RB_BLOCK_MINB)
 #else
-#define RB_BLOCK_BOUNDS __launch_bounds__(256)
+#define RB_BLOCK_BOUNDS \
+    __launch_bounds__(256, (ND > 0 && ND <= 9 && RB_BLOCK_MINB_SMALL > 0) ? RB_BLOCK_MINB_SMALL : 1)
 #endif
 
 // ----------------------------------------------------------- epilogues --
