@@ -6,6 +6,18 @@
 
 namespace rb {
 
+// Iteration state of the PCG loop run on the device (RB_PCG_TRUE_RESIDUAL):
+// the host writes it before each launch of the loop's graph, the last kernel
+// of every iteration advances it.
+constexpr int kPcgChunk = 16;   // iterations one launch of the loop graph may run
+struct PcgCtl {
+    int it;           // iterations done
+    int chunk_base;   // first iteration of this launch
+    int chunk_end;    // last iteration this launch may run
+    int pmode;        // at the start of the next iteration: 0 keep p, 1 p = z + beta p
+    double tol_bb;    // the stopping threshold tol * ||b||
+};
+
 // Krylov scalars live on the device so a whole iteration can be replayed
 // from a CUDA graph without host round trips.
 struct KScal {
@@ -19,6 +31,8 @@ struct KScal {
     double tmp;
     int breakdown;    // p.Ap < 0 or not finite
     int pad;
+    PcgCtl ctl;
+    double chunk_rr[kPcgChunk];   // r.r after each iteration of the launch
 };
 
 template <typename TO, typename TI>
@@ -87,6 +101,34 @@ static __global__ void k_cg_p(long n, double* __restrict__ p, const double* __re
     if (i >= n) return;
     if (restart) p[i] = z[i];
     else p[i] = p[i] * s->beta + z[i];
+}
+
+// p = z + beta p at the start of an iteration of the device-side loop, or
+// nothing when the previous step left p = z (start, restart)
+static __global__ void k_cg_p_dev(long n, double* __restrict__ p, const double* __restrict__ z,
+                                  const KScal* __restrict__ s) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || s->ctl.pmode == 0) return;
+    p[i] = p[i] * s->beta + z[i];
+}
+
+// Last kernel of one iteration of the device-side loop: count the iteration,
+// keep its r.r for the host's residual history, ask for the p update next
+// time, and (use_cond) end the graph's while loop once the iteration broke
+// down, met the tolerance (the host then confirms it with b - A x) or
+// reached the last iteration of this launch.
+static __global__ void k_pcg_step_end(KScal* s, cudaGraphConditionalHandle h, int use_cond) {
+    if (threadIdx.x != 0) return;
+    const int it = s->ctl.it + 1;
+    s->ctl.it = it;
+    const int slot = it - s->ctl.chunk_base;
+    if (slot >= 0 && slot < kPcgChunk) s->chunk_rr[slot] = s->rr;
+    s->ctl.pmode = 1;
+    if (use_cond) {
+        const bool stop = s->breakdown != 0 || sqrt(s->rr) <= s->ctl.tol_bb || it >= s->ctl.chunk_end ||
+                          slot + 1 >= kPcgChunk;
+        cudaGraphSetConditional(h, stop ? 0u : 1u);
+    }
 }
 
 // generic deterministic dot into a KScal field through a finisher

@@ -591,13 +591,15 @@ void Hierarchy::build_cycle_data() {
     ksh.alloc((size_t)n + 1);
     scal.alloc(1);
     scal.zero();
-    RB_CUDA(cudaMallocHost(&host_scal, sizeof(KScal)));
+    if (!host_scal) RB_CUDA(cudaMallocHost(&host_scal, sizeof(KScal)));
+    if (!host_ctl) RB_CUDA(cudaMallocHost(&host_ctl, sizeof(PcgCtl)));
     gA0 = autotune_group(view(*master[0].A), kp.get(), kAp.get(), "A0_fp64");
 }
 
 Hierarchy::~Hierarchy() {
     release_graphs();
     if (host_scal) cudaFreeHost(host_scal);
+    if (host_ctl) cudaFreeHost(host_ctl);
     if (host_barrier_error) cudaFreeHost(host_barrier_error);
 }
 
@@ -982,6 +984,49 @@ void Hierarchy::run_graph(const std::string& key, const std::function<void()>& f
     launch_counter() += graph_kernels[key];
 }
 
+// A graph whose single node is a while loop over the body fn captures
+// (fn gets the loop's condition handle; a kernel of the body sets it to 0 to
+// end the loop).  Built on first use, then replayed; the body's kernel count
+// is kept in graph_kernels[key] and the caller books it per iteration run.
+void Hierarchy::run_while_graph(const std::string& key,
+                                const std::function<void(cudaGraphConditionalHandle)>& fn) {
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+        cudaGraph_t g;
+        RB_CUDA(cudaGraphCreate(&g, 0));
+        std::unique_ptr<CUgraph_st, decltype(&cudaGraphDestroy)> own(g, &cudaGraphDestroy);
+        cudaGraphConditionalHandle h;
+        RB_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        RB_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        const long long c0 = launch_counter();
+        RB_CUDA(cudaStreamBeginCaptureToGraph(stream(), body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t captured_graph;
+        try {
+            fn(h);
+        } catch (...) {
+            cudaStreamEndCapture(stream(), &captured_graph);
+            launch_counter() = c0;
+            throw;
+        }
+        RB_CUDA(cudaStreamEndCapture(stream(), &captured_graph));
+        const long long captured = launch_counter() - c0;
+        launch_counter() = c0;
+        cudaGraphExec_t ge;
+        RB_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        graph_kernels[key] = count_kernel_nodes(body, captured);
+        it = graphs.emplace(key, ge).first;
+    }
+    RB_CUDA(cudaGraphLaunch(it->second, stream()));
+}
+
 static std::string pkey(const char* tag, const void* a, const void* b, const void* c = nullptr) {
     char buf[160];
     snprintf(buf, sizeof(buf), "%s:%p:%p:%p", tag, a, b, c);
@@ -1226,6 +1271,64 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
     };
     int iter = 0;
     int status = RB_ERR_NOT_CONVERGED;
+    if (mode == RB_PCG_TRUE_RESIDUAL && use_graphs) {
+        // The loop runs on the device: one graph launch performs up to nine
+        // iterations in a while node (its last kernel decides whether to go
+        // on), so the host waits once per launch instead of once per
+        // iteration.  Every 10th iteration (b - A x replaces the recursive
+        // residual) is a launch of its own.  The host then replays the
+        // iterations' residual norms into the history and confirms a
+        // converged recursive residual with the true one, as before.
+        int pmode = 0;   // p = z already (set above)
+        auto iteration = [&](bool full_r, cudaGraphConditionalHandle h, int use_cond) {
+            k_cg_p_dev<<<grid_for(n, 256), 256, 0, stream()>>>(n, p, z, S);
+            RB_CHECK_LAUNCH();
+            body(full_r);
+            k_pcg_step_end<<<1, 32, 0, stream()>>>(S, h, use_cond);
+            RB_CHECK_LAUNCH();
+        };
+        const double scale = bb > 0 ? bb : 1.0;
+        while (iter < max_iter) {
+            const bool full_r = (iter + 1) % 10 == 0;
+            const int end = full_r ? iter + 1 : std::min(max_iter, ((iter + 1) / 10) * 10 + 9);
+            *host_ctl = PcgCtl{iter, iter + 1, end, pmode, tol * bb};
+            RB_CUDA(cudaMemcpyAsync(&S->ctl, host_ctl, sizeof(PcgCtl), cudaMemcpyHostToDevice, stream()));
+            const std::string key = pkey(full_r ? "pcgF1" : "pcgW", x, b, &A);
+            if (full_r)
+                run_graph(key, [&] { iteration(true, cudaGraphConditionalHandle(), 0); });
+            else
+                run_while_graph(key, [&](cudaGraphConditionalHandle h) { iteration(false, h, 1); });
+            hs = read_scal();
+            const int done_it = hs.ctl.it;
+            if (!full_r) launch_counter() += graph_kernels[key] * (done_it - iter);
+            for (int i = iter + 1; i <= done_it; i++) {
+                if (i == done_it && hs.breakdown) break;
+                push(std::sqrt(hs.chunk_rr[i - (iter + 1)]) / scale);
+            }
+            iter = done_it;
+            pmode = 1;
+            if (hs.breakdown) {
+                *n_hist = nh;
+                return RB_ERR_BREAKDOWN;
+            }
+            if (std::sqrt(hs.rr) <= tol * bb) {
+                // confirm with the true residual
+                true_residual(A, x, b, r);
+                dot_into(r, r, n, &S->rr);
+                const double tr = std::sqrt(read_scal().rr);
+                if (nh - 1 < cap) hist[nh - 1] = tr / scale;
+                if (tr <= tol * bb) { status = RB_OK; break; }
+                // restart the recurrence from the true residual
+                cycle(z, r, true);
+                RB_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
+                dot_into(r, z, n, &S->rz);
+                pmode = 0;
+            }
+        }
+        *n_hist = nh;
+        last_iters = iter;
+        return status;
+    }
     while (iter < max_iter) {
         iter++;
         const bool full_r = (mode == RB_PCG_REFERENCE) ? (iter % 8 == 0) : (iter % 10 == 0);

@@ -107,6 +107,7 @@ struct Hierarchy {
     DevArray<double> kr, kz, kp, kAp, ks, kAs, krs, kph, ksh;
     DevArray<KScal> scal;
     KScal* host_scal = nullptr;
+    PcgCtl* host_ctl = nullptr;   // pinned staging of the device-side loop state
     int gA0 = 0;
     bool use_graphs = true;
     // fused bottom of the cycle (levels fuse_from .. L-1 in one launch)
@@ -153,6 +154,8 @@ struct Hierarchy {
     void cycle64(double* x, const double* b, bool x_zero);
     void cycle(double* x, const double* b, bool x_zero);
     void run_graph(const std::string& key, const std::function<void()>& fn);
+    void run_while_graph(const std::string& key,
+                         const std::function<void(cudaGraphConditionalHandle)>& fn);
     void release_graphs();
 
     void dot_into(const double* a, const double* b, long n, double* field);
