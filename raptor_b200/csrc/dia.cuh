@@ -29,6 +29,25 @@ constexpr int kMaxDiag = 32;
 #ifndef RB_DIA_MINB
 #define RB_DIA_MINB 4
 #endif
+// The kernels without a dot (stores, residuals, sweeps) run one 32-row slice
+// per warp (grid cap RB_DIA_GRID_ROWS blocks per SM, far above the slices of
+// any level) with at least 3 resident blocks (85 registers); the dot kernel,
+// whose last block sums one partial per block, keeps 32 blocks per SM and 4
+// resident blocks.  Measured on 192^3 (27 diagonals, FP32 values): residual
+// / Jacobi sweep 0.1516 / 0.1561 ms with (4 blocks, 32 per SM), 0.1498 /
+// 0.1556 with (3, 32), 0.1496 / 0.1538 with (4, 64), 0.1455 / 0.1497 with
+// (3, 128), 0.1435 / 0.1478 with (3, one slice per warp), 0.1681 / 0.1986
+// with (2, one slice per warp); the dot kernel with 3 resident blocks 0.180
+// against 0.166 ms.
+#ifndef RB_DIA_MINB_ROWS
+#define RB_DIA_MINB_ROWS 3
+#endif
+#ifndef RB_DIA_GRID_ROWS
+#define RB_DIA_GRID_ROWS 1024
+#endif
+#ifndef RB_DIA_GRID_DOT
+#define RB_DIA_GRID_DOT 32
+#endif
 #ifndef RB_DIA_TWO_PHASE
 #define RB_DIA_TWO_PHASE 1
 #endif
@@ -84,7 +103,7 @@ __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const
 }
 
 template <int ND, typename TV, typename TX, typename Acc, class Epi>
-__global__ void __launch_bounds__(256, RB_DIA_MINB)
+__global__ void __launch_bounds__(256, RB_DIA_MINB_ROWS)
 k_sdia_rows(long n, DiaOff off, const TV* __restrict__ sv, const TX* __restrict__ x, Epi epi) {
     const int lane = threadIdx.x & 31;
     const int nd = ND > 0 ? ND : off.nd;
@@ -126,10 +145,11 @@ k_sdia_rows_dot(long n, DiaOff off, const TV* __restrict__ sv, const double* __r
     block_reduce_finish(red, rs, fin);
 }
 
-inline unsigned dia_grid(long n) {
+inline unsigned dia_grid(long n, bool dot) {
     long blocks = ((n + 31) / 32 + 7) / 8;
-    static const int per_sm = grid_per_sm("RAPTOR_B200_GRID_DIA", 32);
-    long cap = (long)sm_count() * per_sm;
+    static const int per_sm_rows = grid_per_sm("RAPTOR_B200_GRID_DIA", RB_DIA_GRID_ROWS);
+    static const int per_sm_dot = grid_per_sm("RAPTOR_B200_GRID_DIA_DOT", RB_DIA_GRID_DOT);
+    long cap = (long)sm_count() * (dot ? per_sm_dot : per_sm_rows);
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     return (unsigned)blocks;
@@ -139,7 +159,7 @@ template <typename TV, typename TX, class Epi>
 void launch_dia(const DiaOff& off, const TV* sv, long n, const TX* x, Epi epi) {
     if (n <= 0) return;
     using Acc = AccOf2<TV, TX>;
-    const unsigned g = dia_grid(n);
+    const unsigned g = dia_grid(n, false);
     switch (off.nd) {
         case 5: k_sdia_rows<5, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;
         case 7: k_sdia_rows<7, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;
@@ -152,7 +172,7 @@ void launch_dia(const DiaOff& off, const TV* sv, long n, const TX* x, Epi epi) {
 
 template <typename TV, class Fin>
 void launch_dia_dot(const DiaOff& off, const TV* sv, long n, const double* x, double* y, Fin fin) {
-    const unsigned g = dia_grid(n);
+    const unsigned g = dia_grid(n, true);
     ReduceSlot rs = global_reduce_slot(g);
     EpiStoreDot epi{x, y};
     switch (off.nd) {
