@@ -34,10 +34,13 @@ constexpr int kMaxBlockK = 32;
 #define RB_BLOCK_MINB 0
 #endif
 // Resident blocks per SM asked of the diagonal kernels with at most 9
-// diagonals (0: the compiler's choice); wider stencils keep the compiler's
-// choice.  Measured on the SA 160^3 solves, same box: 6 blocks 8.88 / 7.01
-// ms per right-hand side at k = 8 / 32, 8 blocks 9.39 / 7.05, compiler's
-// choice (4 blocks, 64 registers) 9.42 / 7.10.
+// diagonals (0: the compiler's choice); wider stencils, and the kernel with
+// the per-column dots at 32 columns, keep the compiler's choice.  Measured
+// on the SA 160^3 solves, same box: 6 blocks 8.88 / 7.01 ms per right-hand
+// side at k = 8 / 32, 8 blocks 9.39 / 7.05, compiler's choice (4 blocks, 64
+// registers) 9.42 / 7.10; 6 blocks except for the dot kernel 9.41 / 6.69.
+// The dot kernel alone (96^3, k = 32): 0.309 ms with 6 blocks (40
+// registers), 0.200 ms with the compiler's 64 registers.
 #ifndef RB_BLOCK_MINB_SMALL
 #define RB_BLOCK_MINB_SMALL 6
 #endif
@@ -361,7 +364,8 @@ k_sdia_block(long n, int k, DiaOff off, const TV* __restrict__ sv, const TX* __r
 }
 
 template <int ND, int KP, typename TV, class Fin>
-__global__ void RB_BLOCK_BOUNDS
+__global__ void __launch_bounds__(256, (ND > 0 && ND <= 9 && KP < 32 && RB_BLOCK_MINB_SMALL > 0)
+                                           ? RB_BLOCK_MINB_SMALL : 1)
 k_sdia_block_dot(long n, int k, DiaOff off, const TV* __restrict__ sv,
                  const double* __restrict__ P, double* __restrict__ Y, ReduceSlot rsl, Fin fin) {
     constexpr int RPW = 32 / KP;

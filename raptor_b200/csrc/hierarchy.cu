@@ -1271,7 +1271,13 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
     };
     int iter = 0;
     int status = RB_ERR_NOT_CONVERGED;
-    if (mode == RB_PCG_TRUE_RESIDUAL && use_graphs) {
+    // RAPTOR_B200_PCG_DEVICE_LOOP=0 keeps one launch per iteration (profilers
+    // that do not descend into conditional graph nodes then see every kernel)
+    static const bool device_loop = [] {
+        const char* e = getenv("RAPTOR_B200_PCG_DEVICE_LOOP");
+        return !(e && e[0] == '0');
+    }();
+    if (mode == RB_PCG_TRUE_RESIDUAL && use_graphs && device_loop) {
         // The loop runs on the device: one graph launch performs up to nine
         // iterations in a while node (its last kernel decides whether to go
         // on), so the host waits once per launch instead of once per
