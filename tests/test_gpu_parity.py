@@ -265,7 +265,7 @@ def test_hierarchy_bit_exact(prob, interp):
 
 @pytest.mark.parametrize("compat", [1, 0])
 def test_solve_history_jacobi(compat):
-    # 100^2 aniso, RS/PMIS/ModClassical, Jacobi w=2/3, solve to 1e-8
+    # the 100^2 rotated anisotropic case: RS/PMIS/ModClassical, Jacobi w=2/3, solve to 1e-8
     Ao = aniso(100)
     A, ml, om = hierarchy_pair(Ao, "mod_classical", "jacobi", relax_weight=2.0 / 3.0,
                                jacobi_compat=compat, solve_tol=1e-8)
