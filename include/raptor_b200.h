@@ -97,6 +97,28 @@ int rb_laplace_stencil_27pt(double* out27);
 int rb_stencil_grid(const double* stencil, const int* grid, int dim, rb_csr* out);
 /* readParMatrix for PETSc binary AIJ files (gallery/par_matrix_IO.cpp:22+) */
 int rb_read_petsc(const char* path, rb_csr* out);
+/* MatrixMarket coordinate files (real, integer or pattern; general,
+ * symmetric or skew-symmetric).  read_mm (gallery/matrix_market.cpp:18-76):
+ * entries in file order within each row, the symmetry field ignored (the
+ * stored triangle only).  read_par_mm (gallery/par_matrix_market.cpp:
+ * 18-128): the mirror (j, i) of every off-diagonal entry of a symmetric
+ * file is stored too (-v for skew-symmetric) and each row is sorted by
+ * column; unlike the reference, a diagonal entry is stored once. */
+int rb_read_mm(const char* path, rb_csr* out);
+int rb_read_par_mm(const char* path, rb_csr* out);
+/* write_mm / write_par_mm (gallery/matrix_market.cpp:78-105): coordinate
+ * real general, "i j %2.15e" per entry in row order, 1-based. */
+int rb_write_mm(rb_csr A, const char* path);
+/* The same parsing into caller-owned host arrays (no device needed; no
+ * counterpart in the reference).  mirror = 1 and sort_rows = 1 give
+ * read_par_mm's matrix, 0 and 0 read_mm's.  Call with rowptr, cols, vals
+ * NULL to learn n_rows, n_cols and nnz, then again with arrays of
+ * n_rows + 1, nnz and nnz entries. */
+int rb_mm_read_host(const char* path, int mirror, int sort_rows, int* n_rows, int* n_cols,
+                    int64_t* nnz, int* rowptr, int* cols, double* vals);
+/* write_mm from host CSR arrays (no device needed). */
+int rb_mm_write_host(const char* path, int n_rows, int n_cols, int64_t nnz, const int* rowptr,
+                     const int* cols, const double* vals);
 
 /* ----------------------------------------------------- setup components */
 #define RB_STRENGTH_CLASSICAL 0 /* strength_t Classical (core/types.hpp:158) */

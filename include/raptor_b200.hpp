@@ -147,6 +147,21 @@ inline ParCSRMatrix* readParMatrix(const char* filename) {
     check(rb_read_petsc(filename, &h));
     return new ParCSRMatrix(h);
 }
+/* gallery/matrix_market.hpp, gallery/par_matrix_market.hpp (MatrixMarket
+ * coordinate files; see rb_read_mm / rb_read_par_mm for the two readers'
+ * conventions) */
+inline ParCSRMatrix* read_mm(const char* fname) {
+    rb_csr h = nullptr;
+    check(rb_read_mm(fname, &h));
+    return new ParCSRMatrix(h);
+}
+inline ParCSRMatrix* read_par_mm(const char* fname) {
+    rb_csr h = nullptr;
+    check(rb_read_par_mm(fname, &h));
+    return new ParCSRMatrix(h);
+}
+inline void write_mm(ParCSRMatrix* A, const char* fname) { check(rb_write_mm(A->handle(), fname)); }
+inline void write_par_mm(ParCSRMatrix* A, const char* fname) { write_mm(A, fname); }
 
 /* multilevel/par_multilevel.hpp: the option fields are the C options
  * themselves, so `ml->relax_weight = w` and friends work as in the reference */

@@ -228,6 +228,56 @@ def readParMatrix(path):
     return ParCSRMatrix(h)
 
 
+def read_mm(path):
+    """read_mm (gallery/matrix_market.cpp:18-76): file order within rows,
+    the symmetry field ignored."""
+    h = C.c_void_p()
+    check(lib().rb_read_mm(str(path).encode(), C.byref(h)))
+    return ParCSRMatrix(h)
+
+
+def read_par_mm(path):
+    """read_par_mm (gallery/par_matrix_market.cpp:18-128): symmetric files
+    mirrored (each diagonal entry once), rows sorted by column."""
+    h = C.c_void_p()
+    check(lib().rb_read_par_mm(str(path).encode(), C.byref(h)))
+    return ParCSRMatrix(h)
+
+
+def write_mm(A, path):
+    """write_mm / write_par_mm (gallery/matrix_market.cpp:78-105)."""
+    check(lib().rb_write_mm(A.h, str(path).encode()))
+
+
+write_par_mm = write_mm
+
+
+def mm_read_host(path, mirror=True, sort_rows=True):
+    """The MatrixMarket parser into host arrays (no device): returns
+    (n_rows, n_cols, rowptr, cols, vals).  mirror=True, sort_rows=True is
+    read_par_mm's matrix, False/False read_mm's."""
+    m, n, z = C.c_int(), C.c_int(), C.c_int64()
+    p = str(path).encode()
+    check(lib().rb_mm_read_host(p, int(mirror), int(sort_rows), C.byref(m), C.byref(n),
+                                C.byref(z), None, None, None))
+    rp = np.zeros(m.value + 1, np.int32)
+    ci = np.zeros(max(z.value, 1), np.int32)
+    cv = np.zeros(max(z.value, 1), np.float64)
+    check(lib().rb_mm_read_host(p, int(mirror), int(sort_rows), C.byref(m), C.byref(n),
+                                C.byref(z), _ptr(rp), _ptr(ci), _ptr(cv)))
+    return m.value, n.value, rp, ci[:z.value], cv[:z.value]
+
+
+def mm_write_host(path, n_rows, n_cols, rowptr, cols, vals):
+    """write_mm from host CSR arrays (no device)."""
+    rp = np.ascontiguousarray(rowptr, np.int32)
+    ci = np.ascontiguousarray(cols, np.int32)
+    cv = np.ascontiguousarray(vals, np.float64)
+    check(lib().rb_mm_write_host(str(path).encode(), int(n_rows), int(n_cols), int(rp[-1]),
+                                 _ptr(rp), _ptr(ci) if ci.size else None,
+                                 _ptr(cv) if cv.size else None))
+
+
 # setup components ---------------------------------------------------------
 def split_pmis(S, weights=None):
     n = S.global_num_rows

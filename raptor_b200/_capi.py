@@ -84,6 +84,14 @@ SIGNATURES = {
     "rb_laplace_stencil_27pt": (C.c_int, [_D]),
     "rb_stencil_grid": (C.c_int, [_D, _I, C.c_int, _PP]),
     "rb_read_petsc": (C.c_int, [C.c_char_p, _PP]),
+    "rb_read_mm": (C.c_int, [C.c_char_p, _PP]),
+    "rb_read_par_mm": (C.c_int, [C.c_char_p, _PP]),
+    "rb_write_mm": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "rb_mm_read_host": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), C.POINTER(C.c_int64), C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
+    "rb_mm_write_host": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int64, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
     "rb_strength": (C.c_int, [_P, C.c_int, C.c_double, _PP]),
     "rb_split_pmis": (C.c_int, [_P, _P, _I]),
     "rb_interpolation": (C.c_int, [_P, _P, _I, C.c_int, C.c_double, _PP]),

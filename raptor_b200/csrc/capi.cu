@@ -4,6 +4,7 @@
 // into an rb_status plus a per-thread message; nothing throws across the C
 // boundary.  There is no host fallback: without a device every compute call
 // fails with RB_ERR_NO_DEVICE.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -409,6 +410,63 @@ int rb_read_petsc(const char* path, rb_csr* out) {
         int rc = rb_csr_create(m, n, nnz, rp.data(), ci.data(), cv.data(), 0, out);
         if (rc != RB_OK) return rc;
         sort_rows_diag_first(**out, false);   // finalize() sorts rows
+        return RB_OK;
+    });
+}
+
+// ---------------------------------------------------------- MatrixMarket --
+// read_mm / read_par_mm / write_mm (gallery/matrix_market.cpp:18-105,
+// gallery/par_matrix_market.cpp:18-128); the parsing is in mmio.cu.
+int rb_mm_read_host(const char* path, int mirror, int sort_rows, int* n_rows, int* n_cols,
+                    int64_t* nnz, int* rowptr, int* cols, double* vals) {
+    return guarded([&]() -> int {
+        NEED(path); NEED(n_rows); NEED(n_cols); NEED(nnz);
+        HostCsr H = mm_parse(path, mirror != 0, sort_rows != 0);
+        *n_rows = H.n_rows;
+        *n_cols = H.n_cols;
+        *nnz = (int64_t)H.cols.size();
+        if (rowptr) std::copy(H.rowptr.begin(), H.rowptr.end(), rowptr);
+        if (cols) std::copy(H.cols.begin(), H.cols.end(), cols);
+        if (vals) std::copy(H.vals.begin(), H.vals.end(), vals);
+        return RB_OK;
+    });
+}
+
+int rb_mm_write_host(const char* path, int n_rows, int n_cols, int64_t nnz, const int* rowptr,
+                     const int* cols, const double* vals) {
+    return guarded([&]() -> int {
+        NEED(path);
+        mm_write(path, n_rows, n_cols, (long long)nnz, rowptr, cols, vals);
+        return RB_OK;
+    });
+}
+
+static int read_mm_as(const char* path, bool par, rb_csr* out) {
+    return guarded([&]() -> int {
+        ensure_device();
+        NEED(path); NEED(out);
+        HostCsr H = mm_parse(path, par, par);
+        return rb_csr_create(H.n_rows, H.n_cols, (int64_t)H.cols.size(), H.rowptr.data(),
+                             H.cols.data(), H.vals.data(), 0, out);
+    });
+}
+
+int rb_read_mm(const char* path, rb_csr* out) { return read_mm_as(path, false, out); }
+
+int rb_read_par_mm(const char* path, rb_csr* out) { return read_mm_as(path, true, out); }
+
+int rb_write_mm(rb_csr A, const char* path) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(path);
+        std::vector<int> rp((size_t)A->n_rows + 1), ci((size_t)A->nnz);
+        std::vector<double> cv((size_t)A->nnz);
+        A->rowptr.download(rp.data(), rp.size());
+        if (A->nnz) {
+            A->cols.download(ci.data(), ci.size());
+            A->vals.download(cv.data(), cv.size());
+        }
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        mm_write(path, A->n_rows, A->n_cols, A->nnz, rp.data(), ci.data(), cv.data());
         return RB_OK;
     });
 }

@@ -1,6 +1,8 @@
 // rb_internal.cuh -- handle types behind the C ABI and shared declarations.
 #pragma once
 
+#include <vector>
+
 #include "rb_common.cuh"
 
 struct rb_csr_s {
@@ -37,6 +39,18 @@ inline CsrView<double> view(const rb_csr_s& A) {
 }
 
 rb_csr_s* new_csr(int n_rows, int n_cols, long long nnz);
+// CSR arrays on the host (file I/O)
+struct HostCsr {
+    int n_rows = 0, n_cols = 0;
+    std::vector<int> rowptr, cols;
+    std::vector<double> vals;
+};
+// MatrixMarket coordinate file -> host CSR: mirror stores (j, i) for the
+// off-diagonal entries of symmetric / skew-symmetric files, sort_rows sorts
+// each row by column (stable); otherwise file order within a row (mmio.cu)
+HostCsr mm_parse(const char* path, bool mirror, bool sort_rows);
+void mm_write(const char* path, int n_rows, int n_cols, long long nnz, const int* rowptr,
+              const int* cols, const double* vals);
 rb_csr_s* clone_csr(const rb_csr_s& M);
 // Sort every row by column and move the diagonal to the front.
 void sort_rows_diag_first(rb_csr_s& A, bool diag_first);

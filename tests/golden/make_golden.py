@@ -15,6 +15,10 @@ import numpy as np
 
 REF = os.environ.get("RAPTOR_REFERENCE_ROOT", "/root/reference")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "raptor_golden.npz")
+# MatrixMarket files, kept byte for byte (the reader and writer tests parse
+# and rewrite them); sas_P0 and aniso_S have PETSc twins above
+OUT_MM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "raptor_mm.npz")
+MM_FILES = ["sas_P0", "aniso_S", "aniso"]
 
 MATRICES = [
     "aniso", "laplacian27", "random", "laplacian",
@@ -67,6 +71,12 @@ def main():
         out[name] = np.loadtxt(os.path.join(td, name + ".txt"), dtype=np.float64)
     np.savez_compressed(OUT, **out)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
+    mm = {}
+    for name in MM_FILES:
+        with open(os.path.join(td, name + ".mtx"), "rb") as f:
+            mm[name] = np.frombuffer(f.read(), dtype=np.uint8)
+    np.savez_compressed(OUT_MM, **mm)
+    print("wrote", OUT_MM, os.path.getsize(OUT_MM), "bytes")
 
 
 if __name__ == "__main__":
