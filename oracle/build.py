@@ -58,7 +58,7 @@ def build_oracle(force=False):
     hdr = os.path.join(HERE, "raptor_oracle.h")
     if force or _stale(ORACLE_SO, [src, hdr, __file__]):
         _run(["gcc", "-O2", "-std=c99", "-ffp-contract=off", "-fno-fast-math", "-fPIC",
-              "-shared", "-o", ORACLE_SO, src, "-lm"])
+              "-fopenmp", "-shared", "-o", ORACLE_SO, src, "-lm"])
     return ORACLE_SO
 
 

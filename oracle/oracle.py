@@ -44,6 +44,8 @@ def lib():
                                       os.path.getmtime(src) > os.path.getmtime(so)):
             _build.build_oracle()
         L = C.CDLL(so)
+        L.oc_set_threads.argtypes = [C.c_int]
+        L.oc_get_threads.restype = C.c_int
         L.oc_csr_new.restype = _P
         L.oc_csr_new.argtypes = [C.c_int, C.c_int, C.c_int, _I, _I, _D]
         L.oc_csr_free.argtypes = [_P]
@@ -158,6 +160,16 @@ class Borrowed(CSR):
 
     def __del__(self):
         pass
+
+
+def set_threads(n):
+    """Threads for the oracle's row-parallel loops (results are the same
+    for any count; see oc_set_threads)."""
+    lib().oc_set_threads(int(n))
+
+
+def get_threads():
+    return int(lib().oc_get_threads())
 
 
 def stencil_grid(stencil, grid):

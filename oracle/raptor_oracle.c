@@ -15,6 +15,12 @@
 #include <string.h>
 
 #define ZERO_TOL 1e-16 /* core/types.hpp:26 */
+
+/* row-parallel loops: a team only when more than one thread is asked for */
+static int g_threads = 1;
+void oc_set_threads(int n) { g_threads = n > 1 ? n : 1; }
+int oc_get_threads(void) { return g_threads; }
+#define OC_ROWS_PARALLEL _Pragma("omp parallel for num_threads(g_threads) if(g_threads > 1) schedule(static)")
 #define OC_RAND_MAX 2147483647.0 /* glibc RAND_MAX used by par_strength.cpp:78 */
 
 /* ------------------------------------------------------------------------ */
@@ -279,6 +285,7 @@ oc_csr* oc_stencil_grid(const double* stencil, const int* grid, int dim) {
 
 /* CSR_spmv, spmv.cpp:52-67 */
 void oc_spmv(const oc_csr* A, const double* x, double* b) {
+    OC_ROWS_PARALLEL
     for (int i = 0; i < A->n_rows; i++) {
         double v = 0;
         for (int j = A->rowptr[i]; j < A->rowptr[i + 1]; j++) v += A->vals[j] * x[A->cols[j]];
@@ -288,6 +295,7 @@ void oc_spmv(const oc_csr* A, const double* x, double* b) {
 
 /* CSR_residual, spmv.cpp:69-85 */
 void oc_residual(const oc_csr* A, const double* x, const double* b, double* r) {
+    OC_ROWS_PARALLEL
     for (int i = 0; i < A->n_rows; i++) {
         double v = b[i];
         for (int j = A->rowptr[i]; j < A->rowptr[i + 1]; j++) v -= A->vals[j] * x[A->cols[j]];
@@ -304,6 +312,7 @@ void oc_spmv_T(const oc_csr* A, const double* x, double* b) {
 
 /* CSR_append, spmv.cpp:88-103 */
 void oc_spmv_append(const oc_csr* A, const double* x, double* b) {
+    OC_ROWS_PARALLEL
     for (int i = 0; i < A->n_rows; i++) {
         double v = 0;
         for (int j = A->rowptr[i]; j < A->rowptr[i + 1]; j++) v += A->vals[j] * x[A->cols[j]];
@@ -1013,7 +1022,9 @@ static void sor_backward(const oc_csr* A, double* x, const double* y, double ome
 static void jacobi_sweep(const oc_csr* A, double* x, const double* b, double* tmp,
                          double omega, int compat) {
     int n = A->n_rows;
+    OC_ROWS_PARALLEL
     for (int i = 0; i < n; i++) tmp[i] = x[i];
+    OC_ROWS_PARALLEL
     for (int i = 0; i < n; i++) {
         double diag = compat ? 0.0 : A->vals[A->rowptr[i]];
         double row_sum = 0;
@@ -1027,7 +1038,9 @@ static void jacobi_sweep(const oc_csr* A, double* x, const double* b, double* tm
 static void l1_jacobi_sweep(const oc_csr* A, const double* l1, double* x, const double* b,
                             double* tmp, double omega) {
     int n = A->n_rows;
+    OC_ROWS_PARALLEL
     for (int i = 0; i < n; i++) tmp[i] = x[i];
+    OC_ROWS_PARALLEL
     for (int i = 0; i < n; i++) {
         double r = b[i];
         for (int j = A->rowptr[i]; j < A->rowptr[i + 1]; j++) r -= A->vals[j] * tmp[A->cols[j]];
@@ -1314,6 +1327,7 @@ static double vdot(const double* a, const double* b, int n) {
 }
 
 static void vaxpy(double* y, const double* x, double a, int n) {
+    OC_ROWS_PARALLEL
     for (int i = 0; i < n; i++) y[i] += x[i] * a;
 }
 
@@ -1392,6 +1406,7 @@ int oc_pcg_mode(const oc_csr* A, oc_ml* ml, double* x, const double* b, double t
             cycle(ml, z, r, 0);
             double next = vdot(r, z, n);
             double beta = next / rz;
+            OC_ROWS_PARALLEL
             for (int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
             rz = next;
         }

@@ -114,6 +114,13 @@ void oc_laplace_stencil_27pt(double* out27);
 oc_csr* oc_stencil_grid(const double* stencil, const int* grid, int dim);
 
 /* SpMV family: util/linalg/spmv.cpp */
+/* Threads for the row-parallel loops (SpMV, residual, append, Jacobi and
+ * L1-Jacobi sweeps, axpy): each row is still computed alone and in the same
+ * order, so results do not depend on the count; dots and the transposed
+ * (scatter) product stay sequential.  Default 1.  Used by the CPU baseline
+ * timing; only effective when built with OpenMP. */
+void oc_set_threads(int n);
+int oc_get_threads(void);
 void oc_spmv(const oc_csr* A, const double* x, double* b);
 void oc_residual(const oc_csr* A, const double* x, const double* b, double* r);
 void oc_spmv_T(const oc_csr* A, const double* x, double* b);
