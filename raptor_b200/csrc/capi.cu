@@ -613,14 +613,27 @@ void rb_amg_default_opts(rb_amg_opts* o) {
 
 int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_amg* out) {
     return guarded([&]() -> int {
-        NEED(A); NEED(out);
-        RB_REQUIRE(A->n_rows == A->n_cols, "AMG needs a square matrix");
         rb_amg_opts o;
         if (opts) o = *opts;
         else rb_amg_default_opts(&o);
+        // the options are checked before anything touches the matrix, so an
+        // option this build does not have (Direct interpolation, say) is an
+        // error, never a silent substitute
         RB_REQUIRE(o.solver == RB_SOLVER_RS || o.solver == RB_SOLVER_SA, "unknown solver");
+        RB_REQUIRE(o.solver == RB_SOLVER_SA || o.interp_type == RB_INTERP_MODCLASSICAL ||
+                       o.interp_type == RB_INTERP_EXTENDED,
+                   "interpolation must be ModClassical or Extended (Direct is not built)");
+        RB_REQUIRE(o.strength_type == RB_STRENGTH_CLASSICAL || o.strength_type == RB_STRENGTH_SYMMETRIC,
+                   "unknown strength type");
+        RB_REQUIRE(o.relax_type == RB_RELAX_JACOBI || o.relax_type == RB_RELAX_SOR ||
+                       o.relax_type == RB_RELAX_SSOR || o.relax_type == RB_RELAX_L1JACOBI,
+                   "unknown relaxation type");
+        RB_REQUIRE(o.precision == RB_PREC_FP64 || o.precision == RB_PREC_FP32, "unknown precision");
         RB_REQUIRE(o.prolong_smooth_steps >= 0, "prolong_smooth_steps < 0");
         RB_REQUIRE(o.num_smooth_sweeps >= 0, "num_smooth_sweeps < 0");
+        RB_REQUIRE(o.max_levels >= 1 && o.max_coarse >= 1, "max_levels and max_coarse must be >= 1");
+        NEED(A); NEED(out);
+        RB_REQUIRE(A->n_rows == A->n_cols, "AMG needs a square matrix");
         std::unique_ptr<rb_amg_s> ml(new rb_amg_s());
         ml->h.setup(*A, o, weights);
         *out = ml.release();

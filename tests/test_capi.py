@@ -66,3 +66,29 @@ def test_unbuilt_coarsenings_are_rejected():
     import raptor_b200 as rb
     with pytest.raises(rb.RaptorError):
         rb.ParRugeStubenSolver(0.25, rb.CLJP, rb.ModClassical)
+
+
+@pytest.mark.parametrize("field,value,message", [
+    ("interp_type", 0, "Direct is not built"),
+    ("strength_type", 5, "strength"),
+    ("relax_type", 9, "relaxation"),
+    ("precision", 2, "precision"),
+    ("max_levels", 0, "max_levels"),
+    ("solver", 7, "solver"),
+])
+def test_amg_options_are_checked_before_the_matrix(field, value, message):
+    # every option is validated before the matrix handle is touched, so the
+    # checks run without a device; an unbuilt option is an error, never a
+    # silent substitute
+    import raptor_b200 as rb
+    L = rb.lib()
+    opts = rb.AmgOpts()
+    L.rb_amg_default_opts(ctypes.byref(opts))
+    setattr(opts, field, value)
+    h = ctypes.c_void_p()
+    assert L.rb_amg_setup(None, ctypes.byref(opts), None, ctypes.byref(h)) == -1
+    assert message in rb.last_error()
+    # valid options: the missing matrix is what is reported
+    L.rb_amg_default_opts(ctypes.byref(opts))
+    assert L.rb_amg_setup(None, ctypes.byref(opts), None, ctypes.byref(h)) == -1
+    assert "A is NULL" in rb.last_error()
