@@ -57,6 +57,9 @@ def parse():
                    help="independent systems of the uneven batch (0 skips it)")
     p.add_argument("--diff-size", type=int, default=512,
                    help="grid side of the differentiation workload (0 skips it)")
+    p.add_argument("--aniso-size", type=int, default=0,
+                   help="grid side of the 2D anisotropic precision-form workload "
+                        "(4096 for the full case; 0 skips it)")
     return p.parse_args()
 
 
@@ -254,6 +257,39 @@ def run_batching(rb, ev, sync, S, ks=(1, 8, 32), steps=2):
     for k in ks:
         if k1 and k != 1:
             out["k"][str(k)]["per_rhs_speedup_vs_k1"] = k1["ms"] / out["k"][str(k)]["ms_per_rhs"]
+    return out
+
+
+def run_aniso_precision(rb, ev, sync, S, steps=2):
+    """The precision form's second workload: 2D rotated anisotropic
+    diffusion (eps 0.001, theta pi/8) on S^2, RS (PMIS, extended+i,
+    L1-Jacobi), PCG in true-residual mode to 1e-8, FP32 and FP64 cycles."""
+    A = rb.par_stencil_grid(rb.diffusion_stencil_2d(0.001, math.pi / 8.0), [S, S])
+    n = A.global_num_rows
+    b = rb.ParVector(n, values=np.random.default_rng(SEED).uniform(-1.0, 1.0, n))
+    out = {"workload": "aniso (eps 0.001, theta pi/8) %d^2 AMG-PCG to 1e-8 (RS PMIS, "
+                       "extended+i, L1-Jacobi)" % S, "rows": n, "nnz": A.local_nnz}
+    for name, prec in (("fp32", rb.FP32), ("fp64", rb.FP64)):
+        ml = rb.ParRugeStubenSolver(0.25, rb.PMIS, rb.Extended, rb.Classical, rb.L1Jacobi)
+        ml.precision = prec
+        ml.setup(A)
+        x = rb.ParVector(n)
+        times, res = [], []
+        for s in range(1 + steps):
+            x.set_const_value(0.0)
+            res = []
+            sync()
+            e0 = ev()
+            rb.PCG(A, ml, x, b, res, tol=TOL, max_iter=500, mode=rb.PCG_TRUE_RESIDUAL)
+            e1 = ev()
+            sync()
+            if s >= 1:
+                times.append(e0.elapsed_time(e1))
+        out[name] = {"ms": sum(times) / len(times), "iters": len(res) - 1,
+                     "final_rel_res": float(res[-1]), "setup_s": ml.setup_seconds,
+                     "levels": ml.num_levels}
+        del ml
+    out["speedup_fp32_over_fp64"] = out["fp64"]["ms"] / out["fp32"]["ms"]
     return out
 
 
@@ -563,6 +599,9 @@ def run_b200(args, rank, world, local):
     if args.diff_size > 0:
         out["differentiation"] = run_differentiation(rb, ev, lambda: rb.lib().rb_synchronize(),
                                                      args.diff_size)
+    if args.aniso_size > 0:
+        out["aniso_precision"] = run_aniso_precision(rb, ev, lambda: rb.lib().rb_synchronize(),
+                                                     args.aniso_size)
     if rank == 0 and args.cpu_sample > 0:
         out["cpu_baseline"] = cpu_baseline(args.cpu_sample, S, iters32[-1])
     dist.close()
