@@ -123,7 +123,8 @@ int rb_mm_write_host(const char* path, int n_rows, int n_cols, int64_t nnz, cons
 /* ----------------------------------------------------- setup components */
 #define RB_STRENGTH_CLASSICAL 0 /* strength_t Classical (core/types.hpp:158) */
 #define RB_STRENGTH_SYMMETRIC 1 /* strength_t Symmetric */
-#define RB_INTERP_MODCLASSICAL 1 /* interp_t ModClassical (core/types.hpp:161) */
+#define RB_INTERP_DIRECT 0       /* interp_t Direct (core/types.hpp:161) */
+#define RB_INTERP_MODCLASSICAL 1 /* interp_t ModClassical */
 #define RB_INTERP_EXTENDED 2     /* interp_t Extended */
 
 /* ParCSRMatrix::strength (par_strength.cpp:536-546 -> :8-339 / :342-531).

@@ -224,8 +224,8 @@ class ParRugeStubenSolver : public ParMultilevel {
                         relax_t relax_type = SOR)
         : ParMultilevel(strong_threshold, strength_type, relax_type) {
         if (coarsen_type != PMIS) throw error(RB_ERR_INVALID, "raptor_b200: only PMIS coarsening");
-        if (interp_type != ModClassical && interp_type != Extended)
-            throw error(RB_ERR_INVALID, "raptor_b200: interpolation is ModClassical or Extended");
+        if (interp_type != Direct && interp_type != ModClassical && interp_type != Extended)
+            throw error(RB_ERR_INVALID, "raptor_b200: interpolation is Direct, ModClassical or Extended");
         opts.solver = RB_SOLVER_RS;
         opts.interp_type = interp_type;
     }

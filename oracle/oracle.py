@@ -17,7 +17,7 @@ _D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _P = C.c_void_p
 
 RELAX = {"jacobi": 0, "sor": 1, "ssor": 2, "l1_jacobi": 3, "mc_sor": 4, "mc_ssor": 5}
-INTERP = {"mod_classical": 1, "extended": 2}
+INTERP = {"direct": 0, "mod_classical": 1, "extended": 2}
 
 
 class Opts(C.Structure):
@@ -74,6 +74,8 @@ def lib():
         L.oc_jacobi_prolongation.argtypes = [_P, _P, C.c_double, C.c_int]
         L.oc_mod_classical_interp.restype = _P
         L.oc_mod_classical_interp.argtypes = [_P, _P, _I]
+        L.oc_direct_interp.restype = _P
+        L.oc_direct_interp.argtypes = [_P, _P, _I]
         L.oc_extended_interp.restype = _P
         L.oc_extended_interp.argtypes = [_P, _P, _I, C.c_double]
         for f in ("oc_spgemm", "oc_spgemm_T"):
@@ -261,6 +263,8 @@ def interpolation(A, S, states, kind="mod_classical", filt=0.0):
     st = np.ascontiguousarray(states, np.int32)
     if kind == "extended":
         return CSR(lib().oc_extended_interp(A.ptr, S.ptr, st, filt))
+    if kind == "direct":
+        return CSR(lib().oc_direct_interp(A.ptr, S.ptr, st))
     return CSR(lib().oc_mod_classical_interp(A.ptr, S.ptr, st))
 
 

@@ -499,6 +499,79 @@ static int* coarse_index(const int* states, int n, int* nc_out) {
     return map;
 }
 
+/* direct_interpolation, par_interpolation.cpp:1453-1715 (world size 1).
+ * A and S are sorted with the diagonal first (:1466-1469).  For an F row the
+ * A values at the row's strong positions are found by walking A's row in
+ * step with S's (:1476-1490); the strong C neighbours' values are summed by
+ * sign, all off-diagonal values of A likewise, and each strong C neighbour
+ * gets -(sum_all / sum_strong) / a_ii of its sign times its value.  With no
+ * positive strong C neighbour the positive off-diagonal sum is lumped into
+ * the diagonal (:1656-1660).  A row without a negative strong C neighbour
+ * divides by zero there, as the reference does (:1645), but emits no entry
+ * that uses the quotient. */
+oc_csr* oc_direct_interp(const oc_csr* A, const oc_csr* S, const int* states) {
+    int n = A->n_rows, nc;
+    int* c2n = coarse_index(states, n, &nc);
+    oc_csr* P = csr_alloc(n, nc, S->nnz + n);
+    double* sa = (double*)malloc(sizeof(double) * ((size_t)S->nnz + 1));
+    for (int i = 0; i < n; i++) {
+        int ctr = A->rowptr[i], a1 = A->rowptr[i + 1];
+        for (int j = S->rowptr[i]; j < S->rowptr[i + 1]; j++) {
+            while (ctr < a1 && A->cols[ctr] != S->cols[j]) ctr++;
+            sa[j] = ctr < a1 ? A->vals[ctr] : 0.0;
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        if (states[i] == OC_SELECTED) {
+            csr_push(P, c2n[i], 1);
+            P->rowptr[i + 1] = P->nnz;
+            continue;
+        }
+        double sum_strong_pos = 0, sum_strong_neg = 0, sum_all_pos = 0, sum_all_neg = 0;
+        int start = S->rowptr[i], end = S->rowptr[i + 1], nstrong = 0;
+        if (start < end && S->cols[start] == i) start++;
+        for (int j = start; j < end; j++) {
+            if (states[S->cols[j]] == OC_SELECTED) {
+                double val = sa[j];
+                if (val < 0) sum_strong_neg += val;
+                else sum_strong_pos += val;
+                nstrong++;
+            }
+        }
+        if (nstrong == 0) {   /* no entry (and A's row may be empty) */
+            P->rowptr[i + 1] = P->nnz;
+            continue;
+        }
+        int a0 = A->rowptr[i], a1 = A->rowptr[i + 1];
+        double diag = a0 < a1 ? A->vals[a0] : 0.0;
+        for (int j = a0 + 1; j < a1; j++) {
+            double val = A->vals[j];
+            if (val < 0) sum_all_neg += val;
+            else sum_all_pos += val;
+        }
+        double alpha = sum_all_neg / sum_strong_neg, beta;
+        if (sum_strong_pos == 0) {
+            diag += sum_all_pos;
+            beta = 0;
+        } else {
+            beta = sum_all_pos / sum_strong_pos;
+        }
+        double neg_coeff = -alpha / diag;
+        double pos_coeff = -beta / diag;
+        for (int j = start; j < end; j++) {
+            int col = S->cols[j];
+            if (states[col] == OC_SELECTED) {
+                double val = sa[j];
+                csr_push(P, c2n[col], val < 0 ? neg_coeff * val : pos_coeff * val);
+            }
+        }
+        P->rowptr[i + 1] = P->nnz;
+    }
+    free(sa);
+    free(c2n);
+    return P;
+}
+
 /* mod_classical_interpolation, par_interpolation.cpp:991-1451.
  * A and S are sorted with the diagonal first.  pos[] marks the positions of
  * row i's strong C neighbours; entries of earlier rows are < row start. */
@@ -1213,6 +1286,7 @@ oc_ml* oc_ml_setup(const oc_csr* Af, const oc_opts* o, const double* weights, in
             oc_csr* S = oc_classical_strength(A, o->strong_threshold);
             oc_split_pmis(S, w, states);
             if (o->interp == OC_INTERP_EXTENDED) P = oc_extended_interp(A, S, states, o->interp_filter);
+            else if (o->interp == OC_INTERP_DIRECT) P = oc_direct_interp(A, S, states);
             else P = oc_mod_classical_interp(A, S, states);
             Ac = oc_rap(A, P, 1);
             oc_csr_free(S);

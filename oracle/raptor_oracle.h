@@ -53,6 +53,7 @@ typedef struct oc_csr {
 #define OC_RELAX_MCSSOR 5
 
 /* setup kinds */
+#define OC_INTERP_DIRECT 0
 #define OC_INTERP_MODCLASSICAL 1
 #define OC_INTERP_EXTENDED 2
 #define OC_SOLVER_RS 0
@@ -131,6 +132,7 @@ oc_csr* oc_classical_strength(const oc_csr* A, double theta);
 oc_csr* oc_symmetric_strength(const oc_csr* A, double theta);
 void oc_split_pmis(const oc_csr* S, const double* rand_vals, int* states);
 oc_csr* oc_mod_classical_interp(const oc_csr* A, const oc_csr* S, const int* states);
+oc_csr* oc_direct_interp(const oc_csr* A, const oc_csr* S, const int* states);
 oc_csr* oc_extended_interp(const oc_csr* A, const oc_csr* S, const int* states,
                            double filter);
 oc_csr* oc_spgemm(const oc_csr* A, const oc_csr* B);

@@ -152,8 +152,10 @@ Out* rs_interp(int n, const int* arp, const int* aci, const double* acv, const i
     CSRMatrix* A = make_csr(n, n, arp, aci, acv);
     CSRMatrix* S = make_csr(n, n, srp, sci, scv);
     aligned_vector<int> states(states_in, states_in + n);
-    CSRMatrix* P = extended ? extended_interpolation(A, S, states)
-                            : mod_classical_interpolation(A, S, states);
+    // extended: 0 mod_classical, 1 extended, 2 direct
+    CSRMatrix* P = extended == 1   ? extended_interpolation(A, S, states)
+                   : extended == 2 ? direct_interpolation(A, S, states)
+                                   : mod_classical_interpolation(A, S, states);
     Out* o = export_csr(P);
     delete A;
     delete S;

@@ -294,6 +294,10 @@ def interpolation(A, S, states, interp_type=ModClassical, filter_threshold=0.0):
     return ParCSRMatrix(h)
 
 
+def direct_interpolation(A, S, states):
+    return interpolation(A, S, states, Direct)
+
+
 def mod_classical_interpolation(A, S, states):
     return interpolation(A, S, states, ModClassical)
 
@@ -488,8 +492,8 @@ class ParRugeStubenSolver(ParMultilevel):
         super().__init__(strong_threshold, strength_type, relax_type)
         if coarsen_type != PMIS:
             raise RaptorError(-1, "only PMIS coarsening is built")
-        if interp_type not in (ModClassical, Extended):
-            raise RaptorError(-1, "interpolation must be ModClassical or Extended")
+        if interp_type not in (Direct, ModClassical, Extended):
+            raise RaptorError(-1, "interpolation must be Direct, ModClassical or Extended")
         self.opts.interp_type = interp_type
 
 

@@ -499,7 +499,8 @@ int rb_split_pmis(rb_csr S, const double* weights, int* states) {
 int rb_interpolation(rb_csr A, rb_csr S, const int* states, int kind, double filter, rb_csr* P) {
     return guarded([&]() -> int {
         NEED(A); NEED(S); NEED(states); NEED(P);
-        RB_REQUIRE(kind == RB_INTERP_MODCLASSICAL || kind == RB_INTERP_EXTENDED, "unknown interpolation kind");
+        RB_REQUIRE(kind == RB_INTERP_DIRECT || kind == RB_INTERP_MODCLASSICAL || kind == RB_INTERP_EXTENDED,
+                   "unknown interpolation kind");
         DevArray<int> st((size_t)std::max(A->n_rows, 1));
         st.upload(states, A->n_rows);
         *P = interpolation(*A, *S, st.get(), kind, filter);
@@ -620,9 +621,9 @@ int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_am
         // option this build does not have (Direct interpolation, say) is an
         // error, never a silent substitute
         RB_REQUIRE(o.solver == RB_SOLVER_RS || o.solver == RB_SOLVER_SA, "unknown solver");
-        RB_REQUIRE(o.solver == RB_SOLVER_SA || o.interp_type == RB_INTERP_MODCLASSICAL ||
-                       o.interp_type == RB_INTERP_EXTENDED,
-                   "interpolation must be ModClassical or Extended (Direct is not built)");
+        RB_REQUIRE(o.solver == RB_SOLVER_SA || o.interp_type == RB_INTERP_DIRECT ||
+                       o.interp_type == RB_INTERP_MODCLASSICAL || o.interp_type == RB_INTERP_EXTENDED,
+                   "interpolation must be Direct, ModClassical or Extended");
         RB_REQUIRE(o.strength_type == RB_STRENGTH_CLASSICAL || o.strength_type == RB_STRENGTH_SYMMETRIC,
                    "unknown strength type");
         RB_REQUIRE(o.relax_type == RB_RELAX_JACOBI || o.relax_type == RB_RELAX_SOR ||

@@ -11,6 +11,7 @@
 #include <climits>
 #include <cstdlib>
 
+#include "direct_interp.cuh"
 #include "rb_internal.cuh"
 
 namespace rb {
@@ -295,6 +296,21 @@ __global__ void k_modclass_count(int n, const int* __restrict__ srp, const int* 
     int k = 0;
     for (int j = srp[i] + 1; j < srp[i + 1]; j++) k += st[sci[j]] == kSelected;
     cnt[i] = k;
+}
+
+// direct interpolation (direct_interp.cuh), one thread per row
+__global__ void k_direct_count(int n, const int* __restrict__ srp, const int* __restrict__ sci,
+                               const int* __restrict__ st, int* cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) cnt[i] = direct_row_count(i, srp, sci, st);
+}
+
+__global__ void k_direct_fill(int n, const int* __restrict__ arp, const int* __restrict__ aci,
+                              const double* __restrict__ acv, const int* __restrict__ srp,
+                              const int* __restrict__ sci, const int* __restrict__ st,
+                              const int* __restrict__ prp, int* pcols, double* pvals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) direct_row_fill(i, arp, aci, acv, srp, sci, st, prp[i], pcols, pvals);
 }
 
 // pcols holds fine column indices while the row is assembled.
@@ -780,6 +796,27 @@ rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* st, int
     DevArray<int> cnt((size_t)n + 1), prp((size_t)n + 1), kept((size_t)n + 1);
     DevArray<int> pcols;
     DevArray<double> pvals;
+    if (kind == RB_INTERP_DIRECT) {
+        if (n) k_direct_count<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), st, cnt.get());
+        RB_CHECK_LAUNCH();
+        long long nnz = exclusive_scan(cnt.get(), prp.get(), n);
+        rb_csr_s* P = new_csr(n, nc, nnz);
+        P->rowptr = std::move(prp);
+        DevArray<int> fine_cols((size_t)std::max(nnz, 1LL));
+        if (n) k_direct_fill<<<g, 256, 0, stream()>>>(
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(), st,
+            P->rowptr.get(), fine_cols.get(), P->vals.get());
+        RB_CHECK_LAUNCH();
+        // map to coarse indices (S's rows, and so P's, are in increasing column order)
+        DevArray<double> tmpv((size_t)std::max(nnz, 1LL));
+        RB_CUDA(cudaMemcpyAsync(tmpv.get(), P->vals.get(), sizeof(double) * nnz,
+                                cudaMemcpyDeviceToDevice, stream()));
+        if (n) k_compact_rows<<<g, 256, 0, stream()>>>(n, P->rowptr.get(), fine_cols.get(),
+                                                       tmpv.get(), P->rowptr.get(), cmap.get(),
+                                                       P->cols.get(), P->vals.get());
+        RB_CHECK_LAUNCH();
+        return P;
+    }
     if (kind == RB_INTERP_MODCLASSICAL) {
         if (n) k_modclass_count<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), st, cnt.get());
         RB_CHECK_LAUNCH();

@@ -25,6 +25,7 @@ MATRICES = [
     "rss_A0", "rss_A1", "rss_A2", "rss_P0", "rss_P1", "rss_S0", "rss_S1",
     "aniso_S", "aniso_P_mod_class", "aniso_P_extend",
     "laplacian_S", "laplacian_P_mod_class", "laplacian_P_extend",
+    "aniso_P_direct", "laplacian_P_direct",
     "sas_A0", "sas_S0", "sas_T0", "sas_P0", "sas_A1", "sas_S1", "sas_T1", "sas_P1",
 ]
 INT_VECTORS = [

@@ -69,7 +69,7 @@ def test_unbuilt_coarsenings_are_rejected():
 
 
 @pytest.mark.parametrize("field,value,message", [
-    ("interp_type", 0, "Direct is not built"),
+    ("interp_type", 3, "interpolation must be"),
     ("strength_type", 5, "strength"),
     ("relax_type", 9, "relaxation"),
     ("precision", 2, "precision"),
@@ -78,7 +78,7 @@ def test_unbuilt_coarsenings_are_rejected():
 ])
 def test_amg_options_are_checked_before_the_matrix(field, value, message):
     # every option is validated before the matrix handle is touched, so the
-    # checks run without a device; an unbuilt option is an error, never a
+    # checks run without a device; an unknown option is an error, never a
     # silent substitute
     import raptor_b200 as rb
     L = rb.lib()

@@ -93,9 +93,10 @@ def test_pmis_splitting(golden, lvl):
     np.testing.assert_array_equal(states, golden["rss_cf%d_pmis" % lvl])
 
 
-# ruge_stuben/tests/test_par_interpolation.cpp (mod classical + extended, filter 0)
+# ruge_stuben/tests/test_par_interpolation.cpp (direct, mod classical, extended with filter 0)
 @pytest.mark.parametrize("prob", ["aniso", "laplacian"])
-@pytest.mark.parametrize("kind,fix", [("mod_classical", "P_mod_class"), ("extended", "P_extend")])
+@pytest.mark.parametrize("kind,fix", [("mod_classical", "P_mod_class"), ("extended", "P_extend"),
+                                      ("direct", "P_direct")])
 def test_interpolation(golden, prob, kind, fix):
     A = O.sort_diag_first(load(golden, prob))
     S = O.sort_diag_first(load(golden, prob + "_S"))

@@ -98,7 +98,7 @@ def test_pmis_interpolation_and_products(prob):
     # two differ only when such weak connections exist (the rotated
     # anisotropic stencil has positive ones), so extended is compared on the
     # Laplacian, whose off-diagonal entries are all strong.
-    kinds = [("mod_classical", 0)] + ([("extended", 1)] if prob.startswith("lap") else [])
+    kinds = [("mod_classical", 0), ("direct", 2)] + ([("extended", 1)] if prob.startswith("lap") else [])
     for kind, ext in kinds:
         ref = O.ref_take(REF.rs_interp(n, rp, ci, cv, srp, sci, scv, st, ext))
         P = O.interpolation(A, S, st, kind=kind, filt=0.0)
