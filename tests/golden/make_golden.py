@@ -30,6 +30,7 @@ MATRICES = [
 ]
 INT_VECTORS = [
     "rss_cf0_pmis", "rss_cf1_pmis", "aniso_split", "laplacian_split",
+    "rss_cf0", "rss_cf1", "rss_cf0_rs", "rss_cf1_rs",
     "sas_mis0", "sas_agg0", "sas_mis1", "sas_agg1",
 ]
 REAL_VECTORS = [

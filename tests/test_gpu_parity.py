@@ -188,7 +188,7 @@ def test_pmis_vs_oracle(prob):
 
 
 @pytest.mark.parametrize("prob", ["aniso", "laplacian"])
-@pytest.mark.parametrize("kind,fix", [(1, "P_mod_class"), (2, "P_extend")])
+@pytest.mark.parametrize("kind,fix", [(0, "P_direct"), (1, "P_mod_class"), (2, "P_extend")])
 def test_interpolation_golden(golden, prob, kind, fix):
     A = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, prob)).sort_diag_first()
     S = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, prob + "_S")).sort_diag_first()
@@ -209,6 +209,20 @@ def test_interpolation_bit_exact(prob, kind, filt):
     ref = O.interpolation(Ao, So, st, "extended" if kind == 2 else "mod_classical", filt)
     P = rb.interpolation(to_rb(Ao), to_rb(So), st, kind, filt)
     assert_csr_equal(rb_tuple(P), oc_tuple(ref))
+
+
+@pytest.mark.parametrize("lvl", [0, 1])
+def test_direct_interpolation_on_the_rss_hierarchy(golden, lvl):
+    # the fixture hierarchy's prolongators are direct interpolation on its
+    # CLJP splittings (ruge_stuben/tests/test_ruge_stuben.cpp)
+    A = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, "rss_A%d" % lvl)).sort_diag_first()
+    S = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, "rss_S%d" % lvl)).sort_diag_first()
+    P = rb.interpolation(A, S, golden["rss_cf%d" % lvl], 0, 0.0)
+    ref = canon(golden_csr(golden, "rss_P%d" % lvl))
+    got = canon(rb_tuple(P))
+    np.testing.assert_array_equal(got[2], ref[2])
+    np.testing.assert_array_equal(got[3], ref[3])
+    np.testing.assert_allclose(got[4], ref[4], atol=1e-12)
 
 
 @pytest.mark.parametrize("lvl", [0, 1])

@@ -105,6 +105,16 @@ def test_interpolation(golden, prob, kind, fix):
     assert_same(as_tuple(P), golden_csr(golden, prob + "_" + fix), tol=1e-6)
 
 
+# ruge_stuben/tests/test_ruge_stuben.cpp: direct interpolation on the
+# CLJP splitting of the fixture hierarchy reproduces its prolongators
+@pytest.mark.parametrize("lvl", [0, 1])
+def test_direct_interpolation_on_the_rss_hierarchy(golden, lvl):
+    A = O.sort_diag_first(load(golden, "rss_A%d" % lvl))
+    S = O.sort_diag_first(load(golden, "rss_S%d" % lvl))
+    P = O.interpolation(A, S, golden["rss_cf%d" % lvl], kind="direct")
+    assert_same(as_tuple(P), golden_csr(golden, "rss_P%d" % lvl), tol=1e-12)
+
+
 # ruge_stuben/tests/test_par_rap.cpp
 @pytest.mark.parametrize("lvl", [0, 1])
 def test_rap(golden, lvl):
