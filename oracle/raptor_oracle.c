@@ -491,6 +491,102 @@ void oc_split_pmis(const oc_csr* S, const double* rand_vals, int* states) {
 /* interpolation (ruge_stuben/par_interpolation.cpp)                        */
 /* ------------------------------------------------------------------------ */
 
+/* split_cljp, ruge_stuben/cf_splitting.cpp:649-675 -> cljp_main_loop
+ * (:479-545): weights = rand_vals + the number of rows in which a point is a
+ * strong column; each round selects every unassigned point whose weight is
+ * not exceeded by a strong neighbour in its row or its column
+ * (select_independent_set, :324-378), removes the edges those new C points
+ * satisfy (update_weights, :380-447; edgemark per nonzero of S, c_dep_cache
+ * per point) and retires new C points and points whose weight fell below 1
+ * (update_states, :449-477).  S is sorted with the diagonal first; its
+ * column pattern leaves the diagonal out (transpose, :9-67). */
+void oc_split_cljp(const oc_csr* S, const double* rand_vals, int* states) {
+    int n = S->n_rows;
+    int *colptr, *colidx;
+    s_transpose(S, &colptr, &colidx);
+    double* w = (double*)malloc(sizeof(double) * ((size_t)n + 1));
+    int* unassigned = (int*)malloc(sizeof(int) * ((size_t)n + 1));
+    int* newc = (int*)malloc(sizeof(int) * ((size_t)n + 1));
+    int* cdep = (int*)calloc((size_t)n + 1, sizeof(int));
+    char* edgemark = (char*)malloc((size_t)S->nnz + 1);
+    memset(edgemark, 1, (size_t)S->nnz + 1);
+    for (int i = 0; i < n; i++) {
+        w[i] = rand_vals[i];
+        unassigned[i] = i;
+        states[i] = OC_UNASSIGNED;
+    }
+    for (int i = 0; i < n; i++) {
+        int s = S->rowptr[i], e = S->rowptr[i + 1];
+        if (s < e && S->cols[s] == i) s++;
+        for (int j = s; j < e; j++) w[S->cols[j]] += 1;
+    }
+    int remaining = n;
+    while (remaining) {
+        int nnew = 0;
+        for (int k = 0; k < remaining; k++) {
+            int u = unassigned[k], j;
+            double weight = w[u];
+            int s = S->rowptr[u], e = S->rowptr[u + 1];
+            if (s < e && S->cols[s] == u) s++;
+            for (j = s; j < e; j++)
+                if (w[S->cols[j]] > weight) break;
+            if (j != e) continue;
+            for (j = colptr[u]; j < colptr[u + 1]; j++)
+                if (w[colidx[j]] > weight) break;
+            if (j != colptr[u + 1]) continue;
+            states[u] = OC_NEWSELECTION;
+            newc[nnew++] = u;
+        }
+        for (int k = 0; k < nnew; k++) {
+            int c = newc[k];
+            int s = S->rowptr[c], e = S->rowptr[c + 1];
+            if (s < e && S->cols[s] == c) s++;
+            for (int j = s; j < e; j++) {
+                int idx = S->cols[j];
+                if (states[idx] == OC_UNASSIGNED && edgemark[j]) {
+                    edgemark[j] = 0;
+                    w[idx]--;
+                }
+            }
+        }
+        for (int k = 0; k < nnew; k++) {
+            int c = newc[k];
+            for (int j = colptr[c]; j < colptr[c + 1]; j++) {
+                int idx = colidx[j];
+                if (states[idx] == OC_UNASSIGNED) cdep[idx] = c;
+            }
+            for (int j = colptr[c]; j < colptr[c + 1]; j++) {
+                int idx = colidx[j];
+                if (states[idx] == OC_SELECTED) continue;
+                int s = S->rowptr[idx], e = S->rowptr[idx + 1];
+                if (s < e && S->cols[s] == idx) s++;
+                for (int q = s; q < e; q++) {
+                    int idx_k = S->cols[q];
+                    if (states[idx_k] == OC_UNASSIGNED && edgemark[q] && cdep[idx_k] == c) {
+                        edgemark[q] = 0;
+                        w[idx_k]--;
+                    }
+                }
+            }
+        }
+        int ctr = 0;
+        for (int k = 0; k < remaining; k++) {
+            int u = unassigned[k];
+            if (states[u] == OC_NEWSELECTION) {
+                w[u] = 0.0;
+                states[u] = OC_SELECTED;
+            } else if (w[u] < 1.0) {
+                w[u] = 0.0;
+                states[u] = OC_UNSELECTED;
+            } else {
+                unassigned[ctr++] = u;
+            }
+        }
+        remaining = ctr;
+    }
+    free(colptr); free(colidx); free(w); free(unassigned); free(newc); free(cdep); free(edgemark);
+}
+
 static int* coarse_index(const int* states, int n, int* nc_out) {
     int* map = (int*)malloc(sizeof(int) * (n + 1));
     int nc = 0;

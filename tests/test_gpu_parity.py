@@ -225,6 +225,22 @@ def test_direct_interpolation_on_the_rss_hierarchy(golden, lvl):
     np.testing.assert_allclose(got[4], ref[4], atol=1e-12)
 
 
+def test_direct_chain_reproduces_the_fixture_hierarchy(golden):
+    # ruge_stuben/tests/test_ruge_stuben.cpp on the GPU: classical strength
+    # 0.25 -> direct interpolation on the fixture's CLJP splitting ->
+    # Galerkin product, twice, against the fixture's A1 and A2
+    A = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, "rss_A0")).sort_diag_first()
+    for lvl in (0, 1):
+        S = A.strength(0, 0.25)
+        P = rb.interpolation(A, S, golden["rss_cf%d" % lvl], 0, 0.0)
+        A = rb.rap(A, P)
+        ref = canon(golden_csr(golden, "rss_A%d" % (lvl + 1)))
+        got = canon(rb_tuple(A))
+        np.testing.assert_array_equal(got[2], ref[2])
+        np.testing.assert_array_equal(got[3], ref[3])
+        np.testing.assert_allclose(got[4], ref[4], atol=1e-6)
+
+
 @pytest.mark.parametrize("lvl", [0, 1])
 def test_rap_golden(golden, lvl):
     A = rb.ParCSRMatrix.from_arrays(*golden_csr(golden, "rss_A%d" % lvl))

@@ -105,6 +105,14 @@ def test_interpolation(golden, prob, kind, fix):
     assert_same(as_tuple(P), golden_csr(golden, prob + "_" + fix), tol=1e-6)
 
 
+# ruge_stuben/tests/test_splitting.cpp / test_par_splitting.cpp (CLJP half)
+@pytest.mark.parametrize("lvl", [0, 1])
+def test_cljp_splitting(golden, lvl):
+    S = O.sort_diag_first(load(golden, "rss_S%d" % lvl))
+    states = O.split_cljp(S, golden["weights"])
+    np.testing.assert_array_equal(states, golden["rss_cf%d" % lvl])
+
+
 # ruge_stuben/tests/test_ruge_stuben.cpp: direct interpolation on the
 # CLJP splitting of the fixture hierarchy reproduces its prolongators
 @pytest.mark.parametrize("lvl", [0, 1])
@@ -113,6 +121,20 @@ def test_direct_interpolation_on_the_rss_hierarchy(golden, lvl):
     S = O.sort_diag_first(load(golden, "rss_S%d" % lvl))
     P = O.interpolation(A, S, golden["rss_cf%d" % lvl], kind="direct")
     assert_same(as_tuple(P), golden_csr(golden, "rss_P%d" % lvl), tol=1e-12)
+
+
+# ruge_stuben/tests/test_ruge_stuben.cpp: the whole chain, classical
+# strength 0.25 -> CLJP -> direct interpolation -> Galerkin product, twice
+def test_cljp_direct_chain_reproduces_the_fixture_hierarchy(golden):
+    A = O.sort_diag_first(load(golden, "rss_A0"))
+    w = golden["weights"]
+    for lvl in (0, 1):
+        S = O.sort_diag_first(O.classical_strength(A, 0.25))
+        cf = O.split_cljp(S, w)
+        np.testing.assert_array_equal(cf, golden["rss_cf%d" % lvl])
+        P = O.interpolation(A, S, cf, kind="direct")
+        A = O.rap(A, P)
+        assert_same(as_tuple(A), golden_csr(golden, "rss_A%d" % (lvl + 1)), tol=1e-6)
 
 
 # ruge_stuben/tests/test_par_rap.cpp

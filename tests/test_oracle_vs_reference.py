@@ -88,6 +88,10 @@ def test_pmis_interpolation_and_products(prob):
     REF.rs_split_pmis(n, srp, sci, scv, w.copy(), st_ref)
     st = O.split_pmis(S, w)
     np.testing.assert_array_equal(st_ref, st)
+    # CLJP through the reference's own split_cljp
+    cl_ref = np.zeros(n, np.int32)
+    REF.rs_split_cljp(n, srp, sci, scv, w.copy(), cl_ref)
+    np.testing.assert_array_equal(cl_ref, O.split_cljp(S, w))
     # The oracle follows the parallel interpolation (par_interpolation.cpp),
     # the one ParMultilevel calls.  It sums some weights in another order
     # than the sequential interpolation.cpp the shim calls (values agree to
