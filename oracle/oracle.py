@@ -66,6 +66,7 @@ def lib():
         L.oc_symmetric_strength.argtypes = [_P, C.c_double]
         L.oc_split_pmis.argtypes = [_P, _D, _I]
         L.oc_split_cljp.argtypes = [_P, _D, _I]
+        L.oc_split_rs.argtypes = [_P, _I, C.c_int, C.c_int]
         L.oc_mis2.argtypes = [_P, _D, _I]
         L.oc_aggregate.restype = C.c_int
         L.oc_aggregate.argtypes = [_P, _P, _I, _I, C.c_void_p]
@@ -236,6 +237,17 @@ def split_cljp(S, weights):
     st = np.zeros(max(S.shape[0], 1), np.int32)
     lib().oc_split_cljp(S.ptr, np.ascontiguousarray(weights[: S.shape[0]], np.float64), st)
     return st[: S.shape[0]]
+
+
+def split_rs(S, second_pass=True, states=None):
+    """RS splitting; with states given they are kept where assigned (the
+    parallel driver's NoNeighbors), else every point starts unassigned."""
+    n = S.shape[0]
+    st = np.zeros(max(n, 1), np.int32)
+    if states is not None:
+        st[:n] = states
+    lib().oc_split_rs(S.ptr, st, int(states is not None), int(second_pass))
+    return st[:n]
 
 
 def mis2(S, weights):
@@ -415,6 +427,7 @@ def ref_lib():
         L.rs_strength.argtypes = [C.c_int, _I, _I, _D, C.c_double, C.c_int]
         L.rs_split_pmis.argtypes = [C.c_int, _I, _I, _D, _D, _I]
         L.rs_split_cljp.argtypes = [C.c_int, _I, _I, _D, _D, _I]
+        L.rs_split_rs.argtypes = [C.c_int, _I, _I, _D, C.c_int, _I]
         L.rs_mis2.argtypes = [C.c_int, _I, _I, _D, _D, _I]
         L.rs_interp.restype = _P
         L.rs_interp.argtypes = [C.c_int, _I, _I, _D, _I, _I, _D, _I, C.c_int]

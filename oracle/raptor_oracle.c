@@ -491,6 +491,117 @@ void oc_split_pmis(const oc_csr* S, const double* rand_vals, int* states) {
 /* interpolation (ruge_stuben/par_interpolation.cpp)                        */
 /* ------------------------------------------------------------------------ */
 
+/* split_rs, ruge_stuben/cf_splitting.cpp:277-322: weights are the column
+ * counts of S (diagonal left out), rs_first_pass (:69-209) visits the points
+ * from the largest weight down through weight buckets (weight_ptr /
+ * weight_sizes / weight_idx_to_col / col_to_weight_idx, restated with the
+ * same moves so that ties resolve identically): an unassigned point becomes
+ * C, the unassigned points it influences become F and each unassigned
+ * strong neighbour of those gains weight, and the unassigned points that
+ * influence it lose weight; rs_second_pass (:211-275) promotes an F point to
+ * C when a strong F neighbour shares no C point with it.  prev_states keeps
+ * the caller's states (the parallel driver sets NoNeighbors first,
+ * par_cf_splitting.cpp:7-30 -> set_initial_states :114-131); otherwise every
+ * point starts unassigned.  HMIS and Falgout at world size 1 reduce to this:
+ * the first pass only, resp. both passes, followed by PMIS / CLJP loops that
+ * find nothing left to assign (par_cf_splitting.cpp:50-112). */
+void oc_split_rs(const oc_csr* S, int* states, int prev_states, int second_pass) {
+    int n = S->n_rows, nc = S->n_cols;
+    int *colptr, *colidx;
+    s_transpose(S, &colptr, &colidx);
+    if (!prev_states)
+        for (int i = 0; i < n; i++) states[i] = OC_UNASSIGNED;
+    int* w = (int*)malloc(sizeof(int) * ((size_t)nc + 1));
+    int* wptr = (int*)calloc((size_t)nc + 2, sizeof(int));
+    int* wsz = (int*)calloc((size_t)nc + 1, sizeof(int));
+    int* w2c = (int*)malloc(sizeof(int) * ((size_t)nc + 1));
+    int* c2w = (int*)malloc(sizeof(int) * ((size_t)nc + 1));
+    for (int i = 0; i < nc; i++) w[i] = colptr[i + 1] - colptr[i];
+    for (int i = 0; i < nc; i++) wsz[w[i]]++;
+    wptr[0] = 0;
+    for (int i = 0; i < nc; i++) {
+        wptr[i + 1] = wptr[i] + wsz[i];
+        wsz[i] = 0;
+    }
+    for (int i = 0; i < nc; i++) {
+        int wt = w[i];
+        int idx = wptr[wt] + wsz[wt]++;
+        w2c[idx] = i;
+        c2w[i] = idx;
+    }
+    for (int i = nc - 1; i >= 0; i--) {
+        int col = w2c[i];
+        wsz[w[col]]--;
+        if (states[col] != OC_UNASSIGNED) continue;
+        states[col] = OC_SELECTED;
+        for (int j = colptr[col]; j < colptr[col + 1]; j++) {
+            int idx = colidx[j];
+            if (states[idx] != OC_UNASSIGNED) continue;
+            states[idx] = OC_UNSELECTED;
+            int s = S->rowptr[idx], e = S->rowptr[idx + 1];
+            if (s < e && S->cols[s] == idx) s++;
+            for (int k = s; k < e; k++) {
+                int idx_k = S->cols[k];
+                if (states[idx_k] != OC_UNASSIGNED) continue;
+                int wk = w[idx_k];
+                if (wk >= nc - 1) continue;
+                int old_pos = c2w[idx_k];
+                int new_pos = wptr[wk] + wsz[wk] - 1;
+                c2w[w2c[old_pos]] = new_pos;
+                c2w[w2c[new_pos]] = old_pos;
+                int t = w2c[old_pos]; w2c[old_pos] = w2c[new_pos]; w2c[new_pos] = t;
+                wsz[wk] -= 1;
+                wsz[wk + 1] += 1;
+                wptr[wk + 1] = new_pos;
+                w[idx_k]++;
+            }
+        }
+        int s = S->rowptr[col], e = S->rowptr[col + 1];
+        if (s < e && S->cols[s] == col) s++;
+        for (int j = s; j < e; j++) {
+            int idx = S->cols[j];
+            if (states[idx] != OC_UNASSIGNED) continue;
+            int wt = w[idx];
+            if (wt == 0) continue;
+            int old_pos = c2w[idx];
+            int new_pos = wptr[wt];
+            c2w[w2c[old_pos]] = new_pos;
+            c2w[w2c[new_pos]] = old_pos;
+            int t = w2c[old_pos]; w2c[old_pos] = w2c[new_pos]; w2c[new_pos] = t;
+            wsz[wt] -= 1;
+            wsz[wt - 1] += 1;
+            wptr[wt] += 1;
+            wptr[wt - 1] = wptr[wt] - wsz[wt - 1];
+            w[idx]--;
+        }
+    }
+    if (second_pass) {
+        int* row_coarse = (int*)malloc(sizeof(int) * ((size_t)n + 1));
+        for (int i = 0; i < n; i++) row_coarse[i] = -1;
+        for (int i = 0; i < n; i++) {
+            if (states[i] == OC_SELECTED) continue;
+            int s = S->rowptr[i], e = S->rowptr[i + 1];
+            for (int j = s; j < e; j++)
+                if (states[S->cols[j]] == OC_SELECTED) row_coarse[S->cols[j]] = i;
+            for (int j = s; j < e; j++) {
+                int col = S->cols[j];
+                if (states[col] != OC_UNSELECTED) continue;
+                int sk = S->rowptr[col], ek = S->rowptr[col + 1];
+                if (sk == ek) continue;
+                int connection = 0;
+                for (int k = sk; k < ek; k++)
+                    if (row_coarse[S->cols[k]] == i) { connection = 1; break; }
+                if (!connection) {
+                    row_coarse[col] = i;
+                    states[col] = OC_SELECTED;
+                }
+            }
+        }
+        free(row_coarse);
+    }
+    free(colptr); free(colidx); free(w); free(wptr); free(wsz); free(w2c); free(c2w);
+}
+
 /* split_cljp, ruge_stuben/cf_splitting.cpp:649-675 -> cljp_main_loop
  * (:479-545): weights = rand_vals + the number of rows in which a point is a
  * strong column; each round selects every unassigned point whose weight is

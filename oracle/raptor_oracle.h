@@ -132,6 +132,7 @@ oc_csr* oc_classical_strength(const oc_csr* A, double theta);
 oc_csr* oc_symmetric_strength(const oc_csr* A, double theta);
 void oc_split_pmis(const oc_csr* S, const double* rand_vals, int* states);
 void oc_split_cljp(const oc_csr* S, const double* rand_vals, int* states);
+void oc_split_rs(const oc_csr* S, int* states, int prev_states, int second_pass);
 oc_csr* oc_mod_classical_interp(const oc_csr* A, const oc_csr* S, const int* states);
 oc_csr* oc_direct_interp(const oc_csr* A, const oc_csr* S, const int* states);
 oc_csr* oc_extended_interp(const oc_csr* A, const oc_csr* S, const int* states,

@@ -138,6 +138,15 @@ void rs_split_pmis(int n, const int* rp, const int* ci, const double* cv, double
     delete S;
 }
 
+void rs_split_rs(int n, const int* rp, const int* ci, const double* cv, int second_pass,
+                 int* states_out) {
+    CSRMatrix* S = make_csr(n, n, rp, ci, cv);
+    aligned_vector<int> states;
+    split_rs(S, states, false, second_pass != 0);
+    for (int i = 0; i < n; i++) states_out[i] = states[i];
+    delete S;
+}
+
 void rs_split_cljp(int n, const int* rp, const int* ci, const double* cv, double* weights,
                    int* states_out) {
     CSRMatrix* S = make_csr(n, n, rp, ci, cv);

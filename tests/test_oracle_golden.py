@@ -113,6 +113,15 @@ def test_cljp_splitting(golden, lvl):
     np.testing.assert_array_equal(states, golden["rss_cf%d" % lvl])
 
 
+# ruge_stuben/tests/test_splitting.cpp (Ruge-Stuben half): level 0 with both
+# passes, level 1 with the first pass only, as the reference tests them
+@pytest.mark.parametrize("lvl", [0, 1])
+def test_rs_splitting(golden, lvl):
+    S = O.sort_diag_first(load(golden, "rss_S%d" % lvl))
+    states = O.split_rs(S, second_pass=(lvl == 0))
+    np.testing.assert_array_equal(states, golden["rss_cf%d_rs" % lvl])
+
+
 # ruge_stuben/tests/test_ruge_stuben.cpp: direct interpolation on the
 # CLJP splitting of the fixture hierarchy reproduces its prolongators
 @pytest.mark.parametrize("lvl", [0, 1])

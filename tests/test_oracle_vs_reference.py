@@ -92,6 +92,11 @@ def test_pmis_interpolation_and_products(prob):
     cl_ref = np.zeros(n, np.int32)
     REF.rs_split_cljp(n, srp, sci, scv, w.copy(), cl_ref)
     np.testing.assert_array_equal(cl_ref, O.split_cljp(S, w))
+    # Ruge-Stuben (both passes, and the first pass alone) through split_rs
+    for second in (1, 0):
+        rs_ref = np.zeros(n, np.int32)
+        REF.rs_split_rs(n, srp, sci, scv, second, rs_ref)
+        np.testing.assert_array_equal(rs_ref, O.split_rs(S, second_pass=bool(second)))
     # The oracle follows the parallel interpolation (par_interpolation.cpp),
     # the one ParMultilevel calls.  It sums some weights in another order
     # than the sequential interpolation.cpp the shim calls (values agree to
