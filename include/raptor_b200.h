@@ -56,7 +56,8 @@ int rb_csr_destroy(rb_csr A);
 int rb_csr_info(rb_csr A, int* n_rows, int* n_cols, int64_t* nnz);
 /* Copy the matrix to host buffers of n_rows+1, nnz and nnz entries. */
 int rb_csr_download(rb_csr A, int* rowptr, int* cols, double* vals);
-/* Device pointers of the matrix arrays (borrowed). */
+/* Device pointers of the matrix arrays (borrowed).  Values may be rewritten
+ * in place between calls; the pattern (rowptr, cols) may not. */
 int rb_csr_device_arrays(rb_csr A, int** rowptr, int** cols, double** vals);
 /* CSRMatrix::sort then move_diag (core/matrix.cpp:588-618, :730-786). */
 int rb_csr_sort_diag_first(rb_csr A);
@@ -83,7 +84,9 @@ int rb_vec_norm2(rb_vec a, double* out);         /* ParVector::norm(2), par_vect
 int rb_spmv(rb_csr A, rb_vec x, rb_vec b);
 /* ParMatrix::residual, r = b - A x (par_spmv.cpp:215-252 -> spmv.cpp:69-85) */
 int rb_residual(rb_csr A, rb_vec x, rb_vec b, rb_vec r);
-/* ParMatrix::mult_T, b = A^T x (par_spmv.cpp:157-187 -> spmv.cpp:150-163) */
+/* ParMatrix::mult_T, b = A^T x (par_spmv.cpp:157-187 -> spmv.cpp:150-163).
+ * The first call on a matrix builds and keeps A^T's pattern on the handle;
+ * later calls gather A's current values through it. */
 int rb_spmv_T(rb_csr A, rb_vec x, rb_vec b);
 /* ParMatrix::mult_append, b += A x (par_spmv.cpp:91-125 -> spmv.cpp:88-103) */
 int rb_spmv_append(rb_csr A, rb_vec x, rb_vec b);
@@ -240,6 +243,10 @@ int rb_amg_level_storage(rb_amg ml, int level, int* ndiag);
 /* Kernels this library has launched so far (graph replays count their
  * kernel nodes). */
 int rb_launch_count(int64_t* count);
+/* Device allocations (cudaMalloc) this library has made so far.  No
+ * counterpart in the reference; a diagnostic for callers that audit
+ * allocation-free paths. */
+int rb_device_alloc_count(int64_t* count);
 
 /* ||b - A x||_2 into norm_out[0] without allocating device memory.  No
  * counterpart in the reference.  For callers that must not allocate while

@@ -2,11 +2,16 @@
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
 legs import this module.  It loads ``oracle/_build/libraptor_oracle.so``
-(building it first when it is missing and gcc is available) and, for
-cross-checks in the build container, ``oracle/_ref/libraptor_seq_ref.so``.
+(building it first when it is missing and gcc is available) and, where they
+were built (oracle/build.py), the reference's own code:
+``oracle/_ref/libraptor_seq_ref.so`` (sequential routines) and
+``oracle/_ref/libraptor_par_ref{,_jfix}.so`` (the parallel solve path at one
+rank; ``_jfix`` with the Jacobi sweep fixed).
 """
+import contextlib
 import ctypes as C
 import os
+import sys
 
 import numpy as np
 
@@ -446,3 +451,247 @@ def ref_take(ptr):
     L.rs_export(ptr, rp, ci, cv)
     L.rs_free(ptr)
     return (r.value, c.value), rp, ci[: z.value], cv[: z.value]
+
+
+# --- the reference's own parallel solve path (oracle/_ref/libraptor_par_ref*.so)
+
+# the reference's enums (raptor/core/types.hpp:156-162)
+REF_COARSEN = {"rs": 0, "cljp": 1, "falgout": 2, "pmis": 3, "hmis": 4}
+REF_INTERP = {"direct": 0, "mod_classical": 1, "extended": 2}
+REF_RELAX = {"jacobi": 0, "sor": 1, "ssor": 2}
+REF_STRENGTH = {"classical": 0, "symmetric": 1}
+
+
+class RefOpts(C.Structure):
+    _fields_ = [
+        ("solver", C.c_int), ("theta", C.c_double), ("coarsen", C.c_int),
+        ("interp", C.c_int), ("strength", C.c_int), ("relax", C.c_int),
+        ("relax_weight", C.c_double), ("num_smooth_sweeps", C.c_int),
+        ("interp_filter", C.c_double), ("max_coarse", C.c_int), ("max_levels", C.c_int),
+    ]
+
+
+_par = {}
+
+
+def par_ref(jacobi_fix=False):
+    """The reference's parallel path compiled at one rank, or None if not built."""
+    key = bool(jacobi_fix)
+    if key in _par:
+        return _par[key]
+    so = _build.PAR_JFIX_SO if key else _build.PAR_SO
+    if not os.path.exists(so):
+        try:
+            _build.build_reference_parallel()
+        except Exception:  # noqa: BLE001 - no compiler, checkout or OpenBLAS
+            pass
+    if not os.path.exists(so):
+        _par[key] = None
+        return None
+    L = C.CDLL(so)
+    L.rp_matrix_from_csr.restype = _P
+    L.rp_matrix_from_csr.argtypes = [C.c_int, _I, _I, _D]
+    L.rp_diffusion_grid.restype = _P
+    L.rp_diffusion_grid.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int]
+    L.rp_laplace27_grid.restype = _P
+    L.rp_laplace27_grid.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.rp_stencil_grid.restype = _P
+    L.rp_stencil_grid.argtypes = [_D, _I, C.c_int]
+    L.rp_matrix_free.argtypes = [_P]
+    L.rp_matrix_info.argtypes = [_P, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_longlong)]
+    L.rp_matrix_export.restype = C.c_int
+    L.rp_matrix_export.argtypes = [_P, _I, _I, _D]
+    L.rp_spmv.argtypes = [_P, _D, _D]
+    L.rp_spmv_T.argtypes = [_P, _D, _D]
+    L.rp_residual.argtypes = [_P, _D, _D, _D]
+    L.rp_default_opts.argtypes = [C.POINTER(RefOpts)]
+    L.rp_setup.restype = _P
+    L.rp_setup.argtypes = [_P, C.POINTER(RefOpts)]
+    L.rp_free.argtypes = [_P]
+    L.rp_num_levels.restype = C.c_int
+    L.rp_num_levels.argtypes = [_P]
+    L.rp_level.restype = _P
+    L.rp_level.argtypes = [_P, C.c_int, C.c_int]
+    L.rp_level_states.restype = C.c_int
+    L.rp_level_states.argtypes = [_P, C.c_int, _I]
+    L.rp_solve.restype = C.c_int
+    L.rp_solve.argtypes = [_P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+    L.rp_cycle.argtypes = [_P, _D, _D, C.c_int]
+    L.rp_pcg.restype = C.c_int
+    L.rp_pcg.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+    L.rp_cg.restype = C.c_int
+    L.rp_cg.argtypes = [_P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+    L.rp_bicgstab.restype = C.c_int
+    L.rp_bicgstab.argtypes = [_P, _D, _D, C.c_double, C.c_int, _D, C.c_int]
+    L.rp_pending_messages.restype = C.c_int
+    _par[key] = L
+    return L
+
+
+@contextlib.contextmanager
+def quiet_stdout():
+    """Send the C library's stdout to stderr (the reference's PCG and
+    BiCGStab print their iteration counts with printf)."""
+    libc = C.CDLL(None)
+    sys.stdout.flush()
+    libc.fflush(None)
+    saved = os.dup(1)
+    try:
+        os.dup2(2, 1)
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
+def _ref_arrays(L, ptr):
+    r, c, z = C.c_int(), C.c_int(), C.c_longlong()
+    L.rp_matrix_info(ptr, C.byref(r), C.byref(c), C.byref(z))
+    rp = np.zeros(r.value + 1, np.int32)
+    ci = np.zeros(max(z.value, 1), np.int32)
+    cv = np.zeros(max(z.value, 1), np.float64)
+    if L.rp_matrix_export(ptr, rp, ci, cv) != 0:
+        raise RuntimeError("reference matrix has off-process entries at one rank")
+    return (r.value, c.value), rp, ci[: z.value], cv[: z.value]
+
+
+class RefMatrix:
+    """A reference ParCSRMatrix (owned unless borrowed from a hierarchy)."""
+
+    def __init__(self, L, ptr, owner=None):
+        self.L, self.ptr, self._owner = L, ptr, owner
+
+    @classmethod
+    def from_csr(cls, L, rowptr, cols, vals):
+        rp = np.ascontiguousarray(rowptr, np.int32)
+        return cls(L, L.rp_matrix_from_csr(len(rp) - 1, rp, np.ascontiguousarray(cols, np.int32),
+                                           np.ascontiguousarray(vals, np.float64)))
+
+    @classmethod
+    def diffusion(cls, L, eps, theta, nx, ny):
+        return cls(L, L.rp_diffusion_grid(eps, theta, nx, ny))
+
+    @classmethod
+    def laplace27(cls, L, nx, ny, nz):
+        return cls(L, L.rp_laplace27_grid(nx, ny, nz))
+
+    @classmethod
+    def stencil(cls, L, stencil, grid):
+        return cls(L, L.rp_stencil_grid(np.ascontiguousarray(stencil, np.float64),
+                                        np.ascontiguousarray(grid, np.int32), len(grid)))
+
+    def __del__(self):
+        if self._owner is None and getattr(self, "ptr", None):
+            self.L.rp_matrix_free(self.ptr)
+            self.ptr = None
+
+    @property
+    def shape(self):
+        r, c, z = C.c_int(), C.c_int(), C.c_longlong()
+        self.L.rp_matrix_info(self.ptr, C.byref(r), C.byref(c), C.byref(z))
+        return r.value, c.value, z.value
+
+    def arrays(self):
+        return _ref_arrays(self.L, self.ptr)[1:]
+
+    def spmv(self, x):
+        y = np.zeros(self.shape[0])
+        self.L.rp_spmv(self.ptr, np.ascontiguousarray(x, np.float64), y)
+        return y
+
+    def spmv_T(self, x):
+        y = np.zeros(self.shape[1])
+        self.L.rp_spmv_T(self.ptr, np.ascontiguousarray(x, np.float64), y)
+        return y
+
+    def residual(self, x, b):
+        r = np.zeros(self.shape[0])
+        self.L.rp_residual(self.ptr, np.ascontiguousarray(x, np.float64),
+                           np.ascontiguousarray(b, np.float64), r)
+        return r
+
+
+def ref_opts(L, **kw):
+    """Options of the reference's solver classes; strings name its enums."""
+    o = RefOpts()
+    L.rp_default_opts(C.byref(o))
+    maps = {"coarsen": REF_COARSEN, "interp": REF_INTERP, "relax": REF_RELAX,
+            "strength": REF_STRENGTH, "solver": {"rs": 0, "sa": 1}}
+    for k, v in kw.items():
+        if isinstance(v, str):
+            v = maps[k][v]
+        setattr(o, k, v)
+    return o
+
+
+class RefHierarchy:
+    """ml = new ParRugeStubenSolver / ParSmoothedAggregationSolver; ml->setup(A)."""
+
+    def __init__(self, A, **kw):
+        self.L = A.L
+        self.opts = ref_opts(self.L, **kw)
+        self.A0 = A
+        self.ptr = self.L.rp_setup(A.ptr, C.byref(self.opts))
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            self.L.rp_free(self.ptr)
+            self.ptr = None
+
+    @property
+    def num_levels(self):
+        return self.L.rp_num_levels(self.ptr)
+
+    def A(self, l):
+        return RefMatrix(self.L, self.L.rp_level(self.ptr, l, 0), owner=self)
+
+    def P(self, l):
+        return RefMatrix(self.L, self.L.rp_level(self.ptr, l, 1), owner=self)
+
+    def states(self, l):
+        n = self.A(l).shape[0]
+        st = np.zeros(max(n, 1), np.int32)
+        if self.L.rp_level_states(self.ptr, l, st) < 0:
+            raise ValueError("states exist for Ruge-Stuben levels above the coarsest")
+        return st[:n]
+
+    def solve(self, x, b, tol=1e-8, max_iter=100):
+        x = np.ascontiguousarray(x, np.float64).copy()
+        hist = np.zeros(max_iter + 1)
+        it = self.L.rp_solve(self.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter,
+                             hist, len(hist))
+        return x, it, hist[: it + 1]
+
+    def cycle(self, x, b, level=0):
+        x = np.ascontiguousarray(x, np.float64).copy()
+        self.L.rp_cycle(self.ptr, x, np.ascontiguousarray(b, np.float64), level)
+        return x
+
+
+def ref_pcg(A, ml, x, b, tol=1e-5, max_iter=-1, cap=10000):
+    """The reference's PCG(A, ml, x, b, res, tol, max_iter)."""
+    x = np.ascontiguousarray(x, np.float64).copy()
+    hist = np.zeros(cap)
+    with quiet_stdout():
+        nh = A.L.rp_pcg(A.ptr, ml.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter,
+                        hist, cap)
+    return x, hist[: min(nh, cap)]
+
+
+def ref_cg(A, x, b, tol=1e-5, max_iter=-1, cap=10000):
+    x = np.ascontiguousarray(x, np.float64).copy()
+    hist = np.zeros(cap)
+    with quiet_stdout():
+        nh = A.L.rp_cg(A.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter, hist, cap)
+    return x, hist[: min(nh, cap)]
+
+
+def ref_bicgstab(A, x, b, tol=1e-5, max_iter=-1, cap=10000):
+    x = np.ascontiguousarray(x, np.float64).copy()
+    hist = np.zeros(cap)
+    with quiet_stdout():
+        nh = A.L.rp_bicgstab(A.ptr, x, np.ascontiguousarray(b, np.float64), tol, max_iter, hist,
+                             cap)
+    return x, hist[: min(nh, cap)]

@@ -117,6 +117,7 @@ SIGNATURES = {
     "rb_amg_level_storage": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "rb_residual_norm_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "rb_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
+    "rb_device_alloc_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rb_pcg": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_int, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),
     "rb_fv_assemble": (C.c_int, [C.c_int, C.c_int, _P, _PP]),
     "rb_fv_backward": (C.c_int, [C.c_int, C.c_int, _P, _P, _P, _P]),

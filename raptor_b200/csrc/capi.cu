@@ -167,6 +167,7 @@ int rb_csr_sort_diag_first(rb_csr A) {
         NEED(A);
         sort_rows_diag_first(*A, true);
         RB_CHECK_LAUNCH();
+        A->tmap.reset();  // entry positions moved
         return RB_OK;
     });
 }
@@ -323,9 +324,9 @@ int rb_spmv_T(rb_csr A, rb_vec x, rb_vec b) {
     return guarded([&]() -> int {
         NEED(A); NEED(x); NEED(b);
         RB_REQUIRE(x->n == A->n_rows && b->n == A->n_cols, "spmv_T: sizes do not match");
-        // the transpose is a gather over A^T: deterministic, no atomics
-        std::unique_ptr<rb_csr_s> T(transpose(*A));
-        spmv64(view(*T), x->v.get(), b->v.get());
+        // a gather over A^T's pattern, cached on the handle: deterministic,
+        // no atomics, no allocation after the first call
+        spmv_T64(*A, x->v.get(), b->v.get());
         RB_CUDA(cudaStreamSynchronize(stream()));
         return RB_OK;
     });
@@ -782,6 +783,14 @@ int rb_launch_count(int64_t* count) {
     return guarded([&]() -> int {
         NEED(count);
         *count = launch_counter();
+        return RB_OK;
+    });
+}
+
+int rb_device_alloc_count(int64_t* count) {
+    return guarded([&]() -> int {
+        NEED(count);
+        *count = device_alloc_counter();
         return RB_OK;
     });
 }

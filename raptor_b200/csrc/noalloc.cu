@@ -37,6 +37,7 @@
 
 namespace rb {
 void set_last_error(const std::string& msg);
+long long& launch_counter();
 }
 
 namespace {
@@ -121,9 +122,9 @@ extern "C" int rb_residual_norm_noalloc(int n_rows, const int* rowptr, const int
                                         const double* vals, const double* x, const double* b,
                                         double* norm_out, void* stream) {
     rb::set_last_error("");
-    if (n_rows < 0 || (long long)n_rows > kNoAllocMaxRows)
-        return fail(RB_ERR_INVALID, "n_rows > 2^24");
-    if (!rowptr || !norm_out || (n_rows > 0 && (!x || !b)))
+    if (n_rows < 0) return fail(RB_ERR_INVALID, "n_rows < 0");
+    if ((long long)n_rows > kNoAllocMaxRows) return fail(RB_ERR_INVALID, "n_rows > 2^24");
+    if (!rowptr || !norm_out || (n_rows > 0 && (!cols || !vals || !x || !b)))
         return fail(RB_ERR_INVALID, "NULL argument");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
@@ -142,6 +143,8 @@ extern "C" int rb_residual_norm_noalloc(int n_rows, const int* rowptr, const int
         scratch = g_scratch_addr[dev];
     }
     cudaStream_t st = (cudaStream_t)stream;
+    // an error left pending by earlier, unrelated work is not this call's
+    (void)cudaGetLastError();
     const int blocks = n_rows > 0 ? (int)((n_rows + kRowsPerBlock - 1) / kRowsPerBlock) : 1;
     // the completion counter must start at zero
     if (cudaMemsetAsync((unsigned char*)scratch + kNoAllocMaxBlocks * sizeof(double), 0,
@@ -150,5 +153,6 @@ extern "C" int rb_residual_norm_noalloc(int n_rows, const int* rowptr, const int
     k_residual_norm<<<blocks, kBlock, 0, st>>>(n_rows, rowptr, cols, vals, x, b, norm_out,
                                                (unsigned char*)scratch);
     if (cudaGetLastError() != cudaSuccess) return fail(RB_ERR_CUDA, "kernel launch");
+    ++rb::launch_counter();
     return RB_OK;
 }

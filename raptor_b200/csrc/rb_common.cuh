@@ -60,6 +60,10 @@ int grid_per_sm(const char* env, int dflt);
 // (the occupancy calculator's answer, cached per kernel).
 int resident_blocks_per_sm(const void* fn, int threads);
 
+// Device allocations made through DevArray so far (every device buffer of
+// the library is one); read through rb_device_alloc_count.
+long long& device_alloc_counter();
+
 // Owning device array (cudaMalloc'd; freed on destruction).
 template <typename T>
 struct DevArray {
@@ -81,7 +85,10 @@ struct DevArray {
     void alloc(size_t count) {
         release();
         n = count;
-        if (count) RB_CUDA(cudaMalloc(&p, sizeof(T) * count));
+        if (count) {
+            RB_CUDA(cudaMalloc(&p, sizeof(T) * count));
+            ++::rb::device_alloc_counter();
+        }
     }
     void release() {
         if (p) cudaFree(p);

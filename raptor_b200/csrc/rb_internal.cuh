@@ -1,15 +1,28 @@
 // rb_internal.cuh -- handle types behind the C ABI and shared declarations.
 #pragma once
 
+#include <memory>
 #include <vector>
 
 #include "rb_common.cuh"
+
+namespace rb {
+// The pattern of A^T with, for each of its entries, the position in A's
+// value array it comes from: rows of A^T list source rows in increasing
+// order.  Built on the first transposed product and kept on the handle, so
+// later products gather A's current values through it (values may change
+// between calls, the pattern may not).
+struct TransposeMap {
+    DevArray<int> rowptr, rows, src;
+};
+}  // namespace rb
 
 struct rb_csr_s {
     int n_rows = 0, n_cols = 0;
     long long nnz = 0;
     rb::DevArray<int> rowptr, cols;
     rb::DevArray<double> vals;
+    std::unique_ptr<rb::TransposeMap> tmap;  // lazily built by spmv_T64
 };
 
 struct rb_batch_s;
@@ -65,6 +78,8 @@ void dot_async(const double* a, const double* b, int n, double* result_dev);
 void spmv64(const CsrView<double>& A, const double* x, double* y);
 void residual64(const CsrView<double>& A, const double* x, const double* b, double* r);
 void spmv_append64(const CsrView<double>& A, const double* x, double* y);
+// y = A^T x through the handle's cached transpose map (built on first use).
+void spmv_T64(rb_csr_s& A, const double* x, double* y);
 
 // Setup components (setup.cu).
 rb_csr_s* strength(const rb_csr_s& A, int kind, double theta);

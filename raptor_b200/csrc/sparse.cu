@@ -25,6 +25,10 @@ long long& launch_counter() {
     static long long c = 0;
     return c;
 }
+long long& device_alloc_counter() {
+    static long long c = 0;
+    return c;
+}
 const char* last_error_cstr() { return g_last_error.c_str(); }
 
 cudaStream_t stream() {
@@ -198,6 +202,65 @@ rb_csr_s* transpose(const rb_csr_s& A) {
     // atomics leave each row in arbitrary order: sort by source row
     sort_rows_diag_first(*T, false);
     return T;
+}
+
+// ------------------------------------------------- transposed product --
+__global__ void k_iota_vals(long long nnz, double* v) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+         k += (long long)gridDim.x * blockDim.x)
+        v[k] = (double)k;
+}
+
+__global__ void k_to_int(long long nnz, const double* v, int* out) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+         k += (long long)gridDim.x * blockDim.x)
+        out[k] = (int)v[k];
+}
+
+// y_j = sum over the entries of row j of A^T of vals[src] * x[row]: 8 lanes
+// per row, each lane a fixed stride of the row, then a fixed shuffle tree,
+// so the result does not depend on scheduling.
+__global__ void __launch_bounds__(256)
+k_spmv_T_map(int n, const int* __restrict__ rp, const int* __restrict__ rows,
+             const int* __restrict__ src, const double* __restrict__ vals,
+             const double* __restrict__ x, double* __restrict__ y) {
+    constexpr int G = 8;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long j = t / G;
+    const int g = threadIdx.x & (G - 1);
+    double s = 0.0;
+    if (j < n)
+        for (int k = rp[j] + g; k < rp[j + 1]; k += G) s += vals[src[k]] * x[rows[k]];
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
+    if (j < n && g == 0) y[j] = s;
+}
+
+void spmv_T64(rb_csr_s& A, const double* x, double* y) {
+    if (!A.tmap) {
+        // transpose a copy of A whose values are the entry positions: the
+        // transposed values are then the source positions, in the order the
+        // deterministic transpose leaves its rows
+        std::unique_ptr<rb_csr_s> I(clone_csr(A));
+        if (A.nnz)
+            k_iota_vals<<<grid_for(A.nnz, 256), 256, 0, stream()>>>(A.nnz, I->vals.get());
+        RB_CHECK_LAUNCH();
+        std::unique_ptr<rb_csr_s> T(transpose(*I));
+        auto m = std::make_unique<TransposeMap>();
+        m->src.alloc((size_t)A.nnz + 1);
+        if (A.nnz)
+            k_to_int<<<grid_for(A.nnz, 256), 256, 0, stream()>>>(A.nnz, T->vals.get(),
+                                                                  m->src.get());
+        RB_CHECK_LAUNCH();
+        m->rowptr = std::move(T->rowptr);
+        m->rows = std::move(T->cols);
+        A.tmap = std::move(m);
+    }
+    if (A.n_cols)
+        k_spmv_T_map<<<grid_for((long)A.n_cols * 8, 256), 256, 0, stream()>>>(
+            A.n_cols, A.tmap->rowptr.get(), A.tmap->rows.get(), A.tmap->src.get(), A.vals.get(),
+            x, y);
+    RB_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------- dots --

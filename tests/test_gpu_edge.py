@@ -133,3 +133,44 @@ def test_errors_are_status_codes():
     bad = C.c_double()
     assert L.rb_amg_time_operator(ml.h, 0, 9, 3, C.byref(bad)) == -1   # unknown operator
     assert L.rb_amg_level_info(ml.h, 99, None, None, None) == -1       # level out of range
+
+
+def test_mult_T_reuses_its_transpose_and_follows_value_changes():
+    """rb_spmv_T keeps A^T's pattern on the handle after the first call and
+    gathers A's current values through it; reordering the rows
+    (sort_diag_first) drops the kept pattern."""
+    Ao = O.stencil_grid(O.diffusion_stencil_2d(0.001, np.pi / 8), [37, 23])
+    n, m, _ = Ao.shape
+    rp, ci, cv = Ao.arrays()
+    A = rb.ParCSRMatrix.from_arrays(n, m, rp, ci, cv)
+    xh = np.random.default_rng(4).uniform(-1, 1, n)
+    x = rb.ParVector(n, values=xh)
+    y = rb.ParVector(m)
+    for _ in range(2):
+        A.mult_T(x, y)
+        np.testing.assert_allclose(y.numpy(), O.spmv_T(Ao, xh), rtol=1e-13, atol=1e-14)
+    allocs = C.c_int64()
+    rb.check(rb.lib().rb_device_alloc_count(C.byref(allocs)))
+    A.mult_T(x, y)
+    after = C.c_int64()
+    rb.check(rb.lib().rb_device_alloc_count(C.byref(after)))
+    assert after.value == allocs.value
+    # new values through the borrowed device pointers
+    torch = pytest.importorskip("torch")
+    p_rp, p_ci, p_cv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    rb.check(rb.lib().rb_csr_device_arrays(A.h, C.byref(p_rp), C.byref(p_ci), C.byref(p_cv)))
+    cv2 = cv * 1.5 + 0.25
+
+    class _Vals:  # the library's value array as a torch tensor (no copy)
+        __cuda_array_interface__ = {"shape": (len(cv2),), "typestr": "<f8",
+                                    "data": (p_cv.value, False), "version": 3}
+
+    rb.check(rb.lib().rb_synchronize())
+    torch.as_tensor(_Vals(), device="cuda").copy_(torch.from_numpy(cv2))
+    torch.cuda.synchronize()
+    A.mult_T(x, y)
+    Ao2 = O.CSR.from_arrays(n, m, rp, ci, cv2)
+    np.testing.assert_allclose(y.numpy(), O.spmv_T(Ao2, xh), rtol=1e-13, atol=1e-14)
+    A.sort_diag_first()
+    A.mult_T(x, y)
+    np.testing.assert_allclose(y.numpy(), O.spmv_T(Ao2, xh), rtol=1e-13, atol=1e-14)

@@ -6,7 +6,9 @@ scratch is a static device array shared by
 every call and left holding the last call's contents, so this test calls it
 twice in a row and checks both results against rb_residual followed by
 rb_vec_norm2 (which allocate), within the 1e-12 relative tolerance used for
-solve-phase values.  It sits in a file of its own that pytest collects last,
+solve-phase values, and that the library's device-allocation count
+(rb_device_alloc_count, bumped by every cudaMalloc the library makes) does
+not move across the two calls.  It sits in a file of its own that pytest collects last,
 and passes alone in a fresh process as well as after the other tests.
 """
 import ctypes as C
@@ -51,6 +53,8 @@ def test_residual_norm_noalloc_matches_allocating_path(shape, caller_stream):
     ref = r.norm(2)
     out = rb.ParVector(1)
     rp, ci, cv = _dev_ptrs(A)
+    allocs_before = C.c_int64()
+    rb.check(rb.lib().rb_device_alloc_count(C.byref(allocs_before)))
     for _ in range(2):   # two calls in a row share the static scratch
         out.set_const_value(-1.0)
         rc = rb.lib().rb_residual_norm_noalloc(n, rp, ci, cv, C.c_void_p(x.device_ptr()),
@@ -60,13 +64,21 @@ def test_residual_norm_noalloc_matches_allocating_path(shape, caller_stream):
         rb.lib().rb_synchronize()
         got = out.numpy()[0]
         assert abs(got - ref) <= 1e-12 * ref, (got, ref)
+    allocs_after = C.c_int64()
+    rb.check(rb.lib().rb_device_alloc_count(C.byref(allocs_after)))
+    assert allocs_after.value == allocs_before.value
 
 
-def test_residual_norm_noalloc_rejects_oversized_input():
+def test_residual_norm_noalloc_rejects_bad_arguments():
     rb.init(0)
-    # rejected before any pointer is touched
-    rc = rb.lib().rb_residual_norm_noalloc((1 << 24) + 1, C.c_void_p(1), C.c_void_p(1),
-                                           C.c_void_p(1), C.c_void_p(1), C.c_void_p(1),
-                                           C.c_void_p(1), None)
-    assert rc == -1
-    assert "2^24" in rb.last_error()
+    # every case is rejected on the host before any pointer is touched
+    one = C.c_void_p(1)
+    rc = rb.lib().rb_residual_norm_noalloc((1 << 24) + 1, one, one, one, one, one, one, None)
+    assert rc == -1 and "2^24" in rb.last_error()
+    rc = rb.lib().rb_residual_norm_noalloc(-1, one, one, one, one, one, one, None)
+    assert rc == -1 and "< 0" in rb.last_error()
+    for null_at in range(6):
+        args = [one] * 6
+        args[null_at] = None
+        rc = rb.lib().rb_residual_norm_noalloc(10, *args, None)
+        assert rc == -1 and "NULL" in rb.last_error(), null_at
