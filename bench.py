@@ -16,9 +16,18 @@ alone is larger than L2, so no flush is needed); `e2e` times the public API
 with host buffers: pinned b uploaded and x downloaded every step.
 
 Under torchrun each rank solves its own copy (replicas; the solve does not
-shard), timings are the max over ranks.  `--impl reference` times the CPU
-restatement of the reference's algorithm (the reference's own AMG path needs
-MPI and cannot be built here) on a bounded sample on rank 0.
+shard), timings are the max over ranks.
+
+`--impl reference` times the reference's own solve path on the host, rank 0
+only: its ParRugeStubenSolver setup (untimed) and PCG, compiled unmodified
+into oracle/_ref against a single-rank MPI stand-in (one core: the
+reference has no threads), on the same 192^3 problem, with the reference's
+default SOR smoother (it has no L1-Jacobi) and its PCG tolerance calibrated
+so that the solution meets the same ||b - A x|| / ||b|| <= 1e-8.  Where that
+build is absent, the CPU restatement (oracle/) runs the same solve instead,
+on every host core.  The GPU line's `cpu_baseline` is one such reference
+solve on the hierarchy the GPU built (bit-identical to the reference's own
+setup, as the parity tests show), so the sample needs no CPU setup.
 """
 import argparse
 import json
@@ -38,6 +47,19 @@ sys.path.insert(0, ROOT)
 SEED = 20261203
 METRIC = "AMG-PCG time to 1e-8 rel-res"
 TOL = 1e-8
+WORKLOAD = ("laplacian27 %d^3, b ~ U[-1,1]: AMG-PCG to ||b - A x|| / ||b|| <= 1e-8 "
+            "(RS: classical strength 0.25, PMIS, extended+i interpolation, filter 0.3)")
+# the reference's solver options for the same problem (its default SOR
+# smoother: its Jacobi sweep is a no-op and it has no L1-Jacobi)
+REF_KW = dict(theta=0.25, coarsen="pmis", interp="extended", interp_filter=0.3, relax="sor")
+
+
+def bench_config(S, n, nnz, levels, world):
+    """The workload both arms report (the smoother and precisions each arm
+    uses are reported beside it, under "method")."""
+    return {"workload": WORKLOAD % S, "rows": n, "nnz": nnz, "levels": levels,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (A0 FP64 = %.2f GB)" % (nnz * 12 / 1e9)}
 
 
 def parse():
@@ -144,6 +166,13 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first(self, timeout=3.0):
+        """Block until nvidia-smi has printed a sample (it takes a moment to
+        start), so that the timed region that follows is sampled."""
+        t0 = time.perf_counter()
+        while self.proc and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.02)
+
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -187,22 +216,28 @@ def cycle_bytes(ml, vbytes):
     Per level l with n rows, p = nnz(P_l), v = value bytes, i = 4: B_A = one
     pass over A_l in its stored format (a_bytes), B_P = B_R = p(v+i) +
     (rows+1)i.  Pre-smooth from a zero guess reads b and the inverse diagonal
-    and writes x (3nv); residual B_A + 3nv; restriction B_R + n v + n_c v;
-    prolongation B_P + (2n + n_c) v; post-smooth B_A + 4nv (x, b, D^-1 in, x
-    out).  Coarsest level: the dense LU (2 n_c^2 8 bytes)."""
+    and writes x (3nv), then the residual B_A + 3nv; where the level runs the
+    two as one pass (level_fused_first) that pass is B_A + 4nv (b, D^-1 in,
+    x, r out); restriction B_R + n v + n_c v; prolongation B_P + (2n + n_c) v;
+    post-smooth B_A + 4nv (x, b, D^-1 in, x out).  Coarsest level: the dense
+    inverse product (n_c^2 8 bytes)."""
     L = ml.num_levels
     tot = 0.0
     per = []
     for l in range(L):
         n, z, p = ml.level_info(l)
         if l == L - 1:
-            b = 2.0 * n * n * 8
+            b = 1.0 * n * n * 8
         else:
             nc = ml.level_info(l + 1)[0]
             BA = a_bytes(ml, l, vbytes)
             BP = p * (vbytes + 4) + (n + 1) * 4
             BR = p * (vbytes + 4) + (nc + 1) * 4
-            b = (3 * n * vbytes) + (BA + 3 * n * vbytes) + (BR + n * vbytes + nc * vbytes) + \
+            if ml.level_fused_first(l):
+                first = BA + 4 * n * vbytes
+            else:
+                first = (3 * n * vbytes) + (BA + 3 * n * vbytes)
+            b = first + (BR + n * vbytes + nc * vbytes) + \
                 (BP + (2 * n + nc) * vbytes) + (BA + 4 * n * vbytes)
         per.append(b)
         tot += b
@@ -471,6 +506,7 @@ def run_b200(args, rank, world, local):
     setup32 = ml32.setup_seconds
     clocks = ClockSampler(local)
     clocks.start()
+    clocks.wait_first()
     t32, iters32, launches = timed(ml32, args.steps, args.warmup)
     clk = clocks.stop()
     rel32 = true_relres()
@@ -488,7 +524,8 @@ def run_b200(args, rank, world, local):
     # post-smoothing sweep; the residual is the same kernel with one vector less)
     op_ms = {}
     for op, name in ((0, "residual_A0_fp32"), (3, "jacobi_A0_fp32"), (4, "spmv_dot_A0_fp64"),
-                     (1, "restrict_R0_fp32"), (2, "prolong_P0_fp32")):
+                     (1, "restrict_R0_fp32"), (2, "prolong_P0_fp32"),
+                     (6, "first_sweep_residual_A0_fp32"), (7, "first_sweep_A0_fp32")):
         op_ms[name] = ml32.time_operator(0, op, reps=20)
     n0, z0, p0 = ml32.level_info(0)
     n1 = ml32.level_info(1)[0]
@@ -499,6 +536,8 @@ def run_b200(args, rank, world, local):
         "spmv_dot_A0_fp64": BA0 + 2 * n0 * 8,
         "restrict_R0_fp32": p0 * 8 + (n1 + 1) * 4 + n0 * 4 + n1 * 4,
         "prolong_P0_fp32": p0 * 8 + (n0 + 1) * 4 + (2 * n0 + n1) * 4,
+        "first_sweep_residual_A0_fp32": BA0 + 4 * n0 * 4,
+        "first_sweep_A0_fp32": 3 * n0 * 4,
     }
     peak, peak_kind = peaks()
     dom = "jacobi_A0_fp32"
@@ -564,19 +603,21 @@ def run_b200(args, rank, world, local):
         "warmup": args.warmup, "ms_per_step": t32 * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32-vcycle/fp64-outer",
         "data": "synthetic (27-point Laplacian stencil, b ~ U[-1,1] seed %d)" % SEED,
-        "config": {
-            "workload": "laplacian27 %d^3 AMG-PCG to 1e-8 (RS PMIS, extended+i, L1-Jacobi)" % S,
-            "rows": n, "nnz": nnz, "levels": None,
-            "parallelism": "replicas" if world > 1 else "single",
-            "l2": "inputs larger than L2 (A0 FP64 = %.2f GB)" % (nnz * 12 / 1e9),
-        },
+        "config": bench_config(S, n, nnz, None, world),
+        "method": {"smoother": "L1-Jacobi, 1 pre- and 1 post-sweep",
+                   "cycle": "V-cycle in FP32 (hierarchy values FP32, int32 indices)",
+                   "outer": "PCG in FP64, stopping on the true relative residual",
+                   "coarse": "FP64 LU of A_c^T (explicit inverse product)"},
         "iters": iters32[-1], "final_rel_res": rel32, "setup_s": setup32,
         "vcycle": {"ms": cyc_ms, "alg_bytes": cbytes_pc,
                    "gbs": cbytes_pc / (cyc_ms * 1e-3) / 1e9,
                    "frac_of_%s_peak" % peak_kind: cbytes_pc / (cyc_ms * 1e-3) / 1e9 / peak,
                    "timed": "graph replay of z = M r (FP32 cycle with its FP64 conversions)",
                    "profile_ms_per_level": [round(float(v), 5) for v in prof.sum(axis=1)],
-                   "alg_bytes_per_level": per_level},
+                   "alg_bytes_per_level": per_level,
+                   "first_sweep_fused": [ml32.level_fused_first(l)
+                                         for l in range(ml32.num_levels - 1)],
+                   "tail": dict(zip(("start_level", "ctas"), ml32.tail_info()))},
         "fp64_form": fp64,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic_for(dom),
@@ -603,7 +644,7 @@ def run_b200(args, rank, world, local):
         out["aniso_precision"] = run_aniso_precision(rb, ev, lambda: rb.lib().rb_synchronize(),
                                                      args.aniso_size)
     if rank == 0 and args.cpu_sample > 0:
-        out["cpu_baseline"] = cpu_baseline(args.cpu_sample, S, iters32[-1])
+        out["cpu_baseline"] = cpu_baseline(ml32, bh, args.cpu_sample, S)
     dist.close()
     if rank == 0:
         print(json.dumps(out))
@@ -652,46 +693,184 @@ class CpuSample:
         return time.perf_counter() - t0, len(hist) - 1
 
 
+class RefSolve:
+    """The reference's PCG (raptor/krylov/par_cg.cpp:121-263) on a reference
+    hierarchy, run to the same true relative residual as the GPU arm.  The
+    reference stops when r.z < tol sqrt(b.Mb) (its history records r.z /
+    b.Mb), not on ||b - A x|| / ||b||, so its tolerance is calibrated: a
+    first solve to r.z / b.Mb <= 1e-18 gives the ratio c of the squared true
+    relative residual to r.z / b.Mb at its end; the tolerance is then set for
+    r.z / b.Mb <= 0.25 (1e-8)^2 / c, and divided by 10 until a solve's true
+    relative residual (the reference's own residual routine) is <= 1e-8.
+    These calibration solves are the warm-up; every timed solve then stops
+    at the first iteration the calibrated test allows."""
+
+    def __init__(self, O, A, ml, b):
+        self.O, self.A, self.ml, self.b = O, A, ml, b
+        self.bnorm = float(np.linalg.norm(b))
+        z = ml.cycle(np.zeros(len(b)), b)
+        self.sqrt_bMb = math.sqrt(max(float(np.dot(b, z)), 1e-300))
+        self.tol = 1e-18 * self.sqrt_bMb
+        self.iters = None
+        self.relres = None
+        self.last_rz = None
+
+    def solve(self):
+        t0 = time.perf_counter()
+        x, hist = self.O.ref_pcg(self.A, self.ml, np.zeros(len(self.b)), self.b, tol=self.tol,
+                                 max_iter=500)
+        el = time.perf_counter() - t0
+        self.iters = len(hist) - 1
+        self.last_rz = float(hist[-1])
+        self.relres = float(np.linalg.norm(self.A.residual(x, self.b)) / self.bnorm)
+        return el
+
+    def calibrate(self, max_tries=5):
+        """Solves that set the tolerance; returns their count."""
+        self.solve()
+        if self.relres <= TOL and self.last_rz > 0:
+            c = self.relres ** 2 / self.last_rz
+            self.tol = 0.25 * TOL * TOL / c * self.sqrt_bMb
+        for k in range(2, max_tries + 2):
+            self.solve()
+            if self.relres <= TOL:
+                return k
+            self.tol /= 10.0
+        raise RuntimeError("reference PCG did not reach 1e-8 (relres %.3e)" % self.relres)
+
+
+def cpu_baseline(ml, bh, m, S):
+    """One reference PCG solve at the full size on the hierarchy the GPU
+    built (exported level by level into the reference's ParMultilevel, whose
+    duplicate_coarse factors A_c as its setup would), on one core; the CPU
+    restatement on an m^3 sample, scaled by rows, where the reference build
+    is absent."""
+    from oracle import oracle as O
+    L = O.par_ref()
+    if L is None:
+        el, it, n, cores = cpu_sample_solve(m)
+        return {"value": el * (S ** 3) / n, "unit": "s", "cores": cores, "kind": "port",
+                "sample": "CPU restatement's AMG-PCG solve on %d^3 (%d rows, %d iterations, "
+                          "%.2f s on %d threads), scaled by rows to %d^3 (the reference "
+                          "build is absent)" % (m, n, it, el, cores, S)}
+    nl = ml.num_levels
+    As = [ml.level_matrix(l, "A").arrays() for l in range(nl)]
+    Ps = [(ml.level_info(l + 1)[0],) + tuple(ml.level_matrix(l, "P").arrays())
+          for l in range(nl - 1)]
+    hml = O.RefHierarchy.from_levels(L, As, Ps, **REF_KW)
+    del As, Ps
+    rs = RefSolve(O, hml.A(0), hml, bh)
+    warm = rs.calibrate()
+    el = rs.solve()
+    return {"value": el, "unit": "s", "cores": 1, "kind": "reference",
+            "sample": "one %d^3 solve: the reference's own PCG and V-cycle (compiled "
+                      "unmodified, single-rank MPI stand-in, one core; SOR smoother) on the "
+                      "GPU-built hierarchy of %d levels, %d iterations to true relative "
+                      "residual %.2e (PCG tol %.1e after %d calibration solves)"
+                      % (S, nl, rs.iters, rs.relres, rs.tol, warm)}
+
+
 def cpu_sample_solve(m):
     cs = CpuSample(m)
     el, it = cs.solve()
     return el, it, cs.n, cs.cores
 
 
-def cpu_baseline(m, S, iters_full):
-    el, it, n, cores = cpu_sample_solve(m)
-    scale = (S ** 3) / n
-    return {"value": el * scale, "unit": "s", "cores": cores, "kind": "port",
-            "sample": "oracle AMG-PCG solve phase on %d^3 (%d rows, %d iterations, %.2f s on %d "
-                      "threads), scaled by rows to %d^3" % (m, n, it, el, cores, S)}
+def ref_line(args, world, value, steps, warmup, cfg, cpu, extra):
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": value * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp64", "data": "synthetic (27-point Laplacian, b ~ U[-1,1] seed %d)" % SEED,
+        "config": cfg, "cpu_baseline": dict(cpu, value=value),
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    line.update(extra)
+    return line
 
 
 def run_reference(args, rank, world):
+    """The reference's own setup (untimed) and PCG solve on the full problem,
+    rank 0 only; the timed steps are capped so the run stays within a few
+    minutes (the count timed is the line's "steps")."""
     if rank != 0:
         return
+    from oracle import oracle as O
     S = args.size
-    m = args.cpu_sample
-    cs = CpuSample(m)
-    n = cs.n
+    L = O.par_ref()
+    bh = np.random.default_rng(SEED).uniform(-1.0, 1.0, S ** 3)
+    budget_s = float(os.environ.get("RAPTOR_B200_REF_BUDGET_S", "120"))
+    if L is None:
+        # the CPU restatement of the same solve, on every host core
+        cs = CpuSample(S)
+        for _ in range(max(1, min(args.warmup, 1))):
+            cs.solve()
+        times = []
+        while len(times) < args.steps and (not times or sum(times) + times[-1] <= budget_s):
+            el, it = cs.solve()
+            times.append(el)
+        v = sum(times) / len(times)
+        cfg = bench_config(S, cs.n, int(cs.A.shape[2]), cs.ml.num_levels, world)
+        print(json.dumps(ref_line(args, world, v, len(times), 1, cfg, {
+            "unit": "s", "cores": cs.cores, "kind": "port",
+            "sample": "CPU restatement of the reference's AMG-PCG (its compiled build is "
+                      "absent), %d^3, L1-Jacobi, %d iterations, %d of %d requested steps timed "
+                      "on %d threads" % (S, it, len(times), args.steps, cs.cores)},
+            {"method": {"smoother": "L1-Jacobi", "outer": "PCG in FP64 (true residual)"}})))
+        return
+    t0 = time.perf_counter()
+    A = O.RefMatrix.laplace27(L, S, S, S)
+    n, _, nnz = A.shape
+    try:
+        ml = O.RefHierarchy(A, **REF_KW)
+        setup_note = "the reference's own ParRugeStubenSolver setup"
+    except RuntimeError as e:
+        # At one rank the reference's extended interpolation counts an upper
+        # bound of P's nonzeros in an int (par_interpolation.cpp:531-569),
+        # which overflows past about 2^31 / 570 rows of this stencil (so at
+        # 192^3, not at 128^3) and makes the vector resize throw.  The
+        # hierarchy then comes from the CPU restatement's setup, which is
+        # identical to the reference's (A_l, P_l, states, entry order)
+        # wherever the reference runs, and the reference's solve phase is
+        # timed on it.
+        Ao = O.stencil_grid(O.laplace_stencil_27pt(), [S, S, S])
+        om = O.Hierarchy(Ao, relax="sor", interp="extended", interp_filter=0.3)
+        As = [om.A(l).arrays() for l in range(om.num_levels)]
+        Ps = [(om.A(l + 1).shape[0],) + tuple(om.P(l).arrays())
+              for l in range(om.num_levels - 1)]
+        del om, Ao
+        ml = O.RefHierarchy.from_levels(L, As, Ps, **REF_KW)
+        del As, Ps
+        why = str(e).split("setup threw ")[-1]
+        setup_note = ("the CPU restatement's setup (the reference's own ParRugeStubenSolver::"
+                      "setup throws std::length_error (%s) at this size at one rank: its int "
+                      "bound on P's nonzeros in extended interpolation overflows, "
+                      "par_interpolation.cpp:531-569), handed level by level to the "
+                      "reference's ParMultilevel" % why)
+    setup_s = time.perf_counter() - t0
+    rs = RefSolve(O, A, ml, bh)
+    warm = rs.calibrate()
     times = []
-    for s in range(args.warmup + args.steps):
-        el, it = cs.solve()
-        if s >= args.warmup:
-            times.append(el * (S ** 3) / n)
+    while len(times) < args.steps and (not times or sum(times) + times[-1] <= budget_s):
+        times.append(rs.solve())
+        if rs.relres > TOL:
+            raise RuntimeError("reference solve missed 1e-8: %.3e" % rs.relres)
     v = sum(times) / len(times)
-    print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp64", "data": "synthetic (27-point Laplacian, b ~ U[-1,1] seed %d)" % SEED,
-        "config": {"workload": "laplacian27 %d^3 AMG-PCG to 1e-8 (RS PMIS, extended+i, "
-                               "L1-Jacobi)" % S, "parallelism": "single"},
-        "cpu_baseline": {"value": v, "unit": "s", "cores": cs.cores, "kind": "port",
-                         "sample": "CPU restatement of the reference algorithm (the reference "
-                                   "needs MPI), solve phase on %d^3 per step on %d threads, "
-                                   "scaled by rows to %d^3" % (m, cs.cores, S)},
-        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }))
+    cfg = bench_config(S, n, nnz, ml.num_levels, world)
+    print(json.dumps(ref_line(args, world, v, len(times), warm, cfg, {
+        "unit": "s", "cores": 1, "kind": "reference",
+        "sample": "the reference's own PCG and V-cycle (compiled unmodified with a "
+                  "single-rank MPI stand-in and OpenBLAS LU; one core, the reference has no "
+                  "threads) on the full %d^3 problem, hierarchy from %s (%.1f s, untimed); SOR "
+                  "smoother; %d iterations to true relative residual %.2e (PCG tol %.1e after "
+                  "%d calibration solves); %d of the %d requested steps timed within %.0f s"
+                  % (S, setup_note, setup_s, rs.iters, rs.relres, rs.tol, warm, len(times),
+                     args.steps, budget_s)},
+        {"setup_s": setup_s, "iters": rs.iters, "final_rel_res": rs.relres,
+         "method": {"smoother": "SOR (the reference's default; its Jacobi is a no-op, it has "
+                                "no L1-Jacobi), 1 pre- and 1 post-sweep",
+                    "cycle": "V-cycle in FP64", "outer": "the reference's PCG in FP64",
+                    "coarse": "dgetrf_/dgetrs_ (OpenBLAS) of A_c^T"}})))
 
 
 def main():

@@ -197,7 +197,10 @@ typedef struct rb_amg_opts {
     int precision;            /* RB_PREC_FP64 / RB_PREC_FP32 */
     int jacobi_compat;        /* 1: Jacobi leaves x unchanged, as par_relax.cpp:127,146 does */
     int seed_offset;          /* first_local_row in srand(2448422 + first_local_row) */
-    int fuse_coarse;          /* 1: levels below 1e5 rows run as one persistent launch (default 0) */
+    int fuse_coarse;          /* 1 (default): the bottom levels of the cycle run as one launch of one
+                                 thread-block cluster, from the start level that times fastest
+                                 (none if no start beats separate launches); 0: never;
+                                 k >= 2: from level k-1 if that level qualifies */
     int use_graphs;           /* 1: replay cycles / Krylov iterations from CUDA graphs */
 } rb_amg_opts;
 
@@ -227,10 +230,11 @@ int rb_amg_solve(rb_amg ml, rb_vec x, rb_vec b, int* iters, double* hist, int ca
 int rb_amg_cycle_profile(rb_amg ml, double* ms, int cap, int* n_out);
 /* Average milliseconds per launch of one cycle operator over reps launches:
  * op 0 residual with A_l, 1 restriction with R_l, 2 prolongation with P_l,
- * 3 Jacobi sweep with A_l (all in the cycle precision), 4 the outer FP64
- * A p fused with p.Ap on the finest level, 5 one whole preconditioner
- * V-cycle z = M r from a zero guess replayed from its CUDA graph (level is
- * ignored). */
+ * 3 Jacobi sweep with A_l, 6 the first sweep from zero fused with the
+ * residual, 7 the first sweep alone (all in the cycle precision), 4 the
+ * outer FP64 A p fused with p.Ap on the finest level, 5 one whole
+ * preconditioner V-cycle z = M r from a zero guess replayed from its CUDA
+ * graph (level is ignored). */
 int rb_amg_time_operator(rb_amg ml, int level, int op, int reps, double* ms_per_launch);
 /* Wall time of the last rb_amg_setup (seconds) and the autotuner's choices
  * for level l: lanes per row of A_l (0 when A_l is stored by diagonals),
@@ -240,6 +244,14 @@ int rb_amg_level_lanes(rb_amg ml, int level, int* lanes_A, int* lanes_P, int* la
 /* Storage of A_l in the cycle: *ndiag = number of stored diagonals when the
  * autotuner picked the sliced-diagonal layout, 0 for CSR. */
 int rb_amg_level_storage(rb_amg ml, int level, int* ndiag);
+/* 1 when level l's first sweep from zero runs fused with its residual (one
+ * pass over A_l; the autotuner's pick), else 0.  No counterpart in the
+ * reference. */
+int rb_amg_level_fused_first(rb_amg ml, int level, int* fused);
+/* The level from which the rest of the cycle runs as one cluster launch
+ * (-1: none) and the CTAs of that cluster.  No counterpart in the
+ * reference (it describes how this library schedules the cycle). */
+int rb_amg_tail_info(rb_amg ml, int* start_level, int* ctas);
 /* Kernels this library has launched so far (graph replays count their
  * kernel nodes). */
 int rb_launch_count(int64_t* count);
@@ -301,10 +313,12 @@ int rb_adjoint_solve(rb_csr A, rb_amg ml, rb_vec lambda, rb_vec g, double tol, i
 /* An uneven batch of independent systems (no counterpart in the reference).
  * Each matrix gets the hierarchy rb_amg_setup would build for it alone; the
  * levels are packed block-diagonally so one V-cycle of the batch is one
- * launch per operation for all systems, and rb_batch_pcg replays a whole
- * iteration of all systems from one CUDA graph, with per-system CG scalars
- * and stopping tests.  Vectors of a batch are the systems' vectors
- * concatenated in order (rb_batch_offsets gives the first row of each). */
+ * launch per operation for all systems, and rb_batch_pcg runs the
+ * iterations of all systems on the device: one CUDA graph launch holds a
+ * while loop over whole iterations, with per-system CG scalars, active
+ * flags and stopping tests (true-residual confirmation included) kept on the
+ * device.  Vectors of a batch are the systems' vectors concatenated in order
+ * (rb_batch_offsets gives the first row of each). */
 int rb_batch_setup(int n_sys, const rb_csr* mats, const rb_amg_opts* opts, rb_batch* out);
 int rb_batch_destroy(rb_batch B);
 /* number of systems, total rows, levels of the packed hierarchy */
@@ -319,6 +333,11 @@ int rb_batch_cycle(rb_batch B, rb_vec x, rb_vec b);
  * residual.  RB_ERR_NOT_CONVERGED if any system did not reach tol. */
 int rb_batch_pcg(rb_batch B, rb_vec x, rb_vec b, double tol, int max_iter, int* iters,
                  double* relres);
+/* Times the host waited on the device during the last rb_batch_pcg (one per
+ * graph launch of its device-side loop; a launch ends at convergence,
+ * breakdown, the iteration limit or a failed true-residual confirmation).
+ * No counterpart in the reference. */
+int rb_batch_host_waits(rb_batch B, int* waits);
 
 /* One V-cycle from a zero guess applied to k columns at once, X = M B
  * (columns interleaved by row, n * k entries each; k in 2..32; Jacobi or

@@ -490,7 +490,11 @@ def par_ref(jacobi_fix=False):
         return None
     L = C.CDLL(so)
     L.rp_matrix_from_csr.restype = _P
-    L.rp_matrix_from_csr.argtypes = [C.c_int, _I, _I, _D]
+    L.rp_matrix_from_csr.argtypes = [C.c_int, C.c_int, _I, _I, _D, C.c_int, C.c_int, C.c_int]
+    L.rp_matrix_flags.argtypes = [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.rp_hierarchy_from_levels.restype = _P
+    L.rp_hierarchy_from_levels.argtypes = [C.c_int, C.POINTER(_P), C.POINTER(_P),
+                                           C.POINTER(RefOpts)]
     L.rp_diffusion_grid.restype = _P
     L.rp_diffusion_grid.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int]
     L.rp_laplace27_grid.restype = _P
@@ -506,6 +510,7 @@ def par_ref(jacobi_fix=False):
     L.rp_spmv_T.argtypes = [_P, _D, _D]
     L.rp_residual.argtypes = [_P, _D, _D, _D]
     L.rp_default_opts.argtypes = [C.POINTER(RefOpts)]
+    L.rp_last_error.restype = C.c_char_p
     L.rp_setup.restype = _P
     L.rp_setup.argtypes = [_P, C.POINTER(RefOpts)]
     L.rp_free.argtypes = [_P]
@@ -564,10 +569,18 @@ class RefMatrix:
         self.L, self.ptr, self._owner = L, ptr, owner
 
     @classmethod
-    def from_csr(cls, L, rowptr, cols, vals):
+    def from_csr(cls, L, rowptr, cols, vals, n_cols=None):
         rp = np.ascontiguousarray(rowptr, np.int32)
-        return cls(L, L.rp_matrix_from_csr(len(rp) - 1, rp, np.ascontiguousarray(cols, np.int32),
-                                           np.ascontiguousarray(vals, np.float64)))
+        n = len(rp) - 1
+        return cls(L, L.rp_matrix_from_csr(n, n if n_cols is None else n_cols, rp,
+                                           np.ascontiguousarray(cols, np.int32),
+                                           np.ascontiguousarray(vals, np.float64), 0, 0, 0))
+
+    def flags(self):
+        """(sorted, diag_first) of the on-process block."""
+        a, b = C.c_int(), C.c_int()
+        self.L.rp_matrix_flags(self.ptr, C.byref(a), C.byref(b))
+        return a.value, b.value
 
     @classmethod
     def diffusion(cls, L, eps, theta, nx, ny):
@@ -634,6 +647,35 @@ class RefHierarchy:
         self.opts = ref_opts(self.L, **kw)
         self.A0 = A
         self.ptr = self.L.rp_setup(A.ptr, C.byref(self.opts))
+        if not self.ptr:
+            raise RuntimeError("reference setup failed: %s" % self.L.rp_last_error().decode())
+
+    @classmethod
+    def from_levels(cls, L, As, Ps, A_flags=(1, 1), **kw):
+        """The reference's hierarchy object over given levels: As[l] =
+        (rowptr, cols, vals) of A_l in its entry order (diagonal first, as
+        setup leaves every level; A_flags are its sorted / diag_first flags),
+        Ps[l] = (n_cols, rowptr, cols, vals) of P_l in its entry order; no
+        setup runs (duplicate_coarse factors A_c as setup would)."""
+        self = cls.__new__(cls)
+        self.L = L
+        self.opts = ref_opts(L, **kw)
+        nl = len(As)
+        a_ptrs = (_P * nl)()
+        p_ptrs = (_P * max(nl - 1, 1))()
+        for l, (rp, ci, cv) in enumerate(As):
+            n = len(rp) - 1
+            a_ptrs[l] = L.rp_matrix_from_csr(n, n, np.ascontiguousarray(rp, np.int32),
+                                             np.ascontiguousarray(ci, np.int32),
+                                             np.ascontiguousarray(cv, np.float64), 1,
+                                             A_flags[0], A_flags[1])
+        for l, (m, rp, ci, cv) in enumerate(Ps):
+            p_ptrs[l] = L.rp_matrix_from_csr(len(rp) - 1, m, np.ascontiguousarray(rp, np.int32),
+                                             np.ascontiguousarray(ci, np.int32),
+                                             np.ascontiguousarray(cv, np.float64), 1, 0, 0)
+        self.ptr = L.rp_hierarchy_from_levels(nl, a_ptrs, p_ptrs, C.byref(self.opts))
+        self.A0 = self.A(0)
+        return self
 
     def __del__(self):
         if getattr(self, "ptr", None):

@@ -16,6 +16,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
+#include <string>
 
 #include "core/types.hpp"
 #include "core/par_matrix.hpp"
@@ -60,6 +62,8 @@ struct Solver {
     int n0;
 };
 
+std::string g_error;
+
 void set_vec(ParVector& v, const double* a) {
     for (int i = 0; i < v.local_n; i++) v.local[i] = a[i];
 }
@@ -77,23 +81,39 @@ int copy_hist(const aligned_vector<double>& h, int n, double* hist, int cap) {
 
 extern "C" {
 
-// A ParCSRMatrix holding the given rows as they are (finalize sorts each row
-// by column, as every reference constructor does).
-void* rp_matrix_from_csr(int n, const int* rowptr, const int* cols, const double* vals) {
-    ParCSRMatrix* A = new ParCSRMatrix(n, n);
+// A ParCSRMatrix with n rows and m columns holding the given rows
+// (finalize sorts each row by column, as every reference constructor does).
+// keep_order puts the caller's entry order back afterwards, with the
+// matrix's sorted / diag_first flags set as given: a level exported from a
+// hierarchy then sums its rows in the order the hierarchy did.
+void* rp_matrix_from_csr(int n, int m, const int* rowptr, const int* cols, const double* vals,
+                         int keep_order, int sorted, int diag_first) {
+    ParCSRMatrix* A = new ParCSRMatrix(n, m);
     int nnz = rowptr[n];
     A->on_proc->n_rows = n;
-    A->on_proc->n_cols = n;
+    A->on_proc->n_cols = m;
     A->on_proc->idx1.assign(rowptr, rowptr + n + 1);
     A->on_proc->idx2.assign(cols, cols + nnz);
     A->on_proc->vals.assign(vals, vals + nnz);
     A->on_proc->nnz = nnz;
     A->off_proc->n_rows = n;
-    A->off_proc->n_cols = n;
+    A->off_proc->n_cols = m;
     A->off_proc->idx1.assign(n + 1, 0);
     A->off_proc->nnz = 0;
     A->finalize();
+    if (keep_order) {
+        A->on_proc->idx2.assign(cols, cols + nnz);
+        A->on_proc->vals.assign(vals, vals + nnz);
+        A->on_proc->sorted = sorted != 0;
+        A->on_proc->diag_first = diag_first != 0;
+    }
     return A;
+}
+
+void rp_matrix_flags(void* p, int* sorted, int* diag_first) {
+    ParCSRMatrix* A = (ParCSRMatrix*)p;
+    *sorted = A->on_proc->sorted ? 1 : 0;
+    *diag_first = A->on_proc->diag_first ? 1 : 0;
 }
 
 // par_stencil_grid(diffusion_stencil_2d(eps, theta), {nx, ny}, 2)
@@ -196,11 +216,15 @@ void rp_default_opts(rp_opts* o) {
     o->max_levels = 25;
 }
 
+const char* rp_last_error(void) { return g_error.c_str(); }
+
 // new ParRugeStubenSolver(...) or ParSmoothedAggregationSolver(...), the
-// caller's field settings, then ml->setup(A) (which copies A).
+// caller's field settings, then ml->setup(A) (which copies A).  NULL, with
+// the exception's text in rp_last_error(), if the setup throws.
 void* rp_setup(void* pA, const rp_opts* o) {
     ParCSRMatrix* A = (ParCSRMatrix*)pA;
     Solver* s = new Solver;
+    s->ml = NULL;
     s->o = *o;
     s->n0 = A->local_num_rows;
     if (o->solver == 0) {
@@ -217,7 +241,47 @@ void* rp_setup(void* pA, const rp_opts* o) {
     s->ml->num_smooth_sweeps = o->num_smooth_sweeps;
     s->ml->max_coarse = o->max_coarse;
     s->ml->max_levels = o->max_levels;
-    s->ml->setup(A);
+    try {
+        s->ml->setup(A);
+    } catch (const std::exception& e) {
+        g_error = std::string("setup threw ") + e.what();
+        // the partly built hierarchy is left as it is (its state is unknown)
+        delete s;
+        return NULL;
+    }
+    g_error.clear();
+    return s;
+}
+
+// A ParRugeStubenSolver whose levels are given (A_l with the diagonal first,
+// P_l), finished the way ParMultilevel::setup_helper finishes its own
+// (level vectors sized, duplicate_coarse gathering A_c and factoring it with
+// dgetrf_), without running the setup: the reference's solve phase on a
+// hierarchy built elsewhere.  The hierarchy owns the matrices afterwards.
+void* rp_hierarchy_from_levels(int L, void** As, void** Ps, const rp_opts* o) {
+    Solver* s = new Solver;
+    s->o = *o;
+    s->n0 = ((ParCSRMatrix*)As[0])->local_num_rows;
+    ParRugeStubenSolver* rs = new ParRugeStubenSolver(
+        o->theta, (coarsen_t)o->coarsen, (interp_t)o->interp, (strength_t)o->strength,
+        (relax_t)o->relax);
+    rs->interp_filter = o->interp_filter;
+    rs->relax_weight = o->relax_weight;
+    rs->num_smooth_sweeps = o->num_smooth_sweeps;
+    rs->max_coarse = o->max_coarse;
+    rs->max_levels = o->max_levels;
+    for (int l = 0; l < L; l++) {
+        ParLevel* lv = new ParLevel();
+        lv->A = (ParCSRMatrix*)As[l];
+        lv->P = (l + 1 < L) ? (ParCSRMatrix*)Ps[l] : NULL;
+        lv->x.resize(lv->A->global_num_rows, lv->A->local_num_rows);
+        lv->b.resize(lv->A->global_num_rows, lv->A->local_num_rows);
+        lv->tmp.resize(lv->A->global_num_rows, lv->A->local_num_rows);
+        rs->levels.push_back(lv);
+    }
+    rs->num_levels = L;
+    rs->duplicate_coarse();
+    s->ml = rs;
     return s;
 }
 

@@ -476,6 +476,18 @@ class ParMultilevel:
         check(lib().rb_amg_level_storage(self.h, l, C.byref(nd)))
         return nd.value
 
+    def level_fused_first(self, l):
+        """True when level l's first sweep runs fused with its residual."""
+        f = C.c_int()
+        check(lib().rb_amg_level_fused_first(self.h, l, C.byref(f)))
+        return bool(f.value)
+
+    def tail_info(self):
+        """(start level of the one-launch cluster tail or -1, its CTAs)."""
+        f, c = C.c_int(), C.c_int()
+        check(lib().rb_amg_tail_info(self.h, C.byref(f), C.byref(c)))
+        return f.value, c.value
+
     def print_hierarchy(self):
         print("Num Levels = %d" % self.num_levels)
         print("A\tNRow\tNCol\tNNZ")
@@ -547,6 +559,13 @@ class Batch:
 
     def cycle(self, x, b):
         check(lib().rb_batch_cycle(self.h, x.h, b.h))
+
+    @property
+    def host_waits(self):
+        """Host waits of the last pcg (one per launch of its device loop)."""
+        w = C.c_int()
+        check(lib().rb_batch_host_waits(self.h, C.byref(w)))
+        return w.value
 
     def pcg(self, x, b, tol=1e-8, max_iter=-1):
         """Per-system PCG to tol (true relative residual); returns

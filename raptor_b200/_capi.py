@@ -115,6 +115,8 @@ SIGNATURES = {
     "rb_amg_setup_seconds": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "rb_amg_level_lanes": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "rb_amg_level_storage": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_amg_tail_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "rb_amg_level_fused_first": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "rb_residual_norm_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "rb_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rb_device_alloc_count": (C.c_int, [C.POINTER(C.c_int64)]),
@@ -129,6 +131,7 @@ SIGNATURES = {
     "rb_batch_offsets": (C.c_int, [_P, _P, _P]),
     "rb_batch_cycle": (C.c_int, [_P, _P, _P]),
     "rb_batch_pcg": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _I, _D]),
+    "rb_batch_host_waits": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "rb_amg_cycle_block": (C.c_int, [_P, _P, _P, C.c_int]),
     "rb_pcg_block": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_double, C.c_int, _I, _D]),
     "rb_cg": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _P, C.c_int, C.POINTER(C.c_int)]),

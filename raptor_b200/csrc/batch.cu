@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <functional>
 #include <memory>
 #include <string>
 
@@ -111,9 +112,12 @@ __global__ void k_coarse_mv_batch(const int* __restrict__ row0, const int* __res
 
 // Segmented dot: one CTA per chunk writes its partial; then one thread per
 // system sums that system's chunks in order.  Deterministic.
+// gate (optional): the pass runs only when *gate is nonzero (a step of the
+// device-side loop that some iterations skip)
 __global__ void __launch_bounds__(256)
 k_seg_partial(const int* __restrict__ lo, const int* __restrict__ hi, const double* __restrict__ a,
-              const double* __restrict__ b, double* part) {
+              const double* __restrict__ b, double* part, const int* gate) {
+    if (gate && *(volatile const int*)gate == 0) return;
     __shared__ double w[8];
     const int c = blockIdx.x;
     double t = 0.0;
@@ -130,7 +134,8 @@ k_seg_partial(const int* __restrict__ lo, const int* __restrict__ hi, const doub
 
 template <class Fin>
 __global__ void k_seg_finish(int n_sys, const int* __restrict__ chunk0, const double* __restrict__ part,
-                             Fin fin) {
+                             Fin fin, const int* gate) {
+    if (gate && *(volatile const int*)gate == 0) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_sys) return;
     double t = 0.0;
@@ -195,6 +200,77 @@ __global__ void k_seg_ids(int n_sys, const long long* __restrict__ off, int* seg
         seg[i] = s;
 }
 
+// State of the device-side PCG loop of a batch (one copy on the device,
+// staged through pinned host memory between launches).
+struct BatchCtl {
+    int it;        // iterations done
+    int end;       // the iteration limit
+    int pmode;     // 0: p = z already (first iteration, after a restart)
+    int full;      // the iteration under way replaces r by b - A x (every 10th)
+    int confirm;   // a system's recursive residual met the tolerance
+    int restart;   // a candidate failed the true-residual check
+    int done;      // every system has stopped
+    int pad;
+    double tol;
+};
+
+__global__ void k_seg_p_dev(long n, const int* __restrict__ seg, double* __restrict__ p,
+                            const double* __restrict__ z, const double* __restrict__ beta,
+                            const BatchCtl* c) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || c->pmode == 0) return;
+    p[i] = p[i] * beta[seg[i]] + z[i];
+}
+
+// active systems whose recursive residual meets the tolerance
+__global__ void k_batch_candidates(int n_sys, SegScal S, const double* __restrict__ bnorm,
+                                   int* __restrict__ cand, BatchCtl* c) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_sys) return;
+    const int cd = S.active[s] && sqrt(S.rr[s]) <= c->tol * bnorm[s];
+    cand[s] = cd;
+    if (cd) atomicOr(&c->confirm, 1);
+}
+
+// a candidate whose true residual (S.tmp) meets the tolerance stops; one
+// that does not sends the loop back to the host for a restart
+__global__ void k_batch_confirm(int n_sys, SegScal S, const double* __restrict__ bnorm,
+                                int* __restrict__ cand, int* __restrict__ iters,
+                                double* __restrict__ relres, BatchCtl* c) {
+    if (*(volatile const int*)&c->confirm == 0) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_sys || !cand[s]) return;
+    cand[s] = 0;
+    const double tr = sqrt(S.tmp[s]);
+    if (tr <= c->tol * bnorm[s]) {
+        S.active[s] = 0;
+        iters[s] = c->it + 1;
+        relres[s] = tr / bnorm[s];
+    } else {
+        c->restart = 1;
+    }
+}
+
+// end of one iteration: count it, set up the next, and end the graph's
+// while loop on breakdown, when every system has stopped, on a failed
+// confirmation (the host restarts), or at the iteration limit
+constexpr int kStepEndThreads = 256;
+__global__ void __launch_bounds__(kStepEndThreads)
+k_batch_step_end(int n_sys, SegScal S, BatchCtl* c, cudaGraphConditionalHandle h) {
+    int any = 0;
+    for (int s = threadIdx.x; s < n_sys; s += blockDim.x) any |= S.active[s];
+    any = __syncthreads_or(any);
+    if (threadIdx.x != 0) return;
+    const int it = c->it + 1;
+    c->it = it;
+    c->pmode = 1;
+    c->confirm = 0;
+    c->full = ((it + 1) % 10 == 0) ? 1 : 0;
+    c->done = any ? 0 : 1;
+    const bool stop = *S.breakdown != 0 || !any || c->restart != 0 || it >= c->end;
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
 }  // namespace
 
 struct Batch {
@@ -221,16 +297,25 @@ struct Batch {
     SegScal S{};
     std::vector<double> h_rr, h_tmp;
     std::vector<int> h_active;
+    // device-side loop: its state, per-system norms, candidates and results
+    DevArray<BatchCtl> ctl;
+    BatchCtl* h_ctl = nullptr;
+    DevArray<double> bnorm_d, relres_d;
+    DevArray<int> cand_d, iters_d;
+    int host_waits = 0;   // host waits of the last pcg (one per graph launch)
+    ~Batch() {
+        if (h_ctl) cudaFreeHost(h_ctl);
+    }
 
     long long rows() const { return off[0][n_sys]; }
 
     template <class Fin>
-    void seg_dot(const double* a, const double* b, Fin fin) {
+    void seg_dot(const double* a, const double* b, Fin fin, const int* gate = nullptr) {
         k_seg_partial<<<n_chunks, 256, 0, stream()>>>(chunk_lo.get(), chunk_hi.get(), a, b,
-                                                      part.get());
+                                                      part.get(), gate);
         RB_CHECK_LAUNCH();
         k_seg_finish<<<grid_for(n_sys, 128), 128, 0, stream()>>>(n_sys, chunk0.get(), part.get(),
-                                                                  fin);
+                                                                  fin, gate);
         RB_CHECK_LAUNCH();
     }
 
@@ -252,6 +337,9 @@ struct Batch {
     void cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool x_zero);
     void cycle64(double* x, const double* b);
     int pcg(double* x, const double* b, double tol, int max_iter, int* iters, double* relres);
+    int pcg_device_loop(double* x, const double* b, double tol, int max_iter, int* iters,
+                        double* relres, const std::vector<double>& bnorm,
+                        const std::function<void()>& restart);
 };
 
 void Batch::setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o) {
@@ -563,6 +651,8 @@ int Batch::pcg(double* x, const double* b, double tol, int max_iter, int* iters,
         return true;
     };
     if (check()) return RB_OK;
+    host_waits = 0;
+    if (cat.use_graphs) return pcg_device_loop(x, b, tol, max_iter, iters, relres, bnorm, restart);
     auto body = [&](bool full_r) {
         launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, p.get(), EpiStore<double>{Ap.get()},
                     cat.gA0 > 0 ? cat.gA0 : 0);
@@ -600,6 +690,108 @@ int Batch::pcg(double* x, const double* b, double tol, int max_iter, int* iters,
     return status;
 }
 
+// The iterations of Batch::pcg on the device: one graph launch holds a
+// while loop whose body is one iteration for every system (p update, A p and
+// alpha, x and r updates, the every-10th b - A x, r.r, the V-cycle and r.z),
+// followed by the stopping logic the host loop runs otherwise: systems whose
+// recursive residual meets the tolerance are confirmed with the true
+// residual (b - A x and its segmented norm, gated to the iterations that
+// need them) and stop; the loop ends when all have stopped, on breakdown, at
+// the iteration limit, or when a confirmation fails, after which the host
+// restarts the recurrence (r = b - A x, z = M r, p = z) exactly as before and
+// launches again.  The host therefore waits once per launch, not once per
+// iteration; results are the same as the host loop's.
+int Batch::pcg_device_loop(double* x, const double* b, double tol, int max_iter, int* iters,
+                           double* relres, const std::vector<double>& bnorm,
+                           const std::function<void()>& restart) {
+    const rb_csr_s& A = *cat.master[0].A;
+    const long N = A.n_rows;
+    const int n = n_sys;
+    const CsrView<double> Av = view(A);
+    if (!ctl.get()) {
+        ctl.alloc(1);
+        bnorm_d.alloc((size_t)n);
+        relres_d.alloc((size_t)n);
+        cand_d.alloc((size_t)n);
+        iters_d.alloc((size_t)n);
+        RB_CUDA(cudaMallocHost(&h_ctl, sizeof(BatchCtl)));
+    }
+    bnorm_d.upload(bnorm.data(), n);
+    iters_d.upload(iters, n);
+    relres_d.upload(relres, n);
+    cand_d.zero();
+    *h_ctl = BatchCtl{0, max_iter, 0, 0, 0, 0, 0, 0, tol};
+    BatchCtl* C = ctl.get();
+    const unsigned sg = grid_for(n, 128);
+    auto iteration = [&](cudaGraphConditionalHandle h) {
+        k_seg_p_dev<<<grid_for(N, 256), 256, 0, stream()>>>(N, seg.get(), p.get(), z.get(),
+                                                            S.beta, C);
+        RB_CHECK_LAUNCH();
+        launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, p.get(), EpiStore<double>{Ap.get()},
+                    cat.gA0 > 0 ? cat.gA0 : 0);
+        seg_dot(p.get(), Ap.get(), FinSPAp{S});
+        k_seg_update<<<grid_for(N, 256), 256, 0, stream()>>>(N, seg.get(), x, r.get(), p.get(),
+                                                             Ap.get(), S.alpha);
+        RB_CHECK_LAUNCH();
+        launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, x,
+                    EpiResidualIf<double, double>{b, r.get(), &C->full},
+                    cat.gA0 > 0 ? cat.gA0 : 0);
+        seg_dot(r.get(), r.get(), FinSRR{S});
+        cycle64(z.get(), r.get());
+        seg_dot(r.get(), z.get(), FinSRZ{S});
+        k_batch_candidates<<<sg, 128, 0, stream()>>>(n, S, bnorm_d.get(), cand_d.get(), C);
+        RB_CHECK_LAUNCH();
+        launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, x,
+                    EpiResidualIf<double, double>{b, rt.get(), &C->confirm},
+                    cat.gA0 > 0 ? cat.gA0 : 0);
+        seg_dot(rt.get(), rt.get(), FinSTmp{S}, &C->confirm);
+        k_batch_confirm<<<sg, 128, 0, stream()>>>(n, S, bnorm_d.get(), cand_d.get(),
+                                                  iters_d.get(), relres_d.get(), C);
+        RB_CHECK_LAUNCH();
+        k_batch_step_end<<<1, kStepEndThreads, 0, stream()>>>(n, S, C, h);
+        RB_CHECK_LAUNCH();
+    };
+    char key[96];
+    snprintf(key, sizeof(key), "bloop:%p:%p", (void*)x, (const void*)b);
+    int status = RB_ERR_NOT_CONVERGED;
+    int h_break = 0;
+    for (;;) {
+        RB_CUDA(cudaMemcpyAsync(C, h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, stream()));
+        const int it0 = h_ctl->it;
+        cat.run_while_graph(key, iteration);
+        RB_CUDA(cudaMemcpyAsync(h_ctl, C, sizeof(BatchCtl), cudaMemcpyDeviceToHost, stream()));
+        RB_CUDA(cudaMemcpyAsync(&h_break, S.breakdown, sizeof(int), cudaMemcpyDeviceToHost,
+                                stream()));
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        host_waits++;
+        launch_counter() += cat.graph_kernels[key] * (h_ctl->it - it0);
+        if (h_break) return RB_ERR_BREAKDOWN;
+        if (h_ctl->done) { status = RB_OK; break; }
+        if (h_ctl->restart) {
+            // as the host loop: deactivated systems stay stopped, the others
+            // restart from their true residual
+            restart();
+            h_ctl->restart = 0;
+            h_ctl->pmode = 0;
+        }
+        if (h_ctl->it >= max_iter) break;
+    }
+    const int iter = h_ctl->it;
+    iters_d.download(iters, n);
+    relres_d.download(relres, n);
+    RB_CUDA(cudaMemcpyAsync(h_active.data(), S.active, sizeof(int) * n, cudaMemcpyDeviceToHost,
+                            stream()));
+    RB_CUDA(cudaMemcpyAsync(h_rr.data(), S.rr, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                            stream()));
+    RB_CUDA(cudaStreamSynchronize(stream()));
+    for (int s = 0; s < n; s++)
+        if (h_active[s]) {
+            iters[s] = iter;
+            relres[s] = std::sqrt(h_rr[s]) / bnorm[s];
+        }
+    return status;
+}
+
 }  // namespace rb
 
 struct rb_batch_s {
@@ -624,6 +816,7 @@ void batch_cycle(rb_batch_s* B, double* x, const double* b) {
     snprintf(key, sizeof(key), "bcyc:%p:%p", (void*)x, (const void*)b);
     T.cat.run_graph(key, [&] { T.cycle64(x, b); });
 }
+int batch_host_waits(const rb_batch_s* B) { return B->b.host_waits; }
 int batch_pcg(rb_batch_s* B, double* x, const double* b, double tol, int max_iter, int* iters,
               double* relres) {
     return B->b.pcg(x, b, tol, max_iter, iters, relres);

@@ -95,21 +95,23 @@ k_cg_update(long n, double* __restrict__ x, double* __restrict__ r, const double
 }
 
 // p = z + beta p  (or p = z on a restart), par_cg.cpp:234-243
-static __global__ void k_cg_p(long n, double* __restrict__ p, const double* __restrict__ z,
+template <typename TZ>
+static __global__ void k_cg_p(long n, double* __restrict__ p, const TZ* __restrict__ z,
                        const KScal* __restrict__ s, int restart) {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (restart) p[i] = z[i];
-    else p[i] = p[i] * s->beta + z[i];
+    if (restart) p[i] = (double)z[i];
+    else p[i] = p[i] * s->beta + (double)z[i];
 }
 
 // p = z + beta p at the start of an iteration of the device-side loop, or
 // nothing when the previous step left p = z (start, restart)
-static __global__ void k_cg_p_dev(long n, double* __restrict__ p, const double* __restrict__ z,
+template <typename TZ>
+static __global__ void k_cg_p_dev(long n, double* __restrict__ p, const TZ* __restrict__ z,
                                   const KScal* __restrict__ s) {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || s->ctl.pmode == 0) return;
-    p[i] = p[i] * s->beta + z[i];
+    p[i] = p[i] * s->beta + (double)z[i];
 }
 
 // Last kernel of one iteration of the device-side loop: count the iteration,

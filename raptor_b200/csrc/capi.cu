@@ -609,7 +609,7 @@ void rb_amg_default_opts(rb_amg_opts* o) {
     o->precision = RB_PREC_FP64;
     o->jacobi_compat = 0;
     o->seed_offset = 0;
-    o->fuse_coarse = 0;
+    o->fuse_coarse = 1;
     o->use_graphs = 1;
 }
 
@@ -731,7 +731,7 @@ int rb_amg_cycle_profile(rb_amg ml, double* ms, int cap, int* n_out) {
 int rb_amg_time_operator(rb_amg ml, int level, int op, int reps, double* ms_per_launch) {
     return guarded([&]() -> int {
         NEED(ml); NEED(ms_per_launch);
-        RB_REQUIRE(op >= 0 && op <= 5, "unknown operator");
+        RB_REQUIRE(op >= 0 && op <= 7, "unknown operator");
         *ms_per_launch = ml->h.time_operator(level, op, reps);
         return RB_OK;
     });
@@ -775,6 +775,25 @@ int rb_amg_level_storage(rb_amg ml, int level, int* ndiag) {
             const auto& V = ml->h.lv64[level];
             *ndiag = V.dia ? V.off.nd : 0;
         }
+        return RB_OK;
+    });
+}
+
+int rb_amg_level_fused_first(rb_amg ml, int level, int* fused) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(fused);
+        RB_REQUIRE(level >= 0 && level < ml->h.num_levels(), "level out of range");
+        *fused = ml->h.opts.precision == RB_PREC_FP32 ? ml->h.lv32[level].fuse_first
+                                                      : ml->h.lv64[level].fuse_first;
+        return RB_OK;
+    });
+}
+
+int rb_amg_tail_info(rb_amg ml, int* start_level, int* ctas) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(start_level); NEED(ctas);
+        *start_level = ml->h.tail_from;
+        *ctas = ml->h.tail_from >= 0 ? ml->h.tail_ctas : 0;
         return RB_OK;
     });
 }
@@ -908,6 +927,14 @@ int rb_batch_pcg(rb_batch B, rb_vec x, rb_vec b, double tol, int max_iter, int* 
         const long long N = batch_offset(B, batch_num_systems(B));
         RB_REQUIRE(x->n == N && b->n == N, "batch PCG: vector sizes do not match");
         return batch_pcg(B, x->v.get(), b->v.get(), tol, max_iter, iters, relres);
+    });
+}
+
+int rb_batch_host_waits(rb_batch B, int* waits) {
+    return guarded([&]() -> int {
+        NEED(B); NEED(waits);
+        *waits = batch_host_waits(B);
+        return RB_OK;
     });
 }
 

@@ -63,9 +63,11 @@ struct DiaOff {
     long long o[kMaxDiag];
 };
 
-template <int ND, typename TV, typename TX, typename Acc>
+// SC: the gathered vector is x_j * xs_j (the fused first sweep, spmv.cuh)
+template <int ND, typename TV, typename TX, typename Acc, bool SC = false>
 __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const TV* __restrict__ base,
-                                        const TX* __restrict__ x) {
+                                        const TX* __restrict__ x,
+                                        const TX* __restrict__ xs = nullptr) {
     Acc s = 0;
     if constexpr (ND > 0) {
 #if RB_DIA_TWO_PHASE
@@ -78,11 +80,15 @@ __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const
 #pragma unroll
         for (int d = 0; d < ND; d++) {
             const long j = i + off.o[d];
-            xv[d] = (j >= 0 && j < n) ? __ldg(x + j) : TX(0);
+            if constexpr (SC)
+                xv[d] = (j >= 0 && j < n) ? (TX)(__ldg(x + j) * __ldg(xs + j)) : TX(0);
+            else
+                xv[d] = (j >= 0 && j < n) ? __ldg(x + j) : TX(0);
         }
 #pragma unroll
         for (int d = 0; d < ND; d++) s += (Acc)v[d] * (Acc)xv[d];
 #else
+        static_assert(!SC, "scaled gathers need the two-phase row loop");
         TV v[ND];
 #pragma unroll
         for (int d = 0; d < ND; d++) v[d] = __ldg(base + d * 32);
@@ -96,7 +102,11 @@ __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const
 #pragma unroll 4
         for (int d = 0; d < off.nd; d++) {
             const long j = i + off.o[d];
-            if (j >= 0 && j < n) s += (Acc)__ldg(base + d * 32) * (Acc)__ldg(x + j);
+            if (j >= 0 && j < n) {
+                TX xj = __ldg(x + j);
+                if constexpr (SC) xj = (TX)(xj * __ldg(xs + j));
+                s += (Acc)__ldg(base + d * 32) * (Acc)xj;
+            }
         }
     }
     return s;
@@ -105,6 +115,8 @@ __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const
 template <int ND, typename TV, typename TX, typename Acc, class Epi>
 __global__ void __launch_bounds__(256, RB_DIA_MINB_ROWS)
 k_sdia_rows(long n, DiaOff off, const TV* __restrict__ sv, const TX* __restrict__ x, Epi epi) {
+    constexpr bool SC = ScaledGather<Epi>::value;
+    const TX* xs = gather_scale_of<Epi, TX>(epi);
     const int lane = threadIdx.x & 31;
     const int nd = ND > 0 ? ND : off.nd;
     const long nslices = (n + 31) >> 5;
@@ -117,12 +129,12 @@ k_sdia_rows(long n, DiaOff off, const TV* __restrict__ sv, const TX* __restrict_
             // the epilogue's operands are loaded with the row's values and x
             typename Epi::Pre pr{};
             if (i < n) pr = epi.pre(i);
-            const Acc s = sdia_row<ND, TV, TX, Acc>(i, n, off, sv + sl * nd * 32 + lane, x);
+            const Acc s = sdia_row<ND, TV, TX, Acc, SC>(i, n, off, sv + sl * nd * 32 + lane, x, xs);
             if (i < n) epi.post(i, s, red, pr);
         } else
 #endif
         {
-            const Acc s = sdia_row<ND, TV, TX, Acc>(i, n, off, sv + sl * nd * 32 + lane, x);
+            const Acc s = sdia_row<ND, TV, TX, Acc, SC>(i, n, off, sv + sl * nd * 32 + lane, x, xs);
             if (i < n) epi(i, s, red);
         }
     }

@@ -536,6 +536,34 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
         }
         if (!V.dia) tune_idx16(V.A, V.A16, V.gA, V.x.get(), V.r.get(), "A16");
     }
+    // the first sweep from zero fused with the residual, per level, where
+    // one pass over A_l gathering b d beats the sweep and the residual apart
+    const int rt = opts.relax_type;
+    const bool jac1 = ((rt == RB_RELAX_JACOBI && !opts.jacobi_compat) || rt == RB_RELAX_L1JACOBI) &&
+                      opts.num_smooth_sweeps == 1;
+    for (int l = 0; l + 1 < L && jac1; l++) {
+        Level<T>& V = lv[l];
+        const std::string key = tune_key(V.dia ? "first_dia" : "first", V.n, V.A.nnz, (int)sizeof(T));
+        auto& c = tune_cache();
+        auto it = c.m.find(key);
+        if (it != c.m.end()) {
+            V.fuse_first = it->second != 0;
+            continue;
+        }
+        launch_vec<T>(k_fill<T>, V.n, V.b.get(), T(1));
+        const float t_sep = time_launch([&] {
+            k_scale_first<T, T><<<grid_for(V.n, 256), 256, 0, stream()>>>(V.n, V.b.get(),
+                                                                          V.dinv.get(), V.x.get());
+            RB_CHECK_LAUNCH();
+            V.apply_A(V.x.get(), EpiResidual<T, T>{V.b.get(), V.r.get()});
+        });
+        const float t_fused = time_launch([&] {
+            V.apply_A(V.b.get(), EpiFirstResidual<T>{V.b.get(), V.dinv.get(), V.r.get(), V.x.get()});
+        });
+        V.fuse_first = t_fused < t_sep;
+        c.m[key] = V.fuse_first ? 1 : 0;
+        tune_save();
+    }
     RB_CUDA(cudaStreamSynchronize(stream()));
 }
 
@@ -566,7 +594,6 @@ void Hierarchy::build_cycle_data() {
     }
     if (opts.precision == RB_PREC_FP32) {
         build_levels(lv32);
-        build_fused(lv32, fdesc32);
         const rb_csr_s& A0 = *master[0].A;
         DevArray<int> flag(1);
         flag.zero();
@@ -576,7 +603,6 @@ void Hierarchy::build_cycle_data() {
         a0_fp32_exact = read_scalar(flag.get()) == 0;
     } else {
         build_levels(lv64);
-        build_fused(lv64, fdesc64);
     }
     // Krylov work vectors (FP64, finest size)
     const int n = master[0].A->n_rows;
@@ -594,34 +620,29 @@ void Hierarchy::build_cycle_data() {
     if (!host_scal) RB_CUDA(cudaMallocHost(&host_scal, sizeof(KScal)));
     if (!host_ctl) RB_CUDA(cudaMallocHost(&host_ctl, sizeof(PcgCtl)));
     gA0 = autotune_group(view(*master[0].A), kp.get(), kAp.get(), "A0_fp64");
+    if (opts.precision == RB_PREC_FP32) tune_tail(lv32, tdesc32);
+    else tune_tail(lv64, tdesc64);
 }
 
 Hierarchy::~Hierarchy() {
     release_graphs();
     if (host_scal) cudaFreeHost(host_scal);
     if (host_ctl) cudaFreeHost(host_ctl);
-    if (host_barrier_error) cudaFreeHost(host_barrier_error);
 }
 
-// Levels below kFuseRows rows (and every level after them) run inside one
-// cooperative launch when the smoother is Jacobi-type with one sweep.
-constexpr int kFuseRows = 100000;
+// The tail of the cycle (tail_cycle.cuh).  A start level f >= 1 qualifies
+// when every level from f to L-2 is CSR (not by diagonals), the coarse
+// solve is the explicit-inverse product, and the smoother is one
+// Jacobi-type sweep (or the reference's no-op Jacobi); the start is picked
+// by timing the whole cycle for every qualifying f and without the tail
+// (decision cached per hierarchy like the operator widths).
+constexpr int kTailMaxRows = 1 << 20;
 
 template <typename T>
-void Hierarchy::build_fused(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc) {
-    fuse_from = -1;
+void Hierarchy::build_tail(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc, int from) {
     const int L = (int)lv.size();
-    const int rt = opts.relax_type;
-    const bool jac = rt == RB_RELAX_JACOBI || rt == RB_RELAX_L1JACOBI;
-    if (!opts.fuse_coarse || !jac || opts.num_smooth_sweeps != 1 || L < 3 ||
-        coarse_n * 8 > 40000)
-        return;
-    int f = -1;
-    for (int l = 1; l < L - 1; l++)
-        if (lv[l].n <= kFuseRows) { f = l; break; }
-    if (f < 0) return;
     std::vector<LevelDesc<T>> h;
-    for (int l = f; l < L - 1; l++) {
+    for (int l = from; l < L - 1; l++) {
         Level<T>& V = lv[l];
         LevelDesc<T> d{};
         d.n = V.n;
@@ -635,38 +656,117 @@ void Hierarchy::build_fused(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& d
     }
     desc.alloc(h.size());
     desc.upload(h.data(), h.size());
-    barrier.alloc(1);
-    barrier.zero();
-    if (!host_barrier_error) RB_CUDA(cudaMallocHost(&host_barrier_error, sizeof(int)));
-    int per_sm = 0;
-    RB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coarse_cycle<T>, kFuseBlock,
-                                                          sizeof(double) * coarse_n));
-    if (per_sm < 1) return;
-    fuse_grid = sm_count() * std::min(per_sm, 2);
     RB_CUDA(cudaStreamSynchronize(stream()));
-    fuse_from = f;
+    tail_from = from;
 }
 
 template <typename T>
-void Hierarchy::launch_fused(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc) {
+void Hierarchy::launch_tail(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc) {
     const int L = (int)lv.size();
-    const int nl = L - 1 - fuse_from;
+    const int nl = L - 1 - tail_from;
     const int smooth = opts.jacobi_compat && opts.relax_type == RB_RELAX_JACOBI ? 0 : 1;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(fuse_grid);
-    cfg.blockDim = dim3(kFuseBlock);
-    cfg.dynamicSmemBytes = sizeof(double) * std::max(coarse_n, 1);
+    cfg.gridDim = dim3(tail_ctas);
+    cfg.blockDim = dim3(kTailBlock);
+    cfg.dynamicSmemBytes = 0;
     cfg.stream = stream();
     cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = tail_ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    RB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T>, (const LevelDesc<T>*)desc.get(), nl,
-                               (const double*)lu.get(), (const int*)piv.get(), coarse_n,
-                               lv[L - 1].x.get(), (const T*)lv[L - 1].b.get(), smooth,
-                               barrier.get()));
+    RB_CUDA(cudaLaunchKernelEx(&cfg, k_tail_cycle<T>, (const LevelDesc<T>*)desc.get(), nl,
+                               (const double*)cinv.get(), (const double*)lu.get(),
+                               (const int*)piv.get(), coarse_n, lv[L - 1].x.get(),
+                               (const T*)lv[L - 1].b.get(), smooth));
     RB_CHECK_LAUNCH();
+}
+
+template <typename T>
+void Hierarchy::tune_tail(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc) {
+    tail_from = -1;
+    tail_ms.clear();
+    const int L = (int)lv.size();
+    const int rt = opts.relax_type;
+    const bool jac = (rt == RB_RELAX_JACOBI || rt == RB_RELAX_L1JACOBI) &&
+                     (opts.num_smooth_sweeps == 1 || (rt == RB_RELAX_JACOBI && opts.jacobi_compat));
+    if (!opts.fuse_coarse || !jac || L < 3 || !cinv.get() || !use_graphs) return;
+    std::vector<int> cands;
+    for (int f = L - 2; f >= 1; f--) {
+        if (lv[f].dia || lv[f].n > kTailMaxRows) break;
+        cands.push_back(f);
+    }
+    if (cands.empty()) return;
+    // one cluster: as many CTAs of kTailBlock threads as the device allows
+    // (16 with the non-portable size enabled, else 8)
+    if (!tail_ctas) {
+        int cs = 0;
+        if (cudaFuncSetAttribute(k_tail_cycle<T>, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                                 1) == cudaSuccess) {
+            cudaLaunchConfig_t q = {};
+            q.gridDim = dim3(kTailMaxCluster);
+            q.blockDim = dim3(kTailBlock);
+            if (cudaOccupancyMaxPotentialClusterSize(&cs, k_tail_cycle<T>, &q) != cudaSuccess) cs = 0;
+        }
+        (void)cudaGetLastError();
+        tail_ctas = std::min(cs, kTailMaxCluster);
+        if (tail_ctas < 1) return;
+    }
+    const rb_csr_s& A0 = *master[0].A;
+    // keyed by the whole hierarchy's shape (levels, rows and nonzeros of
+    // every level) and the smoother
+    long long shape = 0;
+    for (int l = 0; l < L; l++)
+        shape = shape * 1000003LL + master[l].A->n_rows * 31LL + master[l].A->nnz;
+    char op[64];
+    snprintf(op, sizeof(op), "tail%d_%d_%d_%llx", L, rt, opts.jacobi_compat,
+             (unsigned long long)shape);
+    const std::string key = tune_key(op, A0.n_rows, A0.nnz, (int)sizeof(T));
+    auto& c = tune_cache();
+    auto it = c.m.find(key);
+    int best = -1;
+    if (opts.fuse_coarse >= 2) {
+        best = opts.fuse_coarse - 1;   // a forced start level
+    } else if (it != c.m.end()) {
+        best = it->second;
+    } else {
+        // time the whole cycle (graph replay) from each start, and without
+        const long n = A0.n_rows;
+        launch_vec<double>(k_fill<double>, n, kr.get(), 1.0);
+        auto time_cycle = [&]() {
+            release_graphs();
+            cycle(kz.get(), kr.get(), true);
+            cycle(kz.get(), kr.get(), true);
+            cudaEvent_t e0, e1;
+            RB_CUDA(cudaEventCreate(&e0));
+            RB_CUDA(cudaEventCreate(&e1));
+            RB_CUDA(cudaEventRecord(e0, stream()));
+            for (int r = 0; r < 20; r++) cycle(kz.get(), kr.get(), true);
+            RB_CUDA(cudaEventRecord(e1, stream()));
+            RB_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            RB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return ms / 20;
+        };
+        tail_from = -1;
+        double best_ms = time_cycle();
+        tail_ms.push_back(best_ms);
+        for (int f : cands) {
+            build_tail(lv, desc, f);
+            const double ms = time_cycle();
+            tail_ms.push_back(ms);
+            if (ms < best_ms) { best_ms = ms; best = f; }
+        }
+        tail_from = -1;
+        release_graphs();
+        c.m[key] = best;
+        tune_save();
+    }
+    if (std::find(cands.begin(), cands.end(), best) != cands.end()) build_tail(lv, desc, best);
 }
 
 void Hierarchy::release_graphs() {
@@ -748,23 +848,32 @@ void Hierarchy::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, 
         mark(l * kProfSlots + 5);
         return;
     }
-    if (l == fuse_from) {
-        // x and b are this level's own buffers here (fuse_from >= 1); the
-        // profile books the whole fused bottom as level fuse_from's slot 5
+    if (l == tail_from) {
+        // x and b are this level's own buffers here (tail_from >= 1, x = 0);
+        // the profile books the whole tail as level tail_from's slot 5
         mark(l * kProfSlots + 6);
-        if constexpr (std::is_same<T, float>::value) launch_fused(lv, fdesc32);
-        else launch_fused(lv, fdesc64);
+        if constexpr (std::is_same<T, float>::value) launch_tail(lv, tdesc32);
+        else launch_tail(lv, tdesc64);
         mark(l * kProfSlots + 5);
         return;
     }
     Level<T>& C = lv[l + 1];
     T* cur = x;
     T* other = V.xt.get();
+    const int rt = opts.relax_type;
+    const bool jacobi_type = (rt == RB_RELAX_JACOBI && !opts.jacobi_compat) || rt == RB_RELAX_L1JACOBI;
     mark(l * kProfSlots + 6);
-    smooth(V, cur, other, b, x_zero);
-    mark(l * kProfSlots + 0);
-    // r = b - A x ; b_c = R r   (par_multilevel.hpp:409-411)
-    V.apply_A(cur, EpiResidual<T, T>{b, V.r.get()});
+    if (x_zero && jacobi_type && opts.num_smooth_sweeps == 1 && V.fuse_first) {
+        // one sweep from zero, x = D^-1 b, fused with r = b - A x (the
+        // profile books the pair as the residual)
+        mark(l * kProfSlots + 0);
+        V.apply_A(b, EpiFirstResidual<T>{b, V.dinv.get(), V.r.get(), cur});
+    } else {
+        smooth(V, cur, other, b, x_zero);
+        mark(l * kProfSlots + 0);
+        // r = b - A x ; b_c = R r   (par_multilevel.hpp:409-411)
+        V.apply_A(cur, EpiResidual<T, T>{b, V.r.get()});
+    }
     mark(l * kProfSlots + 1);
     rows_op(V.R, V.R16, C.n, V.r.get(),
                 EpiStore<T>{C.b.get()}, V.gR);
@@ -773,8 +882,6 @@ void Hierarchy::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, 
     mark(l * kProfSlots + 6);
     // x += P x_c (par_multilevel.hpp:430), into the buffer from which the
     // post-smoothing ping-pong ends in x
-    const int rt = opts.relax_type;
-    const bool jacobi_type = (rt == RB_RELAX_JACOBI && !opts.jacobi_compat) || rt == RB_RELAX_L1JACOBI;
     T* start = x;
     if (jacobi_type && (opts.num_smooth_sweeps & 1)) start = (x == V.xt.get()) ? nullptr : V.xt.get();
     if (!start) start = x;
@@ -832,13 +939,16 @@ std::vector<double> Hierarchy::profile_cycle() {
 }
 
 // Average time of one launch of a cycle operator (op 0 residual with A_l,
-// 1 restriction R_l, 2 prolongation P_l, 3 Jacobi sweep with A_l, in the
-// cycle precision; 4 the outer FP64 A p with p.Ap on the finest level).
+// 1 restriction R_l, 2 prolongation P_l, 3 Jacobi sweep with A_l, 6 the
+// first sweep fused with the residual, 7 the first sweep alone, in the
+// cycle precision; 4 the outer FP64 A p with p.Ap on the finest level; 5 one
+// preconditioner application).
 template <typename T>
 static double time_op_impl(Hierarchy& H, std::vector<Level<T>>& lv, int l, int op, int reps) {
     RB_REQUIRE(l >= 0 && l < (int)lv.size(), "level out of range");
     Level<T>& V = lv[l];
-    RB_REQUIRE(op == 0 || op == 3 || l < (int)lv.size() - 1, "the coarsest level has no P/R");
+    RB_REQUIRE(op == 0 || op == 3 || op == 6 || op == 7 || l < (int)lv.size() - 1,
+               "the coarsest level has no P/R");
     auto launch = [&]() {
         switch (op) {
             case 0:
@@ -851,6 +961,15 @@ static double time_op_impl(Hierarchy& H, std::vector<Level<T>>& lv, int l, int o
             case 2:
                 rows_op(V.P, V.P16, V.n, lv[l + 1].x.get(),
                             EpiAppend<T>{V.x.get()}, V.gP);
+                break;
+            case 6:
+                V.apply_A(V.b.get(), EpiFirstResidual<T>{V.b.get(), V.dinv.get() ? V.dinv.get() : V.b.get(),
+                                                         V.r.get(), V.xt.get()});
+                break;
+            case 7:
+                k_scale_first<T, T><<<grid_for(V.n, 256), 256, 0, stream()>>>(
+                    V.n, V.b.get(), V.dinv.get() ? V.dinv.get() : V.b.get(), V.xt.get());
+                RB_CHECK_LAUNCH();
                 break;
             default:
                 V.apply_A(V.x.get(), EpiJacobi<T, T, T>{V.x.get(), V.b.get(),
@@ -1058,18 +1177,18 @@ k_cg_update_f32(long n, double* __restrict__ x, double* __restrict__ r,
     block_reduce_finish(t, rs, fin);
 }
 
-// z = (double) x32 fused with r.z (the V-cycle's output conversion)
+// r.z with z the FP32 V-cycle's output, widened to FP64 as it is read: the
+// preconditioned residual is never stored in FP64 (the p update reads the
+// FP32 copy too), which saves 12 of the 24 bytes a row a conversion pass
+// moves
 template <class Fin>
 __global__ void __launch_bounds__(256)
-k_convert_dot(long n, const float* __restrict__ x32, const double* __restrict__ r,
-              double* __restrict__ z, ReduceSlot rs, Fin fin) {
+k_dot_z32(long n, const float* __restrict__ z32, const double* __restrict__ r, ReduceSlot rs,
+          Fin fin) {
     double t = 0.0;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long)gridDim.x * blockDim.x) {
-        const double zi = (double)x32[i];
-        z[i] = zi;
-        t += r[i] * zi;
-    }
+         i += (long)gridDim.x * blockDim.x)
+        t += r[i] * (double)z32[i];
     block_reduce_finish(t, rs, fin);
 }
 
@@ -1106,12 +1225,7 @@ void Hierarchy::dot_into(const double* a, const double* b, long n, double* field
 
 KScal Hierarchy::read_scal() {
     RB_CUDA(cudaMemcpyAsync(host_scal, scal.get(), sizeof(KScal), cudaMemcpyDeviceToHost, stream()));
-    if (fuse_from >= 0)
-        RB_CUDA(cudaMemcpyAsync(host_barrier_error, &barrier.get()->error, sizeof(int),
-                                cudaMemcpyDeviceToHost, stream()));
     RB_CUDA(cudaStreamSynchronize(stream()));
-    if (fuse_from >= 0 && *host_barrier_error)
-        throw Error(RB_ERR_CUDA, "coarse-cycle grid barrier timed out");
     return *host_scal;
 }
 
@@ -1261,8 +1375,8 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
                 RB_CHECK_LAUNCH();
             }
             cycle_level(lv32, 0, V.x.get(), V.b.get(), true);
-            k_convert_dot<<<rg, 256, 0, stream()>>>(n, V.x.get(), r, z, global_reduce_slot(rg),
-                                                    FinRZ{S});
+            k_dot_z32<<<rg, 256, 0, stream()>>>(n, V.x.get(), r, global_reduce_slot(rg),
+                                                FinRZ{S});
         } else {
             cycle64(z, r, true);
             k_dot_fin<<<rg, 256, 0, stream()>>>(r, z, n, global_reduce_slot(rg), FinRZ{S});
@@ -1287,7 +1401,10 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
         // converged recursive residual with the true one, as before.
         int pmode = 0;   // p = z already (set above)
         auto iteration = [&](bool full_r, cudaGraphConditionalHandle h, int use_cond) {
-            k_cg_p_dev<<<grid_for(n, 256), 256, 0, stream()>>>(n, p, z, S);
+            if (fp32)
+                k_cg_p_dev<<<grid_for(n, 256), 256, 0, stream()>>>(n, p, (const float*)lv32[0].x.get(), S);
+            else
+                k_cg_p_dev<<<grid_for(n, 256), 256, 0, stream()>>>(n, p, (const double*)z, S);
             RB_CHECK_LAUNCH();
             body(full_r);
             k_pcg_step_end<<<1, 32, 0, stream()>>>(S, h, use_cond);
@@ -1370,7 +1487,12 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
         if (done) { status = RB_OK; break; }
         // p = z + beta p  (restart p = z after a full residual)
         const bool restart = (mode == RB_PCG_REFERENCE) && full_r;
-        k_cg_p<<<grid_for(n, 256), 256, 0, stream()>>>(n, p, z, S, restart ? 1 : 0);
+        if (fp32)
+            k_cg_p<<<grid_for(n, 256), 256, 0, stream()>>>(n, p, (const float*)lv32[0].x.get(), S,
+                                                           restart ? 1 : 0);
+        else
+            k_cg_p<<<grid_for(n, 256), 256, 0, stream()>>>(n, p, (const double*)z, S,
+                                                           restart ? 1 : 0);
         RB_CHECK_LAUNCH();
     }
     *n_hist = nh;

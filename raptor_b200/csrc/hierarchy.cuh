@@ -8,9 +8,9 @@
 #include <vector>
 
 #include "blas1.cuh"
-#include "coarse_cycle.cuh"
 #include "dia.cuh"
 #include "rb_internal.cuh"
+#include "tail_cycle.cuh"
 
 namespace rb {
 
@@ -82,6 +82,7 @@ struct Level {
     DevArray<T> x, b, r, xt;
     int gA = 0, gP = 0, gR = 0;        // lanes per row picked by the autotuner
     bool dia = false;                  // A_l by diagonals (the autotuner's pick)
+    bool fuse_first = false;           // first sweep fused with the residual (timed pick)
     DiaOff off{};
     DevArray<T> Adia;
     void alloc_vectors();
@@ -110,17 +111,19 @@ struct Hierarchy {
     PcgCtl* host_ctl = nullptr;   // pinned staging of the device-side loop state
     int gA0 = 0;
     bool use_graphs = true;
-    // fused bottom of the cycle (levels fuse_from .. L-1 in one launch)
-    int fuse_from = -1;
-    int fuse_grid = 0;
-    DevArray<LevelDesc<double>> fdesc64;
-    DevArray<LevelDesc<float>> fdesc32;
-    DevArray<BarrierState> barrier;
-    int* host_barrier_error = nullptr;
+    // bottom of the cycle (levels tail_from .. L-1) in one launch of one
+    // cluster of tail_ctas CTAs (tail_cycle.cuh); tail_from = -1: off
+    int tail_from = -1;
+    int tail_ctas = 0;
+    DevArray<LevelDesc<double>> tdesc64;
+    DevArray<LevelDesc<float>> tdesc32;
     template <typename T>
-    void build_fused(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc);
+    void build_tail(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc, int from);
     template <typename T>
-    void launch_fused(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc);
+    void launch_tail(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc);
+    template <typename T>
+    void tune_tail(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& desc);
+    std::vector<double> tail_ms;   // cycle ms per candidate start (tuning record)
     std::map<std::string, cudaGraphExec_t> graphs;
     std::map<std::string, long long> graph_kernels;
     // the matrix handed to setup: PCG on it reads the hierarchy's copies of

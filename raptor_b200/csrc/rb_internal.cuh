@@ -107,6 +107,7 @@ long long batch_offset(const rb_batch_s* B, int s);
 int batch_levels(const rb_batch_s* B, int s);
 int batch_packed_levels(const rb_batch_s* B);
 void batch_cycle(rb_batch_s* B, double* x, const double* b);
+int batch_host_waits(const rb_batch_s* B);
 int batch_pcg(rb_batch_s* B, double* x, const double* b, double tol, int max_iter, int* iters,
               double* relres);
 

@@ -163,6 +163,67 @@ struct HasPre : std::false_type {};
 template <class Epi>
 struct HasPre<Epi, std::void_t<typename Epi::Pre>> : std::true_type {};
 
+// The first Jacobi-type sweep from a zero iterate fused with the residual
+// that follows it (ParMultilevel::cycle's relax then residual,
+// par_multilevel.hpp:393-409, with x = 0 on entry): the sweep's result is
+// x_i = b_i d_i (d = w / a_ii, or w / sum_j |a_ij| for L1-Jacobi), so the
+// row product gathers b_j d_j in place of x_j, and the epilogue stores both
+// x_i and r_i = b_i - (A x)_i.  Bit for bit what the sweep kernel and the
+// residual kernel compute one after the other, in one pass instead of two:
+// x is neither written before nor read back by the product.
+template <typename T>
+struct EpiFirstResidual {
+    const T* b;
+    const T* d;
+    T* r;
+    T* x;
+    __host__ __device__ const T* gather_scale() const { return d; }
+    template <typename A>
+    __device__ void operator()(long i, A s, double&) const {
+        const T bi = b[i];
+        x[i] = (T)(bi * d[i]);
+        r[i] = (T)((A)bi - s);
+    }
+    struct Pre { T b; T d; };
+    __device__ Pre pre(long i) const { return Pre{__ldg(b + i), __ldg(d + i)}; }
+    template <typename A>
+    __device__ void post(long i, A s, double&, const Pre& p) const {
+        x[i] = (T)(p.b * p.d);
+        r[i] = (T)((A)p.b - s);
+    }
+};
+
+// r = b - A x only when *gate is nonzero (read on the device when the kernel
+// starts; otherwise every block returns at once).  Lets a step that only some
+// iterations of a device-side loop need sit in the loop's graph.
+template <typename TB, typename TY>
+struct EpiResidualIf {
+    const TB* b;
+    TY* r;
+    const int* gate;
+    __device__ bool open() const { return *(volatile const int*)gate != 0; }
+    template <typename A>
+    __device__ void operator()(long i, A s, double&) const { r[i] = (TY)((A)b[i] - s); }
+};
+
+template <class Epi, class = void>
+struct HasGate : std::false_type {};
+template <class Epi>
+struct HasGate<Epi, std::void_t<decltype(std::declval<const Epi&>().open())>> : std::true_type {};
+
+// Epilogues with gather_scale() make the row kernels gather x_j * scale_j.
+template <class Epi, class = void>
+struct ScaledGather : std::false_type {};
+template <class Epi>
+struct ScaledGather<Epi, std::void_t<decltype(std::declval<const Epi&>().gather_scale())>>
+    : std::true_type {};
+
+template <class Epi, typename TX>
+__host__ __device__ inline const TX* gather_scale_of(const Epi& epi) {
+    if constexpr (ScaledGather<Epi>::value) return epi.gather_scale();
+    else return nullptr;
+}
+
 // y = A p and accumulate p.y (the CG denominator)
 struct EpiStoreDot {
     const double* p;
@@ -194,9 +255,10 @@ struct NoFinish {
 #define RB_ROWS_BATCH 4
 #endif
 
-template <int G, int UN, typename Acc, typename CI, typename TV, typename TX>
+template <int G, int UN, typename Acc, bool SC = false, typename CI, typename TV, typename TX>
 __device__ __forceinline__ Acc row_batched(int j, int e, const CI* __restrict__ ci,
-                                           const TV* __restrict__ cv, const TX* __restrict__ xb) {
+                                           const TV* __restrict__ cv, const TX* __restrict__ xb,
+                                           const TX* __restrict__ xsb = nullptr) {
     Acc sum = 0;
     for (; j < e; j += UN * G) {
         int cc[UN];
@@ -209,7 +271,12 @@ __device__ __forceinline__ Acc row_batched(int j, int e, const CI* __restrict__ 
         }
         TX xx[UN];
 #pragma unroll
-        for (int q = 0; q < UN; q++) xx[q] = (j + q * G < e) ? __ldg(xb + cc[q]) : TX(0);
+        for (int q = 0; q < UN; q++) {
+            if constexpr (SC)
+                xx[q] = (j + q * G < e) ? (TX)(__ldg(xb + cc[q]) * __ldg(xsb + cc[q])) : TX(0);
+            else
+                xx[q] = (j + q * G < e) ? __ldg(xb + cc[q]) : TX(0);
+        }
 #pragma unroll
         for (int q = 0; q < UN; q++)
             if (j + q * G < e) sum += (Acc)vv[q] * (Acc)xx[q];
@@ -222,6 +289,11 @@ __global__ void RB_ROWS_BOUNDS
 k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
            const TV* __restrict__ cv, const TX* __restrict__ x, Epi epi) {
     using Acc = AccOf2<TV, TX>;
+    constexpr bool SC = ScaledGather<Epi>::value;
+    if constexpr (HasGate<Epi>::value) {
+        if (!epi.open()) return;
+    }
+    const TX* xs = gather_scale_of<Epi, TX>(epi);
     constexpr int RPW = 32 / G;
     const int lane = threadIdx.x & 31;
     const int sub = lane / G, gl = lane & (G - 1);
@@ -234,8 +306,9 @@ k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
         int s = 0, e = 0;
         if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); }
 #if RB_ROWS_BATCH > 0
-        Acc sum = row_batched<G, RB_ROWS_BATCH, Acc>(s + gl, e, ci, cv, x);
+        Acc sum = row_batched<G, RB_ROWS_BATCH, Acc, SC>(s + gl, e, ci, cv, x, xs);
 #else
+        static_assert(!SC, "scaled gathers need the batched row loop");
         Acc sum = 0;
         int j = s + gl;
         // four independent index/value loads ahead of their gathers
@@ -268,6 +341,8 @@ k_csr_rows16(long n, const int* __restrict__ rp, const int* __restrict__ rbase,
              const unsigned short* __restrict__ ci, const TV* __restrict__ cv,
              const TX* __restrict__ x, Epi epi) {
     using Acc = AccOf2<TV, TX>;
+    constexpr bool SC = ScaledGather<Epi>::value;
+    const TX* xs = gather_scale_of<Epi, TX>(epi);
     constexpr int RPW = 32 / G;
     const int lane = threadIdx.x & 31;
     const int sub = lane / G, gl = lane & (G - 1);
@@ -281,8 +356,10 @@ k_csr_rows16(long n, const int* __restrict__ rp, const int* __restrict__ rbase,
         if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); b0 = __ldg(rbase + row); }
         const TX* xb = x + b0;
 #if RB_ROWS_BATCH > 0
-        Acc sum = row_batched<G, RB_ROWS_BATCH, Acc>(s + gl, e, ci, cv, xb);
+        Acc sum = row_batched<G, RB_ROWS_BATCH, Acc, SC>(s + gl, e, ci, cv, xb,
+                                                         SC ? xs + b0 : nullptr);
 #else
+        static_assert(!SC, "scaled gathers need the batched row loop");
         Acc sum = 0;
         int j = s + gl;
         for (; j + 3 * G < e; j += 4 * G) {

@@ -31,11 +31,17 @@ int main(int argc, char** argv) {
         PCG(A, ml, x, b, res, 1e-8);
         ParVector r(n, n);
         A->residual(x, b, r);
-        std::printf("levels %d pcg_hist %zu relres %.3e\n", ml->num_levels, res.size(),
+        std::printf("levels %d pcg_hist %zu relres %.17e\n", ml->num_levels, res.size(),
                     r.norm(2) / b.norm(2));
+        std::printf("pcg");
+        for (double v : res) std::printf(" %.17e", v);
+        std::printf("\n");
         x.set_const_value(0.0);
         const int it = ml->solve(x, b);
-        std::printf("solve_iters %d last %.3e\n", it, ml->get_residuals().back());
+        std::printf("solve_iters %d last %.17e\n", it, ml->get_residuals().back());
+        std::printf("solve");
+        for (double v : ml->get_residuals()) std::printf(" %.17e", v);
+        std::printf("\n");
         delete ml;
         delete A;
     } catch (const error& e) {

@@ -4,7 +4,9 @@ Every system of a batch must behave as if solved alone: its hierarchy has
 the levels a standalone setup builds, one batch V-cycle equals the
 standalone V-cycle of each system (to rounding: 1e-11 relative in FP64,
 1e-5 in FP32), and the batch PCG gives each system the iterations (within
-one) and the solution of its standalone true-residual PCG.
+one) and the solution of its standalone true-residual PCG, with its
+iterations run on the device (a few host waits per solve, not one per
+iteration).
 """
 import math
 
@@ -79,6 +81,10 @@ def test_batch_pcg_matches_standalone_solves(kind, prec):
     x = rb.ParVector(B.total_rows)
     rc, iters, relres = B.pcg(x, rb.ParVector(B.total_rows, values=bh), tol=1e-8, max_iter=400)
     assert rc == 0
+    # the iterations run on the device: the host waits once per launch of
+    # the device loop (one, plus one per failed true-residual confirmation),
+    # not once per iteration
+    assert 1 <= B.host_waits <= 3 < int(max(iters)), (B.host_waits, int(max(iters)))
     got = x.numpy()
     for s, A in enumerate(mats):
         lo, hi = B.offsets[s], B.offsets[s + 1]

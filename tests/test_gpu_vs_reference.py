@@ -213,6 +213,8 @@ def test_lap27_64_bench_setup_and_histories():
         relres = np.linalg.norm(Ar.residual(x.numpy(), bh)) / np.linalg.norm(bh)
         assert relres <= 1e-8
         if prec == rb.FP64:
-            np.testing.assert_allclose(res, ho, rtol=1e-10, atol=0)
+            # the last entry is the confirming b - A x, whose cancellation
+            # leaves it about 1e-16 absolute (relative to ||b||) accurate
+            np.testing.assert_allclose(res, ho, rtol=1e-10, atol=1e-16)
         else:
             assert abs(len(res) - len(ho)) <= 1

@@ -225,3 +225,24 @@ def test_spmv_family(lap27_24):
     np.testing.assert_array_equal(Ar.spmv(x), O.spmv(Ao, x))
     np.testing.assert_array_equal(Ar.residual(x, b), O.residual(Ao, x, b))
     np.testing.assert_allclose(Ar.spmv_T(x), O.spmv_T(Ao, x), rtol=1e-14, atol=1e-14)
+
+
+def test_hierarchy_from_levels_solves_like_setup(lap27_24):
+    """The reference's ParMultilevel over levels handed to it (no setup;
+    duplicate_coarse factors A_c) runs the same PCG as after its own setup:
+    the form bench.py uses to time the reference's solve phase on a
+    hierarchy the GPU built (bit-identical to the reference's, as the
+    hierarchy tests show)."""
+    Ar, _, _ = lap27_24
+    kw = dict(theta=0.25, coarsen="pmis", interp="extended", interp_filter=0.3, relax="sor")
+    rml = O.RefHierarchy(Ar, **kw)
+    As = [rml.A(l).arrays() for l in range(rml.num_levels)]
+    Ps = [(rml.A(l + 1).shape[0],) + tuple(rml.P(l).arrays()) for l in range(rml.num_levels - 1)]
+    hml = O.RefHierarchy.from_levels(REF, As, Ps, **kw)
+    assert hml.num_levels == rml.num_levels
+    n = Ar.shape[0]
+    b = np.random.default_rng(AMG_SEED).uniform(-1, 1, n)
+    x1, h1 = O.ref_pcg(Ar, rml, np.zeros(n), b, tol=1e-10, max_iter=100)
+    x2, h2 = O.ref_pcg(Ar, hml, np.zeros(n), b, tol=1e-10, max_iter=100)
+    np.testing.assert_array_equal(h1, h2)
+    np.testing.assert_array_equal(x1, x2)
