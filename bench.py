@@ -79,9 +79,12 @@ def parse():
                    help="independent systems of the uneven batch (0 skips it)")
     p.add_argument("--diff-size", type=int, default=512,
                    help="grid side of the differentiation workload (0 skips it)")
-    p.add_argument("--aniso-size", type=int, default=0,
+    p.add_argument("--aniso-size", type=int, default=4096,
                    help="grid side of the 2D anisotropic precision-form workload "
-                        "(4096 for the full case; 0 skips it)")
+                        "(0 skips it)")
+    p.add_argument("--plain-size", type=int, default=128,
+                   help="grid side of the all-FP64 plain-method workload with its "
+                        "SpMV and V-cycle bandwidth figures (0 skips it)")
     return p.parse_args()
 
 
@@ -326,6 +329,65 @@ def run_aniso_precision(rb, ev, sync, S, steps=2):
         del ml
     out["speedup_fp32_over_fp64"] = out["fp64"]["ms"] / out["fp32"]["ms"]
     return out
+
+
+def run_plain_fp64(rb, ev, sync, S, steps=3):
+    """The plain method at scale in FP64: laplacian27 on S^3, RS (PMIS,
+    extended+i, L1-Jacobi), hierarchy and V-cycle in FP64, PCG to 1e-8 true
+    relative residual (b = A 1); plus the standalone bandwidth figures on the
+    finest matrix the reference's examples/benchmark_spmv.cpp times: one
+    SpMV b = A x through the public entry point on the caller's FP64 CSR
+    matrix, and one FP64 V-cycle."""
+    A = rb.par_stencil_grid(rb.laplace_stencil_27pt(), [S, S, S])
+    n = A.global_num_rows
+    nnz = A.local_nnz
+    ones = rb.ParVector(n)
+    ones.set_const_value(1.0)
+    b = rb.ParVector(n)
+    A.mult(ones, b)
+    ml = rb.ParRugeStubenSolver(0.25, rb.PMIS, rb.Extended, rb.Classical, rb.L1Jacobi)
+    ml.precision = rb.FP64
+    ml.setup(A)
+    x = rb.ParVector(n)
+    times, res = [], []
+    for s in range(1 + steps):
+        x.set_const_value(0.0)
+        res = []
+        sync()
+        e0 = ev()
+        rb.PCG(A, ml, x, b, res, tol=TOL, max_iter=500, mode=rb.PCG_TRUE_RESIDUAL)
+        e1 = ev()
+        sync()
+        if s >= 1:
+            times.append(e0.elapsed_time(e1))
+    # SpMV through rb_spmv on the FP64 CSR matrix: 12 B a nonzero, the row
+    # pointers, x gathered once and b written (algorithmic bytes)
+    y = rb.ParVector(n)
+    A.mult(ones, y)
+    sync()
+    reps = 20
+    e0 = ev()
+    for _ in range(reps):
+        A.mult(ones, y)
+    e1 = ev()
+    sync()
+    spmv_ms = e0.elapsed_time(e1) / reps
+    spmv_bytes = nnz * 12 + (n + 1) * 4 + 2 * n * 8
+    cyc_ms = ml.time_operator(0, 5, reps=20)
+    cb, _ = cycle_bytes(ml, 8)
+    peak, kind = peaks()
+    return {"workload": "laplacian27 %d^3, b = A 1: AMG-PCG to 1e-8 (RS: PMIS, extended+i, "
+                        "L1-Jacobi), hierarchy, V-cycle and PCG all FP64" % S,
+            "rows": n, "nnz": nnz, "levels": ml.num_levels, "setup_s": ml.setup_seconds,
+            "pcg_ms": sum(times) / len(times), "iters": len(res) - 1,
+            "final_rel_res": float(res[-1]),
+            "spmv": {"ms": spmv_ms, "alg_bytes": spmv_bytes,
+                     "gbs": spmv_bytes / (spmv_ms * 1e-3) / 1e9,
+                     "frac_of_%s_peak" % kind: spmv_bytes / (spmv_ms * 1e-3) / 1e9 / peak,
+                     "storage": "the caller's CSR, FP64 values, int32 indices"},
+            "vcycle": {"ms": cyc_ms, "alg_bytes": cb,
+                       "gbs": cb / (cyc_ms * 1e-3) / 1e9,
+                       "frac_of_%s_peak" % kind: cb / (cyc_ms * 1e-3) / 1e9 / peak}}
 
 
 def run_uneven_batch(rb, ev, sync, count=64, steps=2):
@@ -617,7 +679,9 @@ def run_b200(args, rank, world, local):
                    "alg_bytes_per_level": per_level,
                    "first_sweep_fused": [ml32.level_fused_first(l)
                                          for l in range(ml32.num_levels - 1)],
-                   "tail": dict(zip(("start_level", "ctas"), ml32.tail_info()))},
+                   "tail": dict(zip(("start_level", "ctas"), ml32.tail_info()),
+                                cycle_ms_by_start=ml32.tail_timings()),
+                   "levels": [ml32.level_info(l) for l in range(ml32.num_levels)]},
         "fp64_form": fp64,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic_for(dom),
@@ -643,6 +707,9 @@ def run_b200(args, rank, world, local):
     if args.aniso_size > 0:
         out["aniso_precision"] = run_aniso_precision(rb, ev, lambda: rb.lib().rb_synchronize(),
                                                      args.aniso_size)
+    if args.plain_size > 0:
+        out["plain_fp64"] = run_plain_fp64(rb, ev, lambda: rb.lib().rb_synchronize(),
+                                           args.plain_size)
     if rank == 0 and args.cpu_sample > 0:
         out["cpu_baseline"] = cpu_baseline(ml32, bh, args.cpu_sample, S)
     dist.close()

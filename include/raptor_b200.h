@@ -80,7 +80,9 @@ int rb_vec_dot(rb_vec a, rb_vec b, double* out); /* ParVector::inner_product, pa
 int rb_vec_norm2(rb_vec a, double* out);         /* ParVector::norm(2), par_vector.cpp:88-98 */
 
 /* --------------------------------------------------------- SpMV family */
-/* ParMatrix::mult, b = A x (util/linalg/par_spmv.cpp:25-59 -> spmv.cpp:52-67) */
+/* ParMatrix::mult, b = A x (util/linalg/par_spmv.cpp:25-59 -> spmv.cpp:52-67).
+ * The first product (of rb_spmv, rb_residual or rb_spmv_append) on a matrix
+ * times the row schedules once and keeps the fastest on the handle. */
 int rb_spmv(rb_csr A, rb_vec x, rb_vec b);
 /* ParMatrix::residual, r = b - A x (par_spmv.cpp:215-252 -> spmv.cpp:69-85) */
 int rb_residual(rb_csr A, rb_vec x, rb_vec b, rb_vec r);
@@ -252,6 +254,11 @@ int rb_amg_level_fused_first(rb_amg ml, int level, int* fused);
  * (-1: none) and the CTAs of that cluster.  No counterpart in the
  * reference (it describes how this library schedules the cycle). */
 int rb_amg_tail_info(rb_amg ml, int* start_level, int* ctas);
+/* The cycle times (ms) the setup measured to pick that level: without the
+ * cluster tail first, then for each qualifying start from the coarsest
+ * upwards (empty when the choice came from the tune cache or was forced).
+ * Writes min(*count, cap) values.  No counterpart in the reference. */
+int rb_amg_tail_timings(rb_amg ml, double* ms, int cap, int* count);
 /* Kernels this library has launched so far (graph replays count their
  * kernel nodes). */
 int rb_launch_count(int64_t* count);

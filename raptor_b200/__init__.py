@@ -482,6 +482,13 @@ class ParMultilevel:
         check(lib().rb_amg_level_fused_first(self.h, l, C.byref(f)))
         return bool(f.value)
 
+    def tail_timings(self):
+        """Cycle ms measured when the tail start was picked (see the C ABI)."""
+        c = C.c_int()
+        buf = np.zeros(64)
+        check(lib().rb_amg_tail_timings(self.h, buf, 64, C.byref(c)))
+        return [float(v) for v in buf[: min(c.value, 64)]]
+
     def tail_info(self):
         """(start level of the one-launch cluster tail or -1, its CTAs)."""
         f, c = C.c_int(), C.c_int()

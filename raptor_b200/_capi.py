@@ -117,6 +117,7 @@ SIGNATURES = {
     "rb_amg_level_storage": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "rb_amg_tail_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "rb_amg_level_fused_first": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_amg_tail_timings": (C.c_int, [_P, _D, C.c_int, C.POINTER(C.c_int)]),
     "rb_residual_norm_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "rb_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rb_device_alloc_count": (C.c_int, [C.POINTER(C.c_int64)]),

@@ -305,7 +305,7 @@ int rb_spmv(rb_csr A, rb_vec x, rb_vec b) {
     return guarded([&]() -> int {
         NEED(A); NEED(x); NEED(b);
         RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows, "spmv: sizes do not match");
-        spmv64(view(*A), x->v.get(), b->v.get());
+        spmv64(view(*A), x->v.get(), b->v.get(), handle_lanes(*A, x->v.get()));
         return RB_OK;
     });
 }
@@ -315,7 +315,7 @@ int rb_residual(rb_csr A, rb_vec x, rb_vec b, rb_vec r) {
         NEED(A); NEED(x); NEED(b); NEED(r);
         RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows && r->n == A->n_rows,
                    "residual: sizes do not match");
-        residual64(view(*A), x->v.get(), b->v.get(), r->v.get());
+        residual64(view(*A), x->v.get(), b->v.get(), r->v.get(), handle_lanes(*A, x->v.get()));
         return RB_OK;
     });
 }
@@ -336,7 +336,7 @@ int rb_spmv_append(rb_csr A, rb_vec x, rb_vec b) {
     return guarded([&]() -> int {
         NEED(A); NEED(x); NEED(b);
         RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows, "spmv_append: sizes do not match");
-        spmv_append64(view(*A), x->v.get(), b->v.get());
+        spmv_append64(view(*A), x->v.get(), b->v.get(), handle_lanes(*A, x->v.get()));
         return RB_OK;
     });
 }
@@ -794,6 +794,16 @@ int rb_amg_tail_info(rb_amg ml, int* start_level, int* ctas) {
         NEED(ml); NEED(start_level); NEED(ctas);
         *start_level = ml->h.tail_from;
         *ctas = ml->h.tail_from >= 0 ? ml->h.tail_ctas : 0;
+        return RB_OK;
+    });
+}
+
+int rb_amg_tail_timings(rb_amg ml, double* ms, int cap, int* count) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(count);
+        const auto& t = ml->h.tail_ms;
+        *count = (int)t.size();
+        for (int i = 0; i < (int)t.size() && i < cap && ms; i++) ms[i] = t[i];
         return RB_OK;
     });
 }

@@ -186,7 +186,10 @@ static int autotune_group(const CsrView<T>& M, T* xin, T* yout, const char* op =
 
 template <typename T>
 static int autotune_group_timed(const CsrView<T>& M, T* xin, T* yout) {
-    static const int cands[6] = {1, 2, 4, 8, 16, 32};
+    // lanes per row on the strided schedule, then (kRowsBlocked) on the
+    // blocked one
+    static const int cands[10] = {1, 2, 4, 8, 16, 32, kRowsBlocked | 4, kRowsBlocked | 8,
+                                  kRowsBlocked | 16, kRowsBlocked | 32};
     cudaEvent_t e0, e1;
     RB_CUDA(cudaEventCreate(&e0));
     RB_CUDA(cudaEventCreate(&e1));
@@ -541,8 +544,15 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
     const int rt = opts.relax_type;
     const bool jac1 = ((rt == RB_RELAX_JACOBI && !opts.jacobi_compat) || rt == RB_RELAX_L1JACOBI) &&
                       opts.num_smooth_sweeps == 1;
+    // RAPTOR_B200_FUSE_FIRST=0 never fuses, =1 always does, unset times it
+    const char* ff = getenv("RAPTOR_B200_FUSE_FIRST");
+    const int force_first = (ff && ff[0] == '0') ? 0 : (ff && ff[0] == '1') ? 1 : -1;
     for (int l = 0; l + 1 < L && jac1; l++) {
         Level<T>& V = lv[l];
+        if (force_first >= 0) {
+            V.fuse_first = force_first == 1;
+            continue;
+        }
         const std::string key = tune_key(V.dia ? "first_dia" : "first", V.n, V.A.nnz, (int)sizeof(T));
         auto& c = tune_cache();
         auto it = c.m.find(key);
@@ -601,6 +611,14 @@ void Hierarchy::build_cycle_data() {
             k_fp32_exact<<<grid_for(A0.nnz, 256), 256, 0, stream()>>>(A0.nnz, A0.vals.get(), flag.get());
         RB_CHECK_LAUNCH();
         a0_fp32_exact = read_scalar(flag.get()) == 0;
+        a0_64.n = 0;
+        a0_64.dia = false;
+        a0_64.Adia.release();
+        if (!a0_fp32_exact && lv32[0].dia) {
+            a0_64.n = A0.n_rows;
+            build_dia(a0_64, A0, lv32[0].off);
+            a0_64.dia = true;
+        }
     } else {
         build_levels(lv64);
     }
@@ -647,9 +665,10 @@ void Hierarchy::build_tail(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& de
         LevelDesc<T> d{};
         d.n = V.n;
         d.nc = lv[l + 1].n;
-        d.arp = V.A.rowptr; d.aci = V.A.cols; d.av = V.A.vals; d.gA = V.gA;
-        d.prp = V.P.rowptr; d.pci = V.P.cols; d.pv = V.P.vals; d.gP = V.gP;
-        d.rrp = V.R.rowptr; d.rci = V.R.cols; d.rv = V.R.vals; d.gR = V.gR;
+        const int lanes = kRowsBlocked - 1;   // the tail's own schedule
+        d.arp = V.A.rowptr; d.aci = V.A.cols; d.av = V.A.vals; d.gA = V.gA & lanes;
+        d.prp = V.P.rowptr; d.pci = V.P.cols; d.pv = V.P.vals; d.gP = V.gP & lanes;
+        d.rrp = V.R.rowptr; d.rci = V.R.cols; d.rv = V.R.vals; d.gR = V.gR & lanes;
         d.dinv = V.dinv.get();
         d.x = V.x.get(); d.b = V.b.get(); d.r = V.r.get(); d.xt = V.xt.get();
         h.push_back(d);
@@ -712,6 +731,9 @@ void Hierarchy::tune_tail(std::vector<Level<T>>& lv, DevArray<LevelDesc<T>>& des
         }
         (void)cudaGetLastError();
         tail_ctas = std::min(cs, kTailMaxCluster);
+        // RAPTOR_B200_TAIL_CTAS caps the cluster (measurements of the size)
+        const char* ce = getenv("RAPTOR_B200_TAIL_CTAS");
+        if (ce && atoi(ce) > 0) tail_ctas = std::min(tail_ctas, atoi(ce));
         if (tail_ctas < 1) return;
     }
     const rb_csr_s& A0 = *master[0].A;
@@ -813,7 +835,7 @@ void Hierarchy::smooth(Level<T>& V, T*& cur, T*& other, const T* b, bool x_zero)
     auto sweep = [&](int c, int backward) {
         const int cnt = V.colour_ptr[c + 1] - V.colour_ptr[c];
         if (cnt <= 0) return;
-        const int G = V.gA;
+        const int G = V.gA & (kRowsBlocked - 1);
         const unsigned grid = row_grid(cnt, G);
         const int* rows = V.colour_rows.get() + V.colour_ptr[c];
         switch (G) {
@@ -1264,6 +1286,10 @@ template <class Fin>
 void Hierarchy::outer_apply(const rb_csr_s& A, bool lowprec, const double* p, double* Ap, Fin fin) {
     const bool finest = is_finest(A);
     const long n = A.n_rows;
+    if (finest && opts.precision == RB_PREC_FP32 && !a0_fp32_exact && a0_64.dia) {
+        launch_dia_dot(a0_64.off, a0_64.Adia.get(), n, p, Ap, fin);
+        return;
+    }
     if (finest && lowprec && opts.precision == RB_PREC_FP32) {
         const Level<float>& V = lv32[0];
         if (V.dia) {
@@ -1291,6 +1317,10 @@ void Hierarchy::true_residual(const rb_csr_s& A, const double* x, const double* 
             lv32[0].apply_A(x, EpiResidual<double, double>{b, r});
             return;
         }
+        if (opts.precision == RB_PREC_FP32 && a0_64.dia) {
+            a0_64.apply_A(x, EpiResidual<double, double>{b, r});
+            return;
+        }
         if (opts.precision == RB_PREC_FP64 && lv64[0].dia) {
             lv64[0].apply_A(x, EpiResidual<double, double>{b, r});
             return;
@@ -1316,7 +1346,10 @@ int Hierarchy::pcg(const rb_csr_s& A, double* x, const double* b, double tol, in
     double* Ap = kAp.get();
     KScal* S = scal.get();
     const CsrView<double> Av = view(A);
-    const bool lowprec = mode == RB_PCG_TRUE_RESIDUAL && opts.precision == RB_PREC_FP32;
+    // the FP32 copy of A_0 serves as the outer operator only when it is A_0
+    // itself (every value exact in FP32); otherwise A p reads FP64 values
+    const bool lowprec = mode == RB_PCG_TRUE_RESIDUAL && opts.precision == RB_PREC_FP32 &&
+                         a0_fp32_exact;
     int nh = 0;
     auto push = [&](double v) {
         if (nh < cap) hist[nh] = v;

@@ -137,6 +137,10 @@ struct Hierarchy {
     // A_0 (FP64 accumulation) then is the operator itself, and residuals of
     // the outer iteration read it instead of the FP64 CSR matrix
     bool a0_fp32_exact = false;
+    // A_0 by diagonals in FP64 for the outer operator of the FP32 form when
+    // A_0's values are not exact in FP32 (then the FP32 copy is a perturbed
+    // operator, which an ill-conditioned problem does not tolerate)
+    Level<double> a0_64;
     void true_residual(const rb_csr_s& A, const double* x, const double* b, double* r);
     double setup_seconds = 0;
     int last_iters = 0;

@@ -23,6 +23,7 @@ struct rb_csr_s {
     rb::DevArray<int> rowptr, cols;
     rb::DevArray<double> vals;
     std::unique_ptr<rb::TransposeMap> tmap;  // lazily built by spmv_T64
+    int lanes = 0;  // row-kernel schedule of the public products (timed on first use)
 };
 
 struct rb_batch_s;
@@ -74,10 +75,15 @@ long long exclusive_scan(const int* in, int* out, int n);
 // Sum of n doubles, deterministic (fixed two-stage tree).
 void dot_async(const double* a, const double* b, int n, double* result_dev);
 
-// SpMV family on FP64 CSR (C ABI primitives).
-void spmv64(const CsrView<double>& A, const double* x, double* y);
-void residual64(const CsrView<double>& A, const double* x, const double* b, double* r);
-void spmv_append64(const CsrView<double>& A, const double* x, double* y);
+// SpMV family on FP64 CSR (C ABI primitives); lanes 0 picks the row
+// schedule from the mean row length.
+void spmv64(const CsrView<double>& A, const double* x, double* y, int lanes = 0);
+void residual64(const CsrView<double>& A, const double* x, const double* b, double* r,
+                int lanes = 0);
+void spmv_append64(const CsrView<double>& A, const double* x, double* y, int lanes = 0);
+// The fastest row schedule for a handle's products, timed once on x (the
+// handle keeps it).
+int handle_lanes(rb_csr_s& A, const double* x);
 // y = A^T x through the handle's cached transpose map (built on first use).
 void spmv_T64(rb_csr_s& A, const double* x, double* y);
 

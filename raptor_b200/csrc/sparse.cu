@@ -315,16 +315,47 @@ void dot_async(const double* a, const double* b, int n, double* result_dev) {
 }
 
 // ------------------------------------------------------- FP64 SpMV ops --
-void spmv64(const CsrView<double>& A, const double* x, double* y) {
-    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiStore<double>{y});
+void spmv64(const CsrView<double>& A, const double* x, double* y, int lanes) {
+    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiStore<double>{y}, lanes);
 }
 
-void residual64(const CsrView<double>& A, const double* x, const double* b, double* r) {
-    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiResidual<double, double>{b, r});
+void residual64(const CsrView<double>& A, const double* x, const double* b, double* r,
+                int lanes) {
+    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiResidual<double, double>{b, r},
+                lanes);
 }
 
-void spmv_append64(const CsrView<double>& A, const double* x, double* y) {
-    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiAppend<double>{y});
+void spmv_append64(const CsrView<double>& A, const double* x, double* y, int lanes) {
+    launch_rows(A.rowptr, A.cols, A.vals, A.n_rows, A.nnz, x, EpiAppend<double>{y}, lanes);
+}
+
+int handle_lanes(rb_csr_s& A, const double* x) {
+    if (A.lanes) return A.lanes;
+    if (A.n_rows < 4096 || A.nnz == 0) return A.lanes = pick_group(A.n_rows, A.nnz);
+    // products into a scratch vector of its own (the caller's output may be
+    // an input too, as in mult_append), each schedule timed over 3 launches
+    DevArray<double> y((size_t)A.n_rows);
+    static const int cands[10] = {2, 4, 8, 16, 32, kRowsBlocked | 4, kRowsBlocked | 8,
+                                  kRowsBlocked | 16, kRowsBlocked | 32, 1};
+    cudaEvent_t e0, e1;
+    RB_CUDA(cudaEventCreate(&e0));
+    RB_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bestG = pick_group(A.n_rows, A.nnz);
+    const CsrView<double> v = view(A);
+    for (int G : cands) {
+        spmv64(v, x, y.get(), G);
+        RB_CUDA(cudaEventRecord(e0, stream()));
+        for (int rep = 0; rep < 3; rep++) spmv64(v, x, y.get(), G);
+        RB_CUDA(cudaEventRecord(e1, stream()));
+        RB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        RB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) { best = ms; bestG = G; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return A.lanes = bestG;
 }
 
 }  // namespace rb

@@ -381,6 +381,77 @@ k_csr_rows16(long n, const int* __restrict__ rp, const int* __restrict__ rbase,
     (void)red;
 }
 
+// The same row kernels with a blocked schedule: one block of
+// kRowBlockBlk threads per SM, block b takes the contiguous rows
+// [b R, (b + 1) R) and its warps walk them RPW rows at a time, so the
+// columns an SM gathers stay within one window of x (a coarse operator's
+// rows couple to neighbouring rows only) and its L1 serves the gathers that
+// the strided schedule sends to L2.  Selected per operator by timing (the
+// lanes-per-row value carries kRowsBlocked).
+constexpr int kRowBlockBlk = 1024;
+constexpr int kRowsBlocked = 64;
+
+template <int G, typename TV, typename TX, class Epi>
+__global__ void __launch_bounds__(kRowBlockBlk, 1)
+k_csr_rows_blk(long n, const int* __restrict__ rp, const int* __restrict__ ci,
+               const TV* __restrict__ cv, const TX* __restrict__ x, Epi epi) {
+    using Acc = AccOf2<TV, TX>;
+    constexpr bool SC = ScaledGather<Epi>::value;
+    if constexpr (HasGate<Epi>::value) {
+        if (!epi.open()) return;
+    }
+    const TX* xs = gather_scale_of<Epi, TX>(epi);
+    constexpr int RPW = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / G, gl = lane & (G - 1);
+    const long per = ((n + gridDim.x - 1) / gridDim.x + RPW - 1) / RPW * RPW;
+    const long first = (long)blockIdx.x * per;
+    const long last = first + per < n ? first + per : n;
+    const int warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    double red = 0.0;
+    for (long base = first + (long)warp * RPW; base < last; base += (long)nw * RPW) {
+        const long row = base + sub;
+        const bool valid = row < last;
+        int s = 0, e = 0;
+        if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); }
+        Acc sum = row_batched<G, RB_ROWS_BATCH, Acc, SC>(s + gl, e, ci, cv, x, xs);
+        sum = group_sum<G>(sum);
+        if (valid && gl == 0) epi(row, sum, red);
+    }
+    (void)red;
+}
+
+template <int G, typename TV, typename TX, class Epi>
+__global__ void __launch_bounds__(kRowBlockBlk, 1)
+k_csr_rows16_blk(long n, const int* __restrict__ rp, const int* __restrict__ rbase,
+                 const unsigned short* __restrict__ ci, const TV* __restrict__ cv,
+                 const TX* __restrict__ x, Epi epi) {
+    using Acc = AccOf2<TV, TX>;
+    constexpr bool SC = ScaledGather<Epi>::value;
+    const TX* xs = gather_scale_of<Epi, TX>(epi);
+    constexpr int RPW = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / G, gl = lane & (G - 1);
+    const long per = ((n + gridDim.x - 1) / gridDim.x + RPW - 1) / RPW * RPW;
+    const long first = (long)blockIdx.x * per;
+    const long last = first + per < n ? first + per : n;
+    const int warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    double red = 0.0;
+    for (long base = first + (long)warp * RPW; base < last; base += (long)nw * RPW) {
+        const long row = base + sub;
+        const bool valid = row < last;
+        int s = 0, e = 0, b0 = 0;
+        if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); b0 = __ldg(rbase + row); }
+        Acc sum = row_batched<G, RB_ROWS_BATCH, Acc, SC>(s + gl, e, ci, cv, x + b0,
+                                                         SC ? xs + b0 : nullptr);
+        sum = group_sum<G>(sum);
+        if (valid && gl == 0) epi(row, sum, red);
+    }
+    (void)red;
+}
+
 template <int G, typename TV, class Fin>
 __global__ void RB_ROWS_BOUNDS
 k_csr_rows_dot(long n, const int* __restrict__ rp, const int* __restrict__ ci,
@@ -428,6 +499,8 @@ ReduceSlot global_reduce_slot(int grid);
 template <typename TV, class Fin>
 void launch_rows_dot(const int* rp, const int* ci, const TV* cv, long n, const double* x,
                      double* y, int G, Fin fin) {
+    G &= kRowsBlocked - 1;   // the dot kernel runs the strided schedule only
+    if (G <= 0) G = 8;
     const unsigned grid = row_grid_fwd(n, G);
     ReduceSlot rs = global_reduce_slot(grid);
     EpiStoreDot epi{x, y};
@@ -470,6 +543,19 @@ void launch_rows(const int* rp, const int* ci, const TV* cv, long n, long long n
     if (n <= 0) return;
     if (!st) st = stream();
     if (G <= 0) G = pick_group(n, nnz);
+    if (G & kRowsBlocked) {
+        const unsigned g = (unsigned)sm_count();
+        switch (G & (kRowsBlocked - 1)) {
+            case 1: k_csr_rows_blk<1><<<g, kRowBlockBlk, 0, st>>>(n, rp, ci, cv, x, epi); break;
+            case 2: k_csr_rows_blk<2><<<g, kRowBlockBlk, 0, st>>>(n, rp, ci, cv, x, epi); break;
+            case 4: k_csr_rows_blk<4><<<g, kRowBlockBlk, 0, st>>>(n, rp, ci, cv, x, epi); break;
+            case 8: k_csr_rows_blk<8><<<g, kRowBlockBlk, 0, st>>>(n, rp, ci, cv, x, epi); break;
+            case 16: k_csr_rows_blk<16><<<g, kRowBlockBlk, 0, st>>>(n, rp, ci, cv, x, epi); break;
+            default: k_csr_rows_blk<32><<<g, kRowBlockBlk, 0, st>>>(n, rp, ci, cv, x, epi); break;
+        }
+        RB_CHECK_LAUNCH();
+        return;
+    }
     const unsigned grid = row_grid(n, G);
     switch (G) {
         case 1: k_csr_rows<1><<<grid, kRowBlock, 0, st>>>(n, rp, ci, cv, x, epi); break;
@@ -487,8 +573,21 @@ void launch_rows16(const int* rp, const int* rbase, const unsigned short* c16, c
                    long n, long long nnz, const TX* x, Epi epi, int G = 0) {
     if (n <= 0) return;
     if (G <= 0) G = pick_group(n, nnz);
-    const unsigned grid = row_grid(n, G);
     cudaStream_t st = stream();
+    if (G & kRowsBlocked) {
+        const unsigned g = (unsigned)sm_count();
+        switch (G & (kRowsBlocked - 1)) {
+            case 1: k_csr_rows16_blk<1><<<g, kRowBlockBlk, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+            case 2: k_csr_rows16_blk<2><<<g, kRowBlockBlk, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+            case 4: k_csr_rows16_blk<4><<<g, kRowBlockBlk, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+            case 8: k_csr_rows16_blk<8><<<g, kRowBlockBlk, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+            case 16: k_csr_rows16_blk<16><<<g, kRowBlockBlk, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+            default: k_csr_rows16_blk<32><<<g, kRowBlockBlk, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
+        }
+        RB_CHECK_LAUNCH();
+        return;
+    }
+    const unsigned grid = row_grid(n, G);
     switch (G) {
         case 1: k_csr_rows16<1><<<grid, kRowBlock, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;
         case 2: k_csr_rows16<2><<<grid, kRowBlock, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;

@@ -40,8 +40,13 @@ __device__ __forceinline__ void cluster_barrier() {
 }
 
 // One row-parallel pass over every warp of the cluster, G lanes a row (G a
-// runtime power of two), f(row, sum) by the row's first lane.  x was written
-// in this launch: it is read through L2.
+// runtime power of two), f(row, sum) by the row's first lane.  A lane takes
+// its nonzeros kTailBatch at a time: the index and value loads of a batch,
+// then all its gathers, then the products in increasing position (the order
+// of the separate row kernel), so a warp keeps a batch of loads in flight
+// instead of one dependent pair.  x was written in this launch: it is read
+// through L2.
+constexpr int kTailBatch = 4;
 template <typename T, class F>
 __device__ __forceinline__ void tail_rows(int n, const int* __restrict__ rp,
                                           const int* __restrict__ ci, const T* __restrict__ cv,
@@ -57,7 +62,22 @@ __device__ __forceinline__ void tail_rows(int n, const int* __restrict__ rp,
         int s = 0, e = 0;
         if (valid) { s = __ldg(rp + row); e = __ldg(rp + row + 1); }
         T sum = 0;
-        for (int j = s + gl; j < e; j += G) sum += __ldg(cv + j) * __ldcg(x + __ldg(ci + j));
+        for (int j = s + gl; j < e; j += kTailBatch * G) {
+            int cc[kTailBatch];
+            T vv[kTailBatch];
+#pragma unroll
+            for (int q = 0; q < kTailBatch; q++) {
+                const bool ok = j + q * G < e;
+                cc[q] = ok ? __ldg(ci + j + q * G) : 0;
+                vv[q] = ok ? __ldg(cv + j + q * G) : T(0);
+            }
+            T xx[kTailBatch];
+#pragma unroll
+            for (int q = 0; q < kTailBatch; q++) xx[q] = (j + q * G < e) ? __ldcg(x + cc[q]) : T(0);
+#pragma unroll
+            for (int q = 0; q < kTailBatch; q++)
+                if (j + q * G < e) sum += vv[q] * xx[q];
+        }
         for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, G);
         if (valid && gl == 0) f(row, sum);
     }
@@ -78,13 +98,13 @@ k_tail_cycle(const LevelDesc<T>* __restrict__ lv, int nl, const double* __restri
     const long nthreads = (long)gridDim.x * blockDim.x;
     // ---- first level: x = D^-1 b from zero (or x = 0)
     {
-        const LevelDesc<T> L = lv[0];
+        const LevelDesc<T>& L = lv[0];
         for (long i = tid; i < L.n; i += nthreads)
             L.x[i] = smooth ? (T)(__ldcg(L.b + i) * __ldg(L.dinv + i)) : T(0);
     }
     // ---- down: residual, restriction (with the next level's first sweep)
     for (int l = 0; l < nl; l++) {
-        const LevelDesc<T> L = lv[l];
+        const LevelDesc<T>& L = lv[l];
         cluster_barrier();
         tail_rows<T>(L.n, L.arp, L.aci, L.av, L.x, L.gA,
                      [&](long i, T s) { L.r[i] = (T)(__ldcg(L.b + i) - s); });
@@ -133,7 +153,7 @@ k_tail_cycle(const LevelDesc<T>* __restrict__ lv, int nl, const double* __restri
     cluster_barrier();
     // ---- up: prolongation (into xt), post-sweep (back into x)
     for (int l = nl - 1; l >= 0; l--) {
-        const LevelDesc<T> L = lv[l];
+        const LevelDesc<T>& L = lv[l];
         const T* xnext = (l + 1 < nl) ? lv[l + 1].x : xc;
         if (smooth) {
             tail_rows<T>(L.n, L.prp, L.pci, L.pv, xnext, L.gP,

@@ -42,7 +42,10 @@ def test_shim_compiles_and_reports_missing_device(tmp_path):
 def test_shim_solves_on_the_gpu(tmp_path):
     """The compiled caller's PCG and stationary-solve histories equal those
     of the same calls through the Python mirror (one library, two front
-    ends), to the 17 digits printed."""
+    ends).  The two processes may pick different lane counts for a row
+    kernel (the autotuner times them), which reorders a row's sums, so the
+    histories agree to 1e-10 relative above a floor of 1e-15 of the first
+    entry rather than bit for bit."""
     exe = build(tmp_path)
     r = subprocess.run([exe, "20"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
@@ -66,8 +69,9 @@ def test_shim_solves_on_the_gpu(tmp_path):
     x = rb.ParVector(n)
     res = []
     rb.PCG(A, ml, x, b, res, 1e-8)
-    np.testing.assert_allclose(pcg_cxx, res, rtol=1e-15, atol=0)
+    np.testing.assert_allclose(pcg_cxx, res, rtol=1e-10, atol=1e-15 * res[0])
     x.set_const_value(0.0)
     ml.solve(x, b)
-    np.testing.assert_allclose(solve_cxx, ml.get_residuals(), rtol=1e-15, atol=0)
+    np.testing.assert_allclose(solve_cxx, ml.get_residuals(), rtol=1e-10,
+                               atol=1e-15 * ml.get_residuals()[0])
     assert solve_cxx[-1] <= 1e-8

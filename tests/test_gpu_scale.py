@@ -95,3 +95,28 @@ def test_192_solve_histories_match_fixture(problem):
         else:
             assert len(res) == len(want) and res[-1] <= 1e-8
         del ml
+
+
+def test_4096_aniso_precision_form_converges():
+    """The precision form's second problem: rotated anisotropic diffusion
+    (eps 0.001, theta pi/8) on 4096^2, whose values are not exact in FP32 and
+    whose condition number is about 1e10.  The FP32 V-cycle preconditions an
+    FP64 outer CG (the outer A p reads FP64 values here: the FP32 copy of
+    A_0 is a perturbed operator such a problem does not tolerate), and must
+    reach the same 1e-8 true relative residual as the all-FP64 solve in
+    about as many iterations."""
+    rb.init(0)
+    A = rb.par_stencil_grid(rb.diffusion_stencil_2d(0.001, np.pi / 8), [4096, 4096])
+    n = A.global_num_rows
+    b = rb.ParVector(n, values=np.random.default_rng(SEED).uniform(-1.0, 1.0, n))
+    iters = {}
+    for prec in (rb.FP64, rb.FP32):
+        ml = make(A, prec)
+        x = rb.ParVector(n)
+        res = []
+        rc = rb.PCG(A, ml, x, b, res, tol=1e-8, max_iter=300, mode=rb.PCG_TRUE_RESIDUAL)
+        assert rc == 0, (prec, len(res), res[-3:])
+        assert res[-1] <= 1e-8
+        iters[prec] = len(res) - 1
+        del ml
+    assert iters[rb.FP32] <= iters[rb.FP64] + 5, iters

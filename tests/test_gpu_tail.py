@@ -83,3 +83,26 @@ def test_tail_choice_is_timed_and_valid(problem):
     ml = make(A, rb.FP32, rb.L1Jacobi, 1)
     f, ctas = ml.tail_info()
     assert f == -1 or (1 <= f <= ml.num_levels - 2 and ctas >= 8)
+
+
+@pytest.mark.parametrize("prec", [rb.FP64, rb.FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [(36, 36, 36), (150, 150)], ids=["lap27_36", "aniso_150"])
+def test_fused_first_sweep_bit_identical(prec, shape, monkeypatch):
+    """The first sweep fused with the residual (one pass gathering b d) gives
+    the cycle the separate sweep and residual give, bit for bit, on every
+    storage the levels use (diagonals, 32- and 16-bit column indices)."""
+    st = O.laplace_stencil_27pt() if len(shape) == 3 else O.diffusion_stencil_2d(0.001, np.pi / 8)
+    Ao = O.stencil_grid(st, list(shape))
+    n = Ao.shape[0]
+    rp, ci, cv = Ao.arrays()
+    A = rb.ParCSRMatrix.from_arrays(n, n, rp, ci, cv)
+    b = rb.ParVector(n, values=np.random.default_rng(8).uniform(-1, 1, n))
+    got = {}
+    for force in ("0", "1"):
+        monkeypatch.setenv("RAPTOR_B200_FUSE_FIRST", force)
+        ml = make(A, prec, rb.L1Jacobi, 0)
+        assert all(ml.level_fused_first(l) == (force == "1") for l in range(ml.num_levels - 1))
+        x = rb.ParVector(n)
+        ml.cycle(x, b)
+        got[force] = x.numpy()
+    np.testing.assert_array_equal(got["0"], got["1"])
