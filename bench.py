@@ -681,7 +681,8 @@ def run_b200(args, rank, world, local):
                                          for l in range(ml32.num_levels - 1)],
                    "tail": dict(zip(("start_level", "ctas"), ml32.tail_info()),
                                 cycle_ms_by_start=ml32.tail_timings()),
-                   "levels": [ml32.level_info(l) for l in range(ml32.num_levels)]},
+                   "levels": [ml32.level_info(l) for l in range(ml32.num_levels)],
+                   "lanes": [ml32.level_lanes(l) for l in range(ml32.num_levels)]},
         "fp64_form": fp64,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic_for(dom),

@@ -240,7 +240,9 @@ int rb_amg_cycle_profile(rb_amg ml, double* ms, int cap, int* n_out);
 int rb_amg_time_operator(rb_amg ml, int level, int op, int reps, double* ms_per_launch);
 /* Wall time of the last rb_amg_setup (seconds) and the autotuner's choices
  * for level l: lanes per row of A_l (0 when A_l is stored by diagonals),
- * P_l and R_l. */
+ * P_l and R_l (1..32), plus 64 when the operator runs the blocked row
+ * schedule (contiguous rows a block) and 128 when it runs the shared-memory
+ * schedule (x's window staged per chunk of rows). */
 int rb_amg_setup_seconds(rb_amg ml, double* seconds);
 int rb_amg_level_lanes(rb_amg ml, int level, int* lanes_A, int* lanes_P, int* lanes_R);
 /* Storage of A_l in the cycle: *ndiag = number of stored diagonals when the

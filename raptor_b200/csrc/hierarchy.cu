@@ -269,6 +269,80 @@ static void tune_idx16(const CsrView<T>& M, Idx16& I, int G, const T* xin, T* yo
     }
 }
 
+// The shared-memory schedule for M (tiled.cuh): chunks of contiguous rows,
+// one a block, sized so that every chunk's window of x fits a block's shared
+// memory (the chunk count grows from one per SM while it does not); kept when
+// its timed product beats the schedule already picked (G), for 2..32 lanes.
+// Returns the lanes value to use (with kRowsTiled when tiled).
+template <typename T>
+static int tune_tiles(const CsrView<T>& M, Idx16& I, int G, const T* xin, T* yout,
+                      const char* op) {
+    I.tchunks = 0;
+    const char* env = getenv("RAPTOR_B200_TILED");
+    const int force = (env && env[0] == '0') ? 0 : (env && env[0] == '1') ? 1 : -1;
+    if (force == 0 || M.nnz == 0 || (force < 0 && M.n_rows < 4096)) return G;
+    const std::string key = tune_key(op, M.n_rows, M.nnz, (int)sizeof(T));
+    auto& c = tune_cache();
+    auto it = c.m.find(key);
+    if (force < 0 && it != c.m.end() && it->second == 0) return G;
+    const long n = M.n_rows;
+    const int sms = sm_count();
+    int R = 0, nch = 0, wmax = 0;
+    for (int mult = 1; mult <= 8; mult *= 2) {
+        R = (int)std::max<long>(32, (n + (long)sms * mult - 1) / ((long)sms * mult));
+        nch = (int)((n + R - 1) / R);
+        I.tlo.alloc((size_t)nch);
+        I.thi.alloc((size_t)nch);
+        k_row_windows<<<nch, 256, 0, stream()>>>(n, R, M.rowptr, I.on ? nullptr : M.cols,
+                                                 I.on ? I.base.get() : nullptr,
+                                                 I.on ? I.c16.get() : nullptr, I.tlo.get(),
+                                                 I.thi.get());
+        RB_CHECK_LAUNCH();
+        std::vector<int> lo(nch), hi(nch);
+        I.tlo.download(lo.data(), nch);
+        I.thi.download(hi.data(), nch);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        wmax = 0;
+        for (int k = 0; k < nch; k++) wmax = std::max(wmax, hi[k] - lo[k]);
+        if ((long)wmax * (long)sizeof(T) <= kTileSmemBytes) break;
+        wmax = -1;
+    }
+    if (wmax < 0) {
+        I.tlo.release();
+        I.thi.release();
+        if (force < 0) {
+            c.m[key] = 0;
+            tune_save();
+        }
+        return G;
+    }
+    I.tchunks = nch;
+    I.trows = R;
+    I.twmax = wmax;
+    int best = 0;
+    if (force > 0) {
+        best = kRowsTiled | (G & (kRowsBlocked - 1) ? G & (kRowsBlocked - 1) : 8);
+    } else if (it != c.m.end()) {
+        best = it->second;
+    } else {
+        float t_best = time_launch([&] { rows_op(M, I, n, xin, EpiStore<T>{yout}, G); });
+        for (int g : {1, 2, 4, 8, 16, 32}) {
+            const float t = time_launch(
+                [&] { rows_op(M, I, n, xin, EpiStore<T>{yout}, kRowsTiled | g); });
+            if (t < t_best) { t_best = t; best = kRowsTiled | g; }
+        }
+        c.m[key] = best;
+        tune_save();
+    }
+    if (!best) {
+        I.tchunks = 0;
+        I.tlo.release();
+        I.thi.release();
+        return G;
+    }
+    return best;
+}
+
 template <typename T>
 static CsrView<T> make_view(const rb_csr_s& M, DevArray<T>& vals) {
     CsrView<T> v;
@@ -536,8 +610,13 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
             V.gR = autotune_group(V.R, V.r.get(), lv[l + 1].b.get(), "R");
             tune_idx16(V.P, V.P16, V.gP, lv[l + 1].x.get(), V.xt.get(), "P16");
             tune_idx16(V.R, V.R16, V.gR, V.r.get(), lv[l + 1].b.get(), "R16");
+            V.gP = tune_tiles(V.P, V.P16, V.gP, lv[l + 1].x.get(), V.xt.get(), "Ptile");
+            V.gR = tune_tiles(V.R, V.R16, V.gR, V.r.get(), lv[l + 1].b.get(), "Rtile");
         }
-        if (!V.dia) tune_idx16(V.A, V.A16, V.gA, V.x.get(), V.r.get(), "A16");
+        if (!V.dia) {
+            tune_idx16(V.A, V.A16, V.gA, V.x.get(), V.r.get(), "A16");
+            V.gA = tune_tiles(V.A, V.A16, V.gA, V.x.get(), V.r.get(), "Atile");
+        }
     }
     // the first sweep from zero fused with the residual, per level, where
     // one pass over A_l gathering b d beats the sweep and the residual apart

@@ -11,6 +11,7 @@
 #include "dia.cuh"
 #include "rb_internal.cuh"
 #include "tail_cycle.cuh"
+#include "tiled.cuh"
 
 namespace rb {
 
@@ -57,15 +58,34 @@ struct MasterLevel {
 // 16-bit column offsets of a CSR operator whose rows each span fewer than
 // 65536 columns (column = base[row] + c16[j]); used when the autotuner
 // finds it faster than the 32-bit indices.
+// The same record holds the chunk windows of the shared-memory schedule
+// (tiled.cuh) when it is built for the operator.
 struct Idx16 {
     bool on = false;
     DevArray<int> base;
     DevArray<unsigned short> c16;
+    int tchunks = 0, trows = 0, twmax = 0;   // tiles: chunks, rows a chunk, largest window
+    DevArray<int> tlo, thi;
 };
 
-// rows of M times x with the epilogue, through 16- or 32-bit column indices
+// rows of M times x with the epilogue, through 16- or 32-bit column indices,
+// on the strided, blocked (kRowsBlocked) or shared-memory (kRowsTiled)
+// schedule the lanes value G names
 template <typename T, typename TX, class Epi>
 void rows_op(const CsrView<T>& M, const Idx16& I, long n_rows, const TX* x, Epi epi, int G) {
+    if ((G & kRowsTiled) && I.tchunks) {
+        const int g = G & (kRowsBlocked - 1);
+        if (I.on)
+            launch_tiled<T, TX, Epi, true>(n_rows, M.rowptr, M.cols, I.base.get(), I.c16.get(),
+                                           M.vals, x, I.tlo.get(), I.thi.get(), I.trows,
+                                           I.tchunks, I.twmax, epi, g);
+        else
+            launch_tiled<T, TX, Epi, false>(n_rows, M.rowptr, M.cols, nullptr, nullptr, M.vals, x,
+                                            I.tlo.get(), I.thi.get(), I.trows, I.tchunks,
+                                            I.twmax, epi, g);
+        return;
+    }
+    G &= ~kRowsTiled;
     if (I.on) launch_rows16(M.rowptr, I.base.get(), I.c16.get(), M.vals, n_rows, M.nnz, x, epi, G);
     else launch_rows(M.rowptr, M.cols, M.vals, n_rows, M.nnz, x, epi, G);
 }

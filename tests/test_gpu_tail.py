@@ -106,3 +106,32 @@ def test_fused_first_sweep_bit_identical(prec, shape, monkeypatch):
         ml.cycle(x, b)
         got[force] = x.numpy()
     np.testing.assert_array_equal(got["0"], got["1"])
+
+
+@pytest.mark.parametrize("prec", [rb.FP64, rb.FP32], ids=["fp64", "fp32"])
+def test_shared_memory_schedule_bit_identical(prec, monkeypatch):
+    """The coarse operators' shared-memory schedule (x's window staged per
+    chunk of rows, tiled.cuh) sums each row in the order of the strided row
+    kernel, so a cycle and a PCG solve are bit-identical with and without it."""
+    Ao = O.stencil_grid(O.laplace_stencil_27pt(), [48, 48, 48])
+    n = Ao.shape[0]
+    rp, ci, cv = Ao.arrays()
+    A = rb.ParCSRMatrix.from_arrays(n, n, rp, ci, cv)
+    b = rb.ParVector(n, values=np.random.default_rng(9).uniform(-1, 1, n))
+    got, hist = {}, {}
+    for force in ("0", "1"):
+        monkeypatch.setenv("RAPTOR_B200_TILED", force)
+        monkeypatch.setenv("RAPTOR_B200_FUSE_FIRST", "1")
+        ml = make(A, prec, rb.L1Jacobi, 0)
+        lanes = [ml.level_lanes(l) for l in range(ml.num_levels)]
+        tiled = any(v & 128 for lv in lanes for v in lv)
+        assert tiled == (force == "1"), lanes
+        x = rb.ParVector(n)
+        ml.cycle(x, b)
+        got[force] = x.numpy()
+        res = []
+        x = rb.ParVector(n)
+        rb.PCG(A, ml, x, b, res, tol=1e-8, mode=rb.PCG_TRUE_RESIDUAL)
+        hist[force] = np.array(res)
+    np.testing.assert_array_equal(got["0"], got["1"])
+    np.testing.assert_array_equal(hist["0"], hist["1"])
