@@ -607,6 +607,7 @@ def run_b200(args, rank, world, local):
 
     # FP64 form
     fp64 = None
+    xs64 = None
     if not args.no_fp64:
         ml64 = make(rb.FP64)
         t64, iters64, _ = timed(ml64, max(2, args.steps // 2), 2)
@@ -712,7 +713,16 @@ def run_b200(args, rank, world, local):
         out["plain_fp64"] = run_plain_fp64(rb, ev, lambda: rb.lib().rb_synchronize(),
                                            args.plain_size)
     if rank == 0 and args.cpu_sample > 0:
-        out["cpu_baseline"] = cpu_baseline(ml32, bh, args.cpu_sample, S)
+        out["cpu_baseline"], x_ref = cpu_baseline(ml32, bh, args.cpu_sample, S)
+        if x_ref is not None:
+            nref = float(np.linalg.norm(x_ref))
+            fe = {"fp32_form": float(np.linalg.norm(xs32 - x_ref) / nref),
+                  "reference": out["cpu_baseline"]["reference_solution"]["timed_solve_rel_error"],
+                  "x_ref": "the reference's PCG on the same hierarchy and b, true relative "
+                           "residual %.1e" % out["cpu_baseline"]["reference_solution"]["true_rel_res"]}
+            if xs64 is not None:
+                fe["fp64_form"] = float(np.linalg.norm(xs64 - x_ref) / nref)
+            out["final_error_vs_fp64_reference"] = fe
     dist.close()
     if rank == 0:
         print(json.dumps(out))
@@ -783,11 +793,12 @@ class RefSolve:
         self.relres = None
         self.last_rz = None
 
-    def solve(self):
+    def solve(self, tol=None, max_iter=500):
         t0 = time.perf_counter()
-        x, hist = self.O.ref_pcg(self.A, self.ml, np.zeros(len(self.b)), self.b, tol=self.tol,
-                                 max_iter=500)
+        x, hist = self.O.ref_pcg(self.A, self.ml, np.zeros(len(self.b)), self.b,
+                                 tol=self.tol if tol is None else tol, max_iter=max_iter)
         el = time.perf_counter() - t0
+        self.x = x
         self.iters = len(hist) - 1
         self.last_rz = float(hist[-1])
         self.relres = float(np.linalg.norm(self.A.residual(x, self.b)) / self.bnorm)
@@ -812,7 +823,10 @@ def cpu_baseline(ml, bh, m, S):
     built (exported level by level into the reference's ParMultilevel, whose
     duplicate_coarse factors A_c as its setup would), on one core; the CPU
     restatement on an m^3 sample, scaled by rows, where the reference build
-    is absent."""
+    is absent.  Returns (entry, x_ref): x_ref is the reference's FP64
+    solution of the same system taken much further (2.5 times the timed
+    solve's iterations, true relative residual near 1e-15), against which
+    the GPU solutions' final errors are stated (None without the build)."""
     from oracle import oracle as O
     L = O.par_ref()
     if L is None:
@@ -820,7 +834,7 @@ def cpu_baseline(ml, bh, m, S):
         return {"value": el * (S ** 3) / n, "unit": "s", "cores": cores, "kind": "port",
                 "sample": "CPU restatement's AMG-PCG solve on %d^3 (%d rows, %d iterations, "
                           "%.2f s on %d threads), scaled by rows to %d^3 (the reference "
-                          "build is absent)" % (m, n, it, el, cores, S)}
+                          "build is absent)" % (m, n, it, el, cores, S)}, None
     nl = ml.num_levels
     As = [ml.level_matrix(l, "A").arrays() for l in range(nl)]
     Ps = [(ml.level_info(l + 1)[0],) + tuple(ml.level_matrix(l, "P").arrays())
@@ -830,12 +844,20 @@ def cpu_baseline(ml, bh, m, S):
     rs = RefSolve(O, hml.A(0), hml, bh)
     warm = rs.calibrate()
     el = rs.solve()
-    return {"value": el, "unit": "s", "cores": 1, "kind": "reference",
-            "sample": "one %d^3 solve: the reference's own PCG and V-cycle (compiled "
-                      "unmodified, single-rank MPI stand-in, one core; SOR smoother) on the "
-                      "GPU-built hierarchy of %d levels, %d iterations to true relative "
-                      "residual %.2e (PCG tol %.1e after %d calibration solves)"
-                      % (S, nl, rs.iters, rs.relres, rs.tol, warm)}
+    entry = {"value": el, "unit": "s", "cores": 1, "kind": "reference",
+             "sample": "one %d^3 solve: the reference's own PCG and V-cycle (compiled "
+                       "unmodified, single-rank MPI stand-in, one core; SOR smoother) on the "
+                       "GPU-built hierarchy of %d levels, %d iterations to true relative "
+                       "residual %.2e (PCG tol %.1e after %d calibration solves)"
+                       % (S, nl, rs.iters, rs.relres, rs.tol, warm)}
+    x_timed, its, rel_timed = rs.x, rs.iters, rs.relres
+    rs.solve(tol=1e-300, max_iter=int(2.5 * its) + 1)
+    x_ref = rs.x
+    entry["reference_solution"] = {
+        "iters": rs.iters, "true_rel_res": rs.relres,
+        "timed_solve_rel_error": float(np.linalg.norm(x_timed - x_ref) / np.linalg.norm(x_ref)),
+        "timed_solve_rel_res": rel_timed}
+    return entry, x_ref
 
 
 def cpu_sample_solve(m):

@@ -148,7 +148,7 @@ int tune_split(const CsrView<T>& M, int k, const T* xin, T* yout, const char* op
     for (int S = 1; S <= 4 && S * KP <= 32; S <<= 1) {
         const float t = time_launch([&] {
             launch_csr_block(M.rowptr, M.cols, M.vals, M.n_rows, k, xin, BStore<T>{yout}, S);
-        });
+        }, xin, sizeof(T) * (size_t)M.n_cols * (size_t)k);
         if (t < best) { best = t; bestS = S; }
     }
     c.m[key] = bestS;

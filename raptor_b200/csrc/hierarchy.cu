@@ -190,24 +190,14 @@ static int autotune_group_timed(const CsrView<T>& M, T* xin, T* yout) {
     // blocked one
     static const int cands[10] = {1, 2, 4, 8, 16, 32, kRowsBlocked | 4, kRowsBlocked | 8,
                                   kRowsBlocked | 16, kRowsBlocked | 32};
-    cudaEvent_t e0, e1;
-    RB_CUDA(cudaEventCreate(&e0));
-    RB_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     int bestG = pick_group(M.n_rows, M.nnz);
     for (int G : cands) {
-        launch_rows(M.rowptr, M.cols, M.vals, M.n_rows, M.nnz, xin, EpiStore<T>{yout}, G);
-        RB_CUDA(cudaEventRecord(e0, stream()));
-        for (int rep = 0; rep < 3; rep++)
-            launch_rows(M.rowptr, M.cols, M.vals, M.n_rows, M.nnz, xin, EpiStore<T>{yout}, G);
-        RB_CUDA(cudaEventRecord(e1, stream()));
-        RB_CUDA(cudaEventSynchronize(e1));
-        float ms = 0;
-        RB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const float ms = time_launch(
+            [&] { launch_rows(M.rowptr, M.cols, M.vals, M.n_rows, M.nnz, xin, EpiStore<T>{yout}, G); },
+            xin, sizeof(T) * (size_t)M.n_cols);
         if (ms < best) { best = ms; bestG = G; }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     return bestG;
 }
 
@@ -250,13 +240,14 @@ static void tune_idx16(const CsrView<T>& M, Idx16& I, int G, const T* xin, T* yo
     } else if (it != c.m.end()) {
         use = it->second != 0;
     } else {
+        const size_t xb = sizeof(T) * (size_t)M.n_cols;
         const float t32 = time_launch([&] {
             launch_rows(M.rowptr, M.cols, M.vals, M.n_rows, M.nnz, xin, EpiStore<T>{yout}, G);
-        });
+        }, xin, xb);
         const float t16 = time_launch([&] {
             launch_rows16(M.rowptr, I.base.get(), I.c16.get(), M.vals, M.n_rows, M.nnz, xin,
                           EpiStore<T>{yout}, G);
-        });
+        }, xin, xb);
         use = t16 < t32;
         c.m[key] = use ? 1 : 0;
         tune_save();
@@ -325,10 +316,11 @@ static int tune_tiles(const CsrView<T>& M, Idx16& I, int G, const T* xin, T* you
     } else if (it != c.m.end()) {
         best = it->second;
     } else {
-        float t_best = time_launch([&] { rows_op(M, I, n, xin, EpiStore<T>{yout}, G); });
+        const size_t xb = sizeof(T) * (size_t)M.n_cols;
+        float t_best = time_launch([&] { rows_op(M, I, n, xin, EpiStore<T>{yout}, G); }, xin, xb);
         for (int g : {1, 2, 4, 8, 16, 32}) {
             const float t = time_launch(
-                [&] { rows_op(M, I, n, xin, EpiStore<T>{yout}, kRowsTiled | g); });
+                [&] { rows_op(M, I, n, xin, EpiStore<T>{yout}, kRowsTiled | g); }, xin, xb);
             if (t < t_best) { t_best = t; best = kRowsTiled | g; }
         }
         c.m[key] = best;
@@ -592,13 +584,14 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
             if (it != c.m.end()) {
                 V.dia = it->second != 0;
             } else {
+                const size_t xb = sizeof(T) * (size_t)V.n;
                 const float t_csr = time_launch([&] {
                     launch_rows(V.A.rowptr, V.A.cols, V.A.vals, V.n, V.A.nnz, V.x.get(),
                                 EpiStore<T>{V.r.get()}, V.gA);
-                });
+                }, V.x.get(), xb);
                 const float t_dia = time_launch([&] {
                     launch_dia(V.off, V.Adia.get(), V.n, V.x.get(), EpiStore<T>{V.r.get()});
-                });
+                }, V.x.get(), xb);
                 V.dia = t_dia < t_csr;
                 c.m[key] = V.dia ? 1 : 0;
                 tune_save();
@@ -645,10 +638,10 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
                                                                           V.dinv.get(), V.x.get());
             RB_CHECK_LAUNCH();
             V.apply_A(V.x.get(), EpiResidual<T, T>{V.b.get(), V.r.get()});
-        });
+        }, V.b.get(), sizeof(T) * (size_t)V.n);
         const float t_fused = time_launch([&] {
             V.apply_A(V.b.get(), EpiFirstResidual<T>{V.b.get(), V.dinv.get(), V.r.get(), V.x.get()});
-        });
+        }, V.b.get(), sizeof(T) * (size_t)V.n);
         V.fuse_first = t_fused < t_sep;
         c.m[key] = V.fuse_first ? 1 : 0;
         tune_save();
