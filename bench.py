@@ -449,6 +449,10 @@ def run_uneven_batch(rb, ev, sync, count=64, steps=2):
             seq.append(e0.elapsed_time(e1))
     seq_ms = sum(seq) / len(seq)
     sides = [p[0] for p in params]
+    rows = [int(B.offsets[s + 1]) - int(B.offsets[s]) for s in range(count)]
+    # the row work the systems need (each its own iterations) against running
+    # every system for the slowest one's iterations
+    need = sum(int(i) * r for i, r in zip(iters, rows)) / (max(int(i) for i in iters) * N)
     return {"workload": "%d rotated-diffusion systems, side log-uniform [64, 1024], eps "
                         "log-uniform [1e-3, 1], theta uniform [0, pi]; RS PMIS extended+i "
                         "L1-Jacobi, FP32 V-cycle, FP64 outer CG per system to 1e-8" % count,
@@ -456,6 +460,9 @@ def run_uneven_batch(rb, ev, sync, count=64, steps=2):
             "packed_levels": int(max(B.levels)), "setup_s": setup_s, "status": rc,
             "batch_ms": batch_ms, "sequential_ms": seq_ms, "speedup_vs_sequential": seq_ms / batch_ms,
             "iters_max": int(max(iters)), "iters_min": int(min(iters)),
+            "row_iterations_needed_vs_all_to_max": need,
+            "stopped_systems": "skipped by the row gates (each system's rows leave the cycle "
+                               "and the outer iteration once it has converged)",
             "max_true_rel_res": float(max(relres))}
 
 

@@ -58,11 +58,14 @@ __global__ void k_fill_rowptr(int n, long row0, int value, int* prp) {
 }
 
 // Dense solve of each listed system's coarsest level (one CTA per system).
+// sys / active (optional): a listed system that has stopped is skipped.
 template <typename T>
 __global__ void k_lu_solve_batch(const int* __restrict__ row0, const int* __restrict__ nrow,
                                  const long long* __restrict__ luo, const int* __restrict__ pivo,
                                  const double* __restrict__ lu_all, const int* __restrict__ piv_all,
-                                 const T* __restrict__ b, T* __restrict__ x) {
+                                 const T* __restrict__ b, T* __restrict__ x,
+                                 const int* __restrict__ sys, const int* __restrict__ active) {
+    if (active && !active[sys[blockIdx.x]]) return;
     extern __shared__ double y[];
     const int n = nrow[blockIdx.x];
     const long r0 = row0[blockIdx.x];
@@ -96,7 +99,9 @@ __global__ void k_lu_solve_batch(const int* __restrict__ row0, const int* __rest
 template <typename T>
 __global__ void k_coarse_mv_batch(const int* __restrict__ row0, const int* __restrict__ nrow,
                                   const long long* __restrict__ ioff, const double* __restrict__ inv_all,
-                                  const T* __restrict__ b, T* __restrict__ x) {
+                                  const T* __restrict__ b, T* __restrict__ x,
+                                  const int* __restrict__ sys, const int* __restrict__ active) {
+    if (active && !active[sys[blockIdx.x]]) return;
     extern __shared__ double bs[];
     const int n = nrow[blockIdx.x];
     const long r0 = row0[blockIdx.x];
@@ -114,12 +119,18 @@ __global__ void k_coarse_mv_batch(const int* __restrict__ row0, const int* __res
 // system sums that system's chunks in order.  Deterministic.
 // gate (optional): the pass runs only when *gate is nonzero (a step of the
 // device-side loop that some iterations skip)
+// csys / active (optional): a chunk of a stopped system writes 0 unread.
 __global__ void __launch_bounds__(256)
 k_seg_partial(const int* __restrict__ lo, const int* __restrict__ hi, const double* __restrict__ a,
-              const double* __restrict__ b, double* part, const int* gate) {
+              const double* __restrict__ b, double* part, const int* gate,
+              const int* __restrict__ csys, const int* __restrict__ active) {
     if (gate && *(volatile const int*)gate == 0) return;
     __shared__ double w[8];
     const int c = blockIdx.x;
+    if (active && !active[csys[c]]) {
+        if (threadIdx.x == 0) part[c] = 0.0;
+        return;
+    }
     double t = 0.0;
     for (int i = lo[c] + threadIdx.x; i < hi[c]; i += blockDim.x) t += a[i] * b[i];
     t = warp_sum(t);
@@ -175,20 +186,78 @@ struct FinSTmp {
     __device__ void operator()(int s, double t) const { S.tmp[s] = t; }
 };
 
+// active (optional): rows of stopped systems are left as they are (their
+// alpha and beta are 0, so the update would not change x or r either)
 __global__ void k_seg_update(long n, const int* __restrict__ seg, double* __restrict__ x,
                              double* __restrict__ r, const double* __restrict__ p,
-                             const double* __restrict__ Ap, const double* __restrict__ alpha) {
+                             const double* __restrict__ Ap, const double* __restrict__ alpha,
+                             const int* __restrict__ active) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (active && !active[seg[i]]) return;
     const double a = alpha[seg[i]];
     x[i] += p[i] * a;
     r[i] = r[i] + Ap[i] * (-1.0 * a);
 }
 
 __global__ void k_seg_p(long n, const int* __restrict__ seg, double* __restrict__ p,
-                        const double* __restrict__ z, const double* __restrict__ beta) {
+                        const double* __restrict__ z, const double* __restrict__ beta,
+                        const int* __restrict__ active) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = p[i] * beta[seg[i]] + z[i];
+    if (i >= n || (active && !active[seg[i]])) return;
+    p[i] = p[i] * beta[seg[i]] + z[i];
+}
+
+// The row gates of the packed levels: closed[c] = 1 when every system with
+// rows in [c 256, (c + 1) 256) of the level has stopped.  Flat over the
+// levels (level l owns chunks cbase[l] .. cbase[l + 1] - 1; offs holds the
+// level's n_sys + 1 row offsets at l (n_sys + 1)).
+__global__ void k_gate_refresh(int L, int n_sys, const long long* __restrict__ offs,
+                               const long long* __restrict__ cbase,
+                               const int* __restrict__ active, unsigned char* __restrict__ closed) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cbase[L]) return;
+    int l = 0;
+    while (c >= cbase[l + 1]) l++;
+    const long long* off = offs + (size_t)l * (n_sys + 1);
+    const long long r0 = (c - cbase[l]) << kGateShift;
+    const long long r1 = min(r0 + (1LL << kGateShift), off[n_sys]);
+    // the last system whose first row is at or before r0
+    int lo = 0, hi = n_sys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= r0) lo = mid;
+        else hi = mid - 1;
+    }
+    unsigned char shut = 1;
+    for (int q = lo; q < n_sys && off[q] < r1; q++)
+        if (off[q + 1] > r0 && active[q]) {
+            shut = 0;
+            break;
+        }
+    closed[c] = shut;
+}
+
+template <typename TO, typename TI>
+__global__ void k_convert_gated(long n, const TI* __restrict__ in, TO* __restrict__ out,
+                                const unsigned char* __restrict__ closed) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !closed[i >> kGateShift]) out[i] = (TO)in[i];
+}
+
+// x = dinv .* b (k_scale_first) on the open rows
+template <typename T>
+__global__ void k_scale_first_gated(long n, const T* __restrict__ b, const T* __restrict__ dinv,
+                                    T* __restrict__ x, const unsigned char* __restrict__ closed) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !closed[i >> kGateShift]) x[i] = (T)(b[i] * dinv[i]);
+}
+
+// e, restricted to the open rows when Gt
+template <bool Gt, class Epi>
+auto gated(const Epi& e, const unsigned char* closed) {
+    if constexpr (Gt) return row_gate(e, closed);
+    else return e;
 }
 
 __global__ void k_seg_ids(int n_sys, const long long* __restrict__ off, int* seg) {
@@ -216,9 +285,9 @@ struct BatchCtl {
 
 __global__ void k_seg_p_dev(long n, const int* __restrict__ seg, double* __restrict__ p,
                             const double* __restrict__ z, const double* __restrict__ beta,
-                            const BatchCtl* c) {
+                            const BatchCtl* c, const int* __restrict__ active) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || c->pmode == 0) return;
+    if (i >= n || c->pmode == 0 || !active[seg[i]]) return;
     p[i] = p[i] * beta[seg[i]] + z[i];
 }
 
@@ -284,7 +353,7 @@ struct Batch {
     DevArray<int> piv;
     struct CoarseTab {
         int count = 0, max_n = 0;
-        DevArray<int> row0, n, pivo;
+        DevArray<int> row0, n, pivo, sys;
         DevArray<long long> luo;
     };
     std::vector<CoarseTab> coarse;
@@ -303,16 +372,38 @@ struct Batch {
     DevArray<double> bnorm_d, relres_d;
     DevArray<int> cand_d, iters_d;
     int host_waits = 0;   // host waits of the last pcg (one per graph launch)
+    // Row gates of the packed levels (one byte per 256 rows, kGateShift):
+    // inside pcg every operation of the cycle and of the outer iteration
+    // passes over the rows of systems that have stopped, so an iteration
+    // costs the rows of the systems still running, not of all of them.
+    // Systems are independent (every packed operator is block-diagonal), so
+    // a skipped row changes no other system's result.
+    DevArray<unsigned char> gates;
+    std::vector<long long> gate_base;   // first byte of each level
+    DevArray<long long> gate_offs, gate_cbase;
+    DevArray<int> chunk_sys;            // system of each reduction chunk
+    bool gating = false;                // set while pcg builds its launches
+    const unsigned char* gate(int l) const { return gates.get() + gate_base[l]; }
+    void refresh_gates() {
+        const long long total = gate_base.back();
+        if (!total) return;
+        k_gate_refresh<<<grid_for(total, 256), 256, 0, stream()>>>(
+            (int)off.size(), n_sys, gate_offs.get(), gate_cbase.get(), S.active, gates.get());
+        RB_CHECK_LAUNCH();
+    }
     ~Batch() {
         if (h_ctl) cudaFreeHost(h_ctl);
     }
 
     long long rows() const { return off[0][n_sys]; }
 
+    // skip_stopped: chunks of systems that have stopped contribute 0
     template <class Fin>
-    void seg_dot(const double* a, const double* b, Fin fin, const int* gate = nullptr) {
+    void seg_dot(const double* a, const double* b, Fin fin, const int* gate = nullptr,
+                 bool skip_stopped = true) {
         k_seg_partial<<<n_chunks, 256, 0, stream()>>>(chunk_lo.get(), chunk_hi.get(), a, b,
-                                                      part.get(), gate);
+                                                      part.get(), gate, chunk_sys.get(),
+                                                      gating && skip_stopped ? S.active : nullptr);
         RB_CHECK_LAUNCH();
         k_seg_finish<<<grid_for(n_sys, 128), 128, 0, stream()>>>(n_sys, chunk0.get(), part.get(),
                                                                   fin, gate);
@@ -323,17 +414,19 @@ struct Batch {
     void coarse_solve(int l, const T* b, T* x) {
         CoarseTab& t = coarse[l];
         if (!t.count) return;
+        const int* act = gating ? S.active : nullptr;
         if (inv.get())
             k_coarse_mv_batch<T><<<t.count, 256, sizeof(double) * std::max(t.max_n, 1), stream()>>>(
-                t.row0.get(), t.n.get(), t.luo.get(), inv.get(), b, x);
+                t.row0.get(), t.n.get(), t.luo.get(), inv.get(), b, x, t.sys.get(), act);
         else
             k_lu_solve_batch<T><<<t.count, 256, sizeof(double) * std::max(t.max_n, 1), stream()>>>(
-                t.row0.get(), t.n.get(), t.luo.get(), t.pivo.get(), lu.get(), piv.get(), b, x);
+                t.row0.get(), t.n.get(), t.luo.get(), t.pivo.get(), lu.get(), piv.get(), b, x,
+                t.sys.get(), act);
         RB_CHECK_LAUNCH();
     }
 
     void setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o);
-    template <typename T>
+    template <bool Gt, typename T>
     void cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool x_zero);
     void cycle64(double* x, const double* b);
     int pcg(double* x, const double* b, double tol, int max_iter, int* iters, double* relres);
@@ -465,13 +558,14 @@ void Batch::setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o) {
     coarse.clear();
     coarse.resize(Lmax);
     for (int l = 0; l < Lmax; l++) {
-        std::vector<int> r0, nr, pv;
+        std::vector<int> r0, nr, pv, sy;
         std::vector<long long> lo;
         int mx = 0;
         for (int s = 0; s < n; s++) {
             if (depth[s] - 1 != l) continue;
             const int nc = (int)(off[l][s + 1] - off[l][s]);
             if (!nc) continue;
+            sy.push_back(s);
             r0.push_back((int)off[l][s]);
             nr.push_back(nc);
             lo.push_back(luo[s]);
@@ -486,14 +580,40 @@ void Batch::setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o) {
             t.n.alloc(t.count); t.n.upload(nr.data(), t.count);
             t.luo.alloc(t.count); t.luo.upload(lo.data(), t.count);
             t.pivo.alloc(t.count); t.pivo.upload(pv.data(), t.count);
+            t.sys.alloc(t.count); t.sys.upload(sy.data(), t.count);
         }
     }
     RB_CUDA(cudaStreamSynchronize(stream()));
     sys.clear();
     // cycle data of the packed levels (value copies, inverse diagonals,
     // colourings, kernel widths)
+    cat.strided_only = true;
     if (o.precision == RB_PREC_FP32) cat.build_levels(cat.lv32);
     else cat.build_levels(cat.lv64);
+    auto zero_levels = [](auto& lv) {
+        for (auto& V : lv) {
+            V.x.zero();
+            V.b.zero();
+            V.r.zero();
+            V.xt.zero();
+        }
+    };
+    if (o.precision == RB_PREC_FP32) zero_levels(cat.lv32);
+    else zero_levels(cat.lv64);
+    // row gates: one byte per 256 rows of every packed level
+    gate_base.assign(Lmax + 1, 0);
+    for (int l = 0; l < Lmax; l++)
+        gate_base[l + 1] = gate_base[l] + ((off[l][n] + (1 << kGateShift) - 1) >> kGateShift);
+    gates.alloc((size_t)std::max<long long>(gate_base[Lmax], 1));
+    gates.zero();
+    {
+        std::vector<long long> flat;
+        for (int l = 0; l < Lmax; l++) flat.insert(flat.end(), off[l].begin(), off[l].end());
+        gate_offs.alloc(flat.size());
+        gate_offs.upload(flat.data(), flat.size());
+        gate_cbase.alloc(gate_base.size());
+        gate_cbase.upload(gate_base.data(), gate_base.size());
+    }
     // outer CG: segments and chunks of the finest level
     const long long N = off[0][n];
     std::vector<int> clo, chi, c0(n + 1, 0);
@@ -510,6 +630,13 @@ void Batch::setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o) {
     chunk_lo.alloc(clo.size()); chunk_lo.upload(clo.data(), clo.size());
     chunk_hi.alloc(chi.size()); chunk_hi.upload(chi.data(), chi.size());
     chunk0.alloc(c0.size()); chunk0.upload(c0.data(), c0.size());
+    {
+        std::vector<int> cs(std::max<size_t>(clo.size(), 1), 0);
+        for (int s = 0; s < n; s++)
+            for (int c = c0[s]; c < c0[s + 1]; c++) cs[c] = s;
+        chunk_sys.alloc(cs.size());
+        chunk_sys.upload(cs.data(), cs.size());
+    }
     part.alloc((size_t)n_chunks);
     seg.alloc((size_t)std::max<long long>(N, 1));
     DevArray<long long> offd((size_t)n + 1);
@@ -518,6 +645,7 @@ void Batch::setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o) {
     RB_CHECK_LAUNCH();
     const size_t m = (size_t)std::max<long long>(N, 1);
     r.alloc(m); z.alloc(m); p.alloc(m); Ap.alloc(m); rt.alloc(m);
+    r.zero(); z.zero(); p.zero(); Ap.zero(); rt.zero();
     sc.alloc((size_t)6 * n);
     si.alloc((size_t)n + 1);
     S = SegScal{sc.get(), sc.get() + n, sc.get() + 2 * n, sc.get() + 3 * n, sc.get() + 4 * n,
@@ -529,8 +657,10 @@ void Batch::setup(int n, const rb_csr_s* const* mats, const rb_amg_opts& o) {
 }
 
 // ParMultilevel::cycle on the packed levels, plus the dense solve of the
-// systems whose coarsest level is l.
-template <typename T>
+// systems whose coarsest level is l.  Gt: the rows of systems that have
+// stopped are passed over (the row gates; Jacobi-type smoothing only, the
+// multicolour sweeps run every row).
+template <bool Gt, typename T>
 void Batch::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool x_zero) {
     const int L = (int)lv.size();
     if (l == L - 1) {
@@ -539,26 +669,43 @@ void Batch::cycle_level(std::vector<Level<T>>& lv, int l, T* x, const T* b, bool
     }
     Level<T>& V = lv[l];
     Level<T>& C = lv[l + 1];
-    T* cur = x;
-    T* other = V.xt.get();
-    cat.smooth(V, cur, other, b, x_zero);
-    V.apply_A(cur, EpiResidual<T, T>{b, V.r.get()});
-    rows_op(V.R, V.R16, C.n, V.r.get(), EpiStore<T>{C.b.get()},
-                V.gR);
-    cycle_level(lv, l + 1, C.x.get(), C.b.get(), true);
+    const unsigned char* gl = Gt ? gate(l) : nullptr;
+    const unsigned char* gc = Gt ? gate(l + 1) : nullptr;
     const int rt = opts.relax_type;
     const bool jt = (rt == RB_RELAX_JACOBI && !opts.jacobi_compat) || rt == RB_RELAX_L1JACOBI;
+    auto smooth = [&](T*& cur, T*& other, bool xz) {
+        if (!Gt || !jt || opts.num_smooth_sweeps <= 0) {
+            cat.smooth(V, cur, other, b, xz);
+            return;
+        }
+        // Hierarchy::smooth's Jacobi-type sweeps on the open rows
+        for (int s = 0; s < opts.num_smooth_sweeps; s++) {
+            if (s == 0 && xz) {
+                k_scale_first_gated<T><<<grid_for(V.n, 256), 256, 0, stream()>>>(
+                    V.n, b, V.dinv.get(), cur, gl);
+                RB_CHECK_LAUNCH();
+                continue;
+            }
+            V.apply_A(cur, gated<Gt>(EpiJacobi<T, T, T>{cur, b, V.dinv.get(), other}, gl));
+            std::swap(cur, other);
+        }
+    };
+    T* cur = x;
+    T* other = V.xt.get();
+    smooth(cur, other, x_zero);
+    V.apply_A(cur, gated<Gt>(EpiResidual<T, T>{b, V.r.get()}, gl));
+    rows_op(V.R, V.R16, C.n, V.r.get(), gated<Gt>(EpiStore<T>{C.b.get()}, gc), V.gR);
+    cycle_level<Gt>(lv, l + 1, C.x.get(), C.b.get(), true);
     T* start = x;
     if (jt && (opts.num_smooth_sweeps & 1)) start = (x == V.xt.get()) ? x : V.xt.get();
     if (cur == start) {
-        rows_op(V.P, V.P16, V.n, C.x.get(), EpiAppend<T>{cur}, V.gP);
+        rows_op(V.P, V.P16, V.n, C.x.get(), gated<Gt>(EpiAppend<T>{cur}, gl), V.gP);
     } else {
-        rows_op(V.P, V.P16, V.n, C.x.get(),
-                    EpiAddTo<T>{cur, start}, V.gP);
+        rows_op(V.P, V.P16, V.n, C.x.get(), gated<Gt>(EpiAddTo<T>{cur, start}, gl), V.gP);
         cur = start;
     }
     other = (cur == x) ? V.xt.get() : x;
-    cat.smooth(V, cur, other, b, false);
+    smooth(cur, other, false);
     if (cur != x)
         RB_CUDA(cudaMemcpyAsync(x, cur, sizeof(T) * V.n, cudaMemcpyDeviceToDevice, stream()));
     // systems whose hierarchy ends here: the direct solve replaces the sweeps
@@ -569,13 +716,25 @@ void Batch::cycle64(double* x, const double* b) {
     if (opts.precision == RB_PREC_FP32) {
         Level<float>& V = cat.lv32[0];
         const long n = V.n;
+        if (gating) {
+            k_convert_gated<float, double><<<grid_for(n, 256), 256, 0, stream()>>>(n, b, V.b.get(),
+                                                                                  gate(0));
+            RB_CHECK_LAUNCH();
+            cycle_level<true>(cat.lv32, 0, V.x.get(), V.b.get(), true);
+            k_convert_gated<double, float><<<grid_for(n, 256), 256, 0, stream()>>>(n, V.x.get(), x,
+                                                                                  gate(0));
+            RB_CHECK_LAUNCH();
+            return;
+        }
         k_convert<float, double><<<grid_for(n, 256), 256, 0, stream()>>>(n, b, V.b.get());
         RB_CHECK_LAUNCH();
-        cycle_level(cat.lv32, 0, V.x.get(), V.b.get(), true);
+        cycle_level<false>(cat.lv32, 0, V.x.get(), V.b.get(), true);
         k_convert<double, float><<<grid_for(n, 256), 256, 0, stream()>>>(n, V.x.get(), x);
         RB_CHECK_LAUNCH();
+    } else if (gating) {
+        cycle_level<true>(cat.lv64, 0, x, b, true);
     } else {
-        cycle_level(cat.lv64, 0, x, b, true);
+        cycle_level<false>(cat.lv64, 0, x, b, true);
     }
 }
 
@@ -583,6 +742,11 @@ void Batch::cycle64(double* x, const double* b) {
 // b - A x every 10 iterations, a system stops once its true relative
 // residual meets tol; stopped systems keep alpha = beta = 0.
 int Batch::pcg(double* x, const double* b, double tol, int max_iter, int* iters, double* relres) {
+    struct GatingOn {
+        bool& g;
+        explicit GatingOn(bool& f) : g(f) { g = true; }
+        ~GatingOn() { g = false; }
+    } gating_on(gating);
     const rb_csr_s& A = *cat.master[0].A;
     const long N = A.n_rows;
     const int n = n_sys;
@@ -596,10 +760,11 @@ int Batch::pcg(double* x, const double* b, double tol, int max_iter, int* iters,
     auto push_active = [&]() {
         RB_CUDA(cudaMemcpyAsync(S.active, h_active.data(), sizeof(int) * n, cudaMemcpyHostToDevice,
                                 stream()));
+        refresh_gates();
     };
     RB_CUDA(cudaMemsetAsync(sc.get(), 0, sizeof(double) * 6 * n, stream()));
     RB_CUDA(cudaMemsetAsync(si.get(), 0, sizeof(int) * (n + 1), stream()));
-    seg_dot(b, b, FinSTmp{S});
+    seg_dot(b, b, FinSTmp{S}, nullptr, false);
     read(h_tmp, S.tmp);
     std::vector<double> bnorm(n);
     for (int s = 0; s < n; s++) {
@@ -654,13 +819,16 @@ int Batch::pcg(double* x, const double* b, double tol, int max_iter, int* iters,
     host_waits = 0;
     if (cat.use_graphs) return pcg_device_loop(x, b, tol, max_iter, iters, relres, bnorm, restart);
     auto body = [&](bool full_r) {
-        launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, p.get(), EpiStore<double>{Ap.get()},
-                    cat.gA0 > 0 ? cat.gA0 : 0);
+        launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, p.get(),
+                    row_gate(EpiStore<double>{Ap.get()}, gate(0)), cat.gA0 > 0 ? cat.gA0 : 0);
         seg_dot(p.get(), Ap.get(), FinSPAp{S});
         k_seg_update<<<grid_for(N, 256), 256, 0, stream()>>>(N, seg.get(), x, r.get(), p.get(),
-                                                             Ap.get(), S.alpha);
+                                                             Ap.get(), S.alpha, S.active);
         RB_CHECK_LAUNCH();
-        if (full_r) residual64(Av, x, b, r.get());
+        if (full_r)
+            launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, x,
+                        row_gate(EpiResidual<double, double>{b, r.get()}, gate(0)),
+                        cat.gA0 > 0 ? cat.gA0 : 0);
         seg_dot(r.get(), r.get(), FinSRR{S});
         cycle64(z.get(), r.get());
         seg_dot(r.get(), z.get(), FinSRZ{S});
@@ -678,7 +846,8 @@ int Batch::pcg(double* x, const double* b, double tol, int max_iter, int* iters,
         RB_CUDA(cudaStreamSynchronize(stream()));
         if (h_break) return RB_ERR_BREAKDOWN;
         if (check()) { status = RB_OK; break; }
-        k_seg_p<<<grid_for(N, 256), 256, 0, stream()>>>(N, seg.get(), p.get(), z.get(), S.beta);
+        k_seg_p<<<grid_for(N, 256), 256, 0, stream()>>>(N, seg.get(), p.get(), z.get(), S.beta,
+                                                        S.active);
         RB_CHECK_LAUNCH();
     }
     if (status != RB_OK)
@@ -725,16 +894,16 @@ int Batch::pcg_device_loop(double* x, const double* b, double tol, int max_iter,
     const unsigned sg = grid_for(n, 128);
     auto iteration = [&](cudaGraphConditionalHandle h) {
         k_seg_p_dev<<<grid_for(N, 256), 256, 0, stream()>>>(N, seg.get(), p.get(), z.get(),
-                                                            S.beta, C);
+                                                            S.beta, C, S.active);
         RB_CHECK_LAUNCH();
-        launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, p.get(), EpiStore<double>{Ap.get()},
-                    cat.gA0 > 0 ? cat.gA0 : 0);
+        launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, p.get(),
+                    row_gate(EpiStore<double>{Ap.get()}, gate(0)), cat.gA0 > 0 ? cat.gA0 : 0);
         seg_dot(p.get(), Ap.get(), FinSPAp{S});
         k_seg_update<<<grid_for(N, 256), 256, 0, stream()>>>(N, seg.get(), x, r.get(), p.get(),
-                                                             Ap.get(), S.alpha);
+                                                             Ap.get(), S.alpha, S.active);
         RB_CHECK_LAUNCH();
         launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, x,
-                    EpiResidualIf<double, double>{b, r.get(), &C->full},
+                    row_gate(EpiResidualIf<double, double>{b, r.get(), &C->full}, gate(0)),
                     cat.gA0 > 0 ? cat.gA0 : 0);
         seg_dot(r.get(), r.get(), FinSRR{S});
         cycle64(z.get(), r.get());
@@ -742,12 +911,13 @@ int Batch::pcg_device_loop(double* x, const double* b, double tol, int max_iter,
         k_batch_candidates<<<sg, 128, 0, stream()>>>(n, S, bnorm_d.get(), cand_d.get(), C);
         RB_CHECK_LAUNCH();
         launch_rows(Av.rowptr, Av.cols, Av.vals, N, Av.nnz, x,
-                    EpiResidualIf<double, double>{b, rt.get(), &C->confirm},
+                    row_gate(EpiResidualIf<double, double>{b, rt.get(), &C->confirm}, gate(0)),
                     cat.gA0 > 0 ? cat.gA0 : 0);
         seg_dot(rt.get(), rt.get(), FinSTmp{S}, &C->confirm);
         k_batch_confirm<<<sg, 128, 0, stream()>>>(n, S, bnorm_d.get(), cand_d.get(),
                                                   iters_d.get(), relres_d.get(), C);
         RB_CHECK_LAUNCH();
+        refresh_gates();
         k_batch_step_end<<<1, kStepEndThreads, 0, stream()>>>(n, S, C, h);
         RB_CHECK_LAUNCH();
     };

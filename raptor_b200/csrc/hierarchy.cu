@@ -169,30 +169,34 @@ std::string tune_key(const char* op, long n, long long nnz, int vbytes) {
 
 // Time the row kernel for each group width and keep the fastest.
 template <typename T>
-static int autotune_group_timed(const CsrView<T>& M, T* xin, T* yout);
+static int autotune_group_timed(const CsrView<T>& M, T* xin, T* yout, bool strided);
 
+// strided: the strided schedule's widths only (the levels of a batch)
 template <typename T>
-static int autotune_group(const CsrView<T>& M, T* xin, T* yout, const char* op = "rows") {
+static int autotune_group(const CsrView<T>& M, T* xin, T* yout, const char* op = "rows",
+                          bool strided = false) {
     if (M.n_rows < 4096) return pick_group(M.n_rows, M.nnz);
-    const std::string key = tune_key(op, M.n_rows, M.nnz, (int)sizeof(T));
+    const std::string key = tune_key((strided ? std::string("s") + op : std::string(op)).c_str(),
+                                     M.n_rows, M.nnz, (int)sizeof(T));
     auto& c = tune_cache();
     auto it = c.m.find(key);
     if (it != c.m.end()) return it->second;
-    const int G = autotune_group_timed(M, xin, yout);
+    const int G = autotune_group_timed(M, xin, yout, strided);
     c.m[key] = G;
     tune_save();
     return G;
 }
 
 template <typename T>
-static int autotune_group_timed(const CsrView<T>& M, T* xin, T* yout) {
+static int autotune_group_timed(const CsrView<T>& M, T* xin, T* yout, bool strided) {
     // lanes per row on the strided schedule, then (kRowsBlocked) on the
     // blocked one
     static const int cands[10] = {1, 2, 4, 8, 16, 32, kRowsBlocked | 4, kRowsBlocked | 8,
                                   kRowsBlocked | 16, kRowsBlocked | 32};
     float best = 1e30f;
     int bestG = pick_group(M.n_rows, M.nnz);
-    for (int G : cands) {
+    for (int k = 0; k < (strided ? 6 : 10); k++) {
+        const int G = cands[k];
         const float ms = time_launch(
             [&] { launch_rows(M.rowptr, M.cols, M.vals, M.n_rows, M.nnz, xin, EpiStore<T>{yout}, G); },
             xin, sizeof(T) * (size_t)M.n_cols);
@@ -574,8 +578,8 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
     // storage of A_l (CSR or diagonals) by timing both
     for (int l = 0; l < L; l++) {
         Level<T>& V = lv[l];
-        V.gA = autotune_group(V.A, V.x.get(), V.r.get(), "A");
-        const DiaOff off = find_diagonals(*master[l].A);
+        V.gA = autotune_group(V.A, V.x.get(), V.r.get(), "A", strided_only);
+        const DiaOff off = strided_only ? DiaOff{} : find_diagonals(*master[l].A);
         if (off.nd > 0) {
             build_dia(V, *master[l].A, off);
             const std::string key = tune_key("A_dia", V.n, V.A.nnz, (int)sizeof(T));
@@ -599,16 +603,18 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
             if (!V.dia) V.Adia.release();
         }
         if (l < L - 1) {
-            V.gP = autotune_group(V.P, lv[l + 1].x.get(), V.xt.get(), "P");
-            V.gR = autotune_group(V.R, V.r.get(), lv[l + 1].b.get(), "R");
-            tune_idx16(V.P, V.P16, V.gP, lv[l + 1].x.get(), V.xt.get(), "P16");
-            tune_idx16(V.R, V.R16, V.gR, V.r.get(), lv[l + 1].b.get(), "R16");
-            V.gP = tune_tiles(V.P, V.P16, V.gP, lv[l + 1].x.get(), V.xt.get(), "Ptile");
-            V.gR = tune_tiles(V.R, V.R16, V.gR, V.r.get(), lv[l + 1].b.get(), "Rtile");
+            V.gP = autotune_group(V.P, lv[l + 1].x.get(), V.xt.get(), "P", strided_only);
+            V.gR = autotune_group(V.R, V.r.get(), lv[l + 1].b.get(), "R", strided_only);
+            tune_idx16(V.P, V.P16, V.gP, lv[l + 1].x.get(), V.xt.get(), strided_only ? "sP16" : "P16");
+            tune_idx16(V.R, V.R16, V.gR, V.r.get(), lv[l + 1].b.get(), strided_only ? "sR16" : "R16");
+            if (!strided_only) {
+                V.gP = tune_tiles(V.P, V.P16, V.gP, lv[l + 1].x.get(), V.xt.get(), "Ptile");
+                V.gR = tune_tiles(V.R, V.R16, V.gR, V.r.get(), lv[l + 1].b.get(), "Rtile");
+            }
         }
         if (!V.dia) {
-            tune_idx16(V.A, V.A16, V.gA, V.x.get(), V.r.get(), "A16");
-            V.gA = tune_tiles(V.A, V.A16, V.gA, V.x.get(), V.r.get(), "Atile");
+            tune_idx16(V.A, V.A16, V.gA, V.x.get(), V.r.get(), strided_only ? "sA16" : "A16");
+            if (!strided_only) V.gA = tune_tiles(V.A, V.A16, V.gA, V.x.get(), V.r.get(), "Atile");
         }
     }
     // the first sweep from zero fused with the residual, per level, where
@@ -619,7 +625,7 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
     // RAPTOR_B200_FUSE_FIRST=0 never fuses, =1 always does, unset times it
     const char* ff = getenv("RAPTOR_B200_FUSE_FIRST");
     const int force_first = (ff && ff[0] == '0') ? 0 : (ff && ff[0] == '1') ? 1 : -1;
-    for (int l = 0; l + 1 < L && jac1; l++) {
+    for (int l = 0; l + 1 < L && jac1 && !strided_only; l++) {
         Level<T>& V = lv[l];
         if (force_first >= 0) {
             V.fuse_first = force_first == 1;

@@ -89,7 +89,9 @@ struct Idx16 {
 // schedule the lanes value G names
 template <typename T, typename TX, class Epi>
 void rows_op(const CsrView<T>& M, const Idx16& I, long n_rows, const TX* x, Epi epi, int G) {
-    if ((G & kRowsTiled) && I.tchunks) {
+    if constexpr (HasRowSkip<Epi>::value) {
+        G &= kRowsBlocked - 1;   // row-gated epilogues run the strided schedule
+    } else if ((G & kRowsTiled) && I.tchunks) {
         const int g = G & (kRowsBlocked - 1);
         if (I.on)
             launch_tiled<T, TX, Epi, true>(n_rows, M.rowptr, M.cols, I.base.get(), I.c16.get(),
@@ -126,7 +128,8 @@ struct Level {
     // y-epilogue over the rows of A_l times x, in whichever format was picked
     template <typename TX, class Epi>
     void apply_A(const TX* xin, Epi epi) const {
-        if (dia) launch_dia(off, Adia.get(), n, xin, epi);
+        if constexpr (HasRowSkip<Epi>::value) rows_op(A, A16, n, xin, epi, gA);
+        else if (dia) launch_dia(off, Adia.get(), n, xin, epi);
         else rows_op(A, A16, n, xin, epi, gA);
     }
 };
@@ -147,6 +150,10 @@ struct Hierarchy {
     PcgCtl* host_ctl = nullptr;   // pinned staging of the device-side loop state
     int gA0 = 0;
     bool use_graphs = true;
+    // the levels of an uneven batch: every operator on the strided schedule
+    // in CSR (16- or 32-bit indices), which the row gates of stopped systems
+    // apply to
+    bool strided_only = false;
     // bottom of the cycle (levels tail_from .. L-1) in one launch of one
     // cluster of tail_ctas CTAs (tail_cycle.cuh); tail_from = -1: off
     int tail_from = -1;

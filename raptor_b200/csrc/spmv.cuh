@@ -211,6 +211,33 @@ struct HasGate : std::false_type {};
 template <class Epi>
 struct HasGate<Epi, std::void_t<decltype(std::declval<const Epi&>().open())>> : std::true_type {};
 
+// Epilogues with skip(base) let the strided row kernels pass over the rows
+// [base, base + 32 / G) of a warp step without loading anything: an uneven
+// batch's systems that have stopped (RowGate).  The answer must be the same
+// for all rows of the step.  The blocked and shared-memory schedules are not
+// compiled for such epilogues.
+template <class Epi, class = void>
+struct HasRowSkip : std::false_type {};
+template <class Epi>
+struct HasRowSkip<Epi, std::void_t<decltype(std::declval<const Epi&>().skip(0L))>>
+    : std::true_type {};
+
+// Rows per byte of a row gate (a multiple of every warp step's 32 / G rows,
+// so that a step never straddles two bytes).
+constexpr int kGateShift = 8;
+
+// Epi restricted to the rows whose gate byte is zero: closed[row >> 8] != 0
+// marks 256 rows that need no update.
+template <class Epi>
+struct RowGate : Epi {
+    const unsigned char* closed;
+    __device__ bool skip(long base) const { return closed[base >> kGateShift] != 0; }
+};
+template <class Epi>
+RowGate<Epi> row_gate(const Epi& e, const unsigned char* closed) {
+    return RowGate<Epi>{e, closed};
+}
+
 // Epilogues with gather_scale() make the row kernels gather x_j * scale_j.
 template <class Epi, class = void>
 struct ScaledGather : std::false_type {};
@@ -301,6 +328,9 @@ k_csr_rows(long n, const int* __restrict__ rp, const int* __restrict__ ci,
     const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
     double red = 0.0;
     for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        if constexpr (HasRowSkip<Epi>::value) {
+            if (epi.skip(base)) continue;
+        }
         const long row = base + sub;
         const bool valid = row < n;
         int s = 0, e = 0;
@@ -350,6 +380,9 @@ k_csr_rows16(long n, const int* __restrict__ rp, const int* __restrict__ rbase,
     const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
     double red = 0.0;
     for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        if constexpr (HasRowSkip<Epi>::value) {
+            if (epi.skip(base)) continue;
+        }
         const long row = base + sub;
         const bool valid = row < n;
         int s = 0, e = 0, b0 = 0;
@@ -543,7 +576,8 @@ void launch_rows(const int* rp, const int* ci, const TV* cv, long n, long long n
     if (n <= 0) return;
     if (!st) st = stream();
     if (G <= 0) G = pick_group(n, nnz);
-    if (G & kRowsBlocked) {
+    if constexpr (HasRowSkip<Epi>::value) G &= kRowsBlocked - 1;
+    else if (G & kRowsBlocked) {
         const unsigned g = (unsigned)sm_count();
         switch (G & (kRowsBlocked - 1)) {
             case 1: k_csr_rows_blk<1><<<g, kRowBlockBlk, 0, st>>>(n, rp, ci, cv, x, epi); break;
@@ -574,7 +608,8 @@ void launch_rows16(const int* rp, const int* rbase, const unsigned short* c16, c
     if (n <= 0) return;
     if (G <= 0) G = pick_group(n, nnz);
     cudaStream_t st = stream();
-    if (G & kRowsBlocked) {
+    if constexpr (HasRowSkip<Epi>::value) G &= kRowsBlocked - 1;
+    else if (G & kRowsBlocked) {
         const unsigned g = (unsigned)sm_count();
         switch (G & (kRowsBlocked - 1)) {
             case 1: k_csr_rows16_blk<1><<<g, kRowBlockBlk, 0, st>>>(n, rp, rbase, c16, cv, x, epi); break;

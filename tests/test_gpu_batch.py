@@ -117,3 +117,36 @@ def test_batch_with_multicolour_ssor_and_zero_system():
     assert rc == 0
     assert iters[1] == 0 and np.all(x.numpy()[B.offsets[1]:B.offsets[2]] == 0.0)
     assert all(iters[s] > 0 for s in (0, 2, 3))
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_batch_stopped_systems_left_alone(prec):
+    """Systems that stop early leave the batch's cycle and outer iteration
+    (their rows are passed over from then on): a zero right-hand side stops
+    before the first iteration and its solution stays exactly zero, and every
+    other system, whichever iteration it stopped at, ends with the solution
+    and iteration count of its standalone solve."""
+    mats = systems(31, 5)
+    B = rb.Batch(mats, make_ml("rs", prec))
+    bh = np.random.default_rng(4).uniform(-1, 1, B.total_rows)
+    bh[B.offsets[2]:B.offsets[3]] = 0.0
+    x = rb.ParVector(B.total_rows)
+    rc, iters, relres = B.pcg(x, rb.ParVector(B.total_rows, values=bh), tol=1e-8, max_iter=400)
+    assert rc == 0
+    got = x.numpy()
+    assert iters[2] == 0 and np.all(got[B.offsets[2]:B.offsets[3]] == 0.0)
+    assert int(max(iters)) > int(min(i for i in iters if i > 0))
+    for s, A in enumerate(mats):
+        if s == 2:
+            continue
+        lo, hi = B.offsets[s], B.offsets[s + 1]
+        n = hi - lo
+        ml = make_ml("rs", prec)
+        ml.setup(A)
+        xs = rb.ParVector(n)
+        res = []
+        rb.PCG(A, ml, xs, rb.ParVector(n, values=bh[lo:hi]), res, tol=1e-8, max_iter=400,
+               mode=rb.PCG_TRUE_RESIDUAL)
+        assert abs(int(iters[s]) - (len(res) - 1)) <= 1, (s, iters[s], len(res) - 1)
+        ref = xs.numpy()
+        assert np.linalg.norm(got[lo:hi] - ref) <= 1e-6 * np.linalg.norm(ref), s
