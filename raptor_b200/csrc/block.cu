@@ -83,12 +83,13 @@ struct FinBTmp {
     __device__ void operator()(int c, double t) const { s->tmp[c] = t; }
 };
 
-// X += alpha_c P ; R -= alpha_c AP ; rr_c = R_c . R_c
+// X += alpha_c P ; R -= alpha_c AP ; rr_c = R_c . R_c; r32 (optional): R in
+// FP32 as well (the next block cycle's right-hand side in the FP32 form)
 template <int KP>
 __global__ void __launch_bounds__(256)
 k_bcg_update(long n, int k, double* __restrict__ X, double* __restrict__ R,
              const double* __restrict__ P, const double* __restrict__ AP,
-             const BlockScal* __restrict__ s, ReduceSlot rs, FinBRR fin) {
+             const BlockScal* __restrict__ s, ReduceSlot rs, FinBRR fin, float* __restrict__ r32) {
     constexpr int RPW = 32 / KP;
     const int lane = threadIdx.x & 31;
     const int c = lane % KP, sub = lane / KP;
@@ -102,19 +103,25 @@ k_bcg_update(long n, int k, double* __restrict__ X, double* __restrict__ R,
             X[e] += P[e] * alpha;
             const double ri = R[e] + AP[e] * (-1.0 * alpha);
             R[e] = ri;
+            if (r32) r32[e] = (float)ri;
             t += ri * ri;
         }
     }
     block_reduce_cols<KP>(t, k, rs, fin);
 }
 
-// P = Z + beta_c P (P = Z on a restart)
-__global__ void k_bcg_p(long n, int k, double* __restrict__ P, const double* __restrict__ Z,
+// P = Z + beta_c P (P = Z on a restart); Z FP64 or the FP32 output of the
+// block cycle.  Thread t: row t / KP, column t % KP.
+template <int KP, typename TZ>
+__global__ void k_bcg_p(long n, int k, double* __restrict__ P, const TZ* __restrict__ Z,
                         const BlockScal* __restrict__ s, int restart) {
-    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n * k) return;
-    if (restart) P[e] = Z[e];
-    else P[e] = P[e] * s->beta[e % k] + Z[e];
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long i = t / KP;
+    const int c = (int)(t % KP);
+    if (i >= n || c >= k) return;
+    const long e = i * k + c;
+    if (restart) P[e] = (double)Z[e];
+    else P[e] = P[e] * s->beta[c] + (double)Z[e];
 }
 
 std::string bkey(const char* tag, int k, const void* a, const void* b, const void* c) {
@@ -191,8 +198,17 @@ void bsmooth(const Hierarchy& H, const Level<T>& V, const BLevel<T>& W, T*& cur,
     if (!jt) return;   // Jacobi in compatibility mode leaves x unchanged
     for (int s = 0; s < sweeps; s++) {
         if (s == 0 && x_zero) {
-            k_scale_first_block<T><<<grid_for((long)V.n * k, 256), 256, 0, stream()>>>(
-                V.n, k, b, V.dinv.get(), cur);
+            if (const int lpr = vec_lanes(k, b, BStore<T>{cur})) {
+                RB_BLOCK_LPR_SWITCH(lpr, {
+                    k_scale_first_block_v<kL, T><<<grid_for((long)V.n * kL, 256), 256, 0,
+                                                   stream()>>>(V.n, k, b, V.dinv.get(), cur);
+                });
+            } else {
+                RB_BLOCK_KP_SWITCH(pow2_at_least(k), {
+                    k_scale_first_block<kKP, T><<<grid_for((long)V.n * kKP, 256), 256, 0,
+                                                  stream()>>>(V.n, k, b, V.dinv.get(), cur);
+                });
+            }
             RB_CHECK_LAUNCH();
             continue;
         }
@@ -354,12 +370,41 @@ int Hierarchy::pcg_block(const rb_csr_s& A, double* X, const double* B, int k, d
         relres[c] = 0.0;
     }
     push_active();
+    // In the FP32 form the block cycle reads R in FP32 (written by the update
+    // kernel, or converted after a full residual) and its FP32 output z is
+    // read directly by the r.z dots and the P update, without an FP64 copy.
+    const bool f32 = opts.precision == RB_PREC_FP32;
+    const long nk = n * k;
+    const int KP = pow2_at_least(k);
+    float* r32 = f32 ? bs.l32[0].b.get() : nullptr;
+    const float* z32 = f32 ? bs.l32[0].x.get() : nullptr;
+    auto to_r32 = [&]() {
+        k_convert<float, double><<<grid_for(nk, 256), 256, 0, stream()>>>(nk, R, r32);
+        RB_CHECK_LAUNCH();
+    };
+    auto precond = [&]() {   // z = M r from a zero guess
+        if (f32) block_cycle_level(*this, lv32, bs.l32, 0, bs.l32[0].x.get(), r32, true, k);
+        else block_cycle_level(*this, lv64, bs.l64, 0, Z, R, true, k);
+    };
+    auto dot_rz = [&](auto fin) {
+        if (f32) launch_block_dot(n, k, R, z32, fin);
+        else launch_block_dot(n, k, R, (const double*)Z, fin);
+    };
+    auto p_update = [&](int restart) {
+        const unsigned g = grid_for(n * KP, 256);
+        RB_BLOCK_KP_SWITCH(KP, {
+            if (f32) k_bcg_p<kKP, float><<<g, 256, 0, stream()>>>(n, k, P, z32, S, restart);
+            else k_bcg_p<kKP, double><<<g, 256, 0, stream()>>>(n, k, P, Z, S, restart);
+        });
+        RB_CHECK_LAUNCH();
+    };
     // R = B - A X ; Z = M R ; P = Z ; rz, rr
     auto restart = [&]() {
         block_residual64(bs, A, X, B, R);
-        block_cycle64(*this, bs, Z, R);
-        RB_CUDA(cudaMemcpyAsync(P, Z, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, stream()));
-        launch_block_dot(n, k, R, Z, FinBSetRZ{S});
+        if (f32) to_r32();
+        precond();
+        p_update(1);
+        dot_rz(FinBSetRZ{S});
         launch_block_dot(n, k, R, R, FinBRR{S});
     };
     restart();
@@ -401,22 +446,22 @@ int Hierarchy::pcg_block(const rb_csr_s& A, double* X, const double* B, int k, d
         return true;
     };
     if (check()) return RB_OK;
-    const long nk = n * k;
-    const int KP = pow2_at_least(k);
     auto body = [&](bool full_r) {
         block_outer_apply(*this, bs, A, P, AP);
         const unsigned g = block_grid(n, KP, 1);
         ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+        float* r32_out = (f32 && !full_r) ? r32 : nullptr;
         RB_BLOCK_KP_SWITCH(KP, {
-            k_bcg_update<kKP><<<g, 256, 0, stream()>>>(n, k, X, R, P, AP, S, rs, FinBRR{S});
+            k_bcg_update<kKP><<<g, 256, 0, stream()>>>(n, k, X, R, P, AP, S, rs, FinBRR{S}, r32_out);
         });
         RB_CHECK_LAUNCH();
         if (full_r) {
             block_residual64(bs, A, X, B, R);
             launch_block_dot(n, k, R, R, FinBRR{S});
+            if (f32) to_r32();
         }
-        block_cycle64(*this, bs, Z, R);
-        launch_block_dot(n, k, R, Z, FinBRZ{S});
+        precond();
+        dot_rz(FinBRZ{S});
     };
     int status = RB_ERR_NOT_CONVERGED;
     while (iter < max_iter) {
@@ -426,8 +471,7 @@ int Hierarchy::pcg_block(const rb_csr_s& A, double* X, const double* B, int k, d
         read();
         if (h.breakdown) return RB_ERR_BREAKDOWN;
         if (check()) { status = RB_OK; break; }
-        k_bcg_p<<<grid_for(nk, 256), 256, 0, stream()>>>(n, k, P, Z, S, 0);
-        RB_CHECK_LAUNCH();
+        p_update(0);
     }
     if (status != RB_OK) {
         for (int c = 0; c < k; c++)

@@ -51,12 +51,78 @@ constexpr int kMaxBlockK = 32;
     __launch_bounds__(256, (ND > 0 && ND <= 9 && RB_BLOCK_MINB_SMALL > 0) ? RB_BLOCK_MINB_SMALL : 1)
 #endif
 
+// ------------------------------------------------- 16-byte column groups --
+// VW = 16 / sizeof(T) consecutive columns of one block-vector row move as one
+// 16-byte access (float4 / double2).  The vectorised kernels give a lane VW
+// columns of its row, so a warp covers VW times the rows of the
+// one-column-a-lane layout per step and every load instruction moves four
+// (FP32) or two (FP64) times the bytes: at k >= VW the block kernels are
+// bound by the loads they keep in flight, not by their bytes.  Used when k is
+// a multiple of VW and every vector the kernel touches starts on a 16-byte
+// boundary (rows then start on one too).
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using type = float4;
+    static constexpr int n = 4;
+};
+template <>
+struct Vec16<double> {
+    using type = double2;
+    static constexpr int n = 2;
+};
+
+template <typename T, int VW>
+__device__ __forceinline__ void vunpack(const typename Vec16<T>::type& u, T (&v)[VW]) {
+    static_assert(VW == Vec16<T>::n, "16-byte groups");
+    if constexpr (VW == 4) {
+        v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
+    } else {
+        v[0] = u.x; v[1] = u.y;
+    }
+}
+// through the read-only path (vectors no thread of the kernel writes)
+template <typename T, int VW>
+__device__ __forceinline__ void vload_ro(const T* p, T (&v)[VW]) {
+    vunpack<T, VW>(__ldg(reinterpret_cast<const typename Vec16<T>::type*>(p)), v);
+}
+// a plain load (the thread may write the same entries afterwards)
+template <typename T, int VW>
+__device__ __forceinline__ void vload(const T* p, T (&v)[VW]) {
+    vunpack<T, VW>(*reinterpret_cast<const typename Vec16<T>::type*>(p), v);
+}
+template <typename T, int VW>
+__device__ __forceinline__ void vstore(T* p, const T (&v)[VW]) {
+    static_assert(VW == Vec16<T>::n, "16-byte groups");
+    typename Vec16<T>::type u;
+    if constexpr (VW == 4) {
+        u.x = v[0]; u.y = v[1]; u.z = v[2]; u.w = v[3];
+    } else {
+        u.x = v[0]; u.y = v[1];
+    }
+    *reinterpret_cast<typename Vec16<T>::type*>(p) = u;
+}
+
+inline bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
 // ----------------------------------------------------------- epilogues --
+// operator(): one entry (i, c); vec: the VW entries (i, c0 .. c0 + VW - 1),
+// each computed as operator() computes it; al16: every vector starts on a
+// 16-byte boundary.
 template <typename TY>
 struct BStore {
     TY* y;
     template <typename A>
     __device__ void operator()(long i, int c, int k, A s) const { y[i * k + c] = (TY)s; }
+    template <int VW, typename A>
+    __device__ void vec(long i, int c0, int k, const A (&s)[VW]) const {
+        TY o[VW];
+#pragma unroll
+        for (int v = 0; v < VW; v++) o[v] = (TY)s[v];
+        vstore<TY, VW>(y + i * k + c0, o);
+    }
+    bool al16v() const { return al16(y); }
 };
 
 template <typename TB, typename TY>
@@ -67,6 +133,16 @@ struct BResidual {
     __device__ void operator()(long i, int c, int k, A s) const {
         r[i * k + c] = (TY)((A)b[i * k + c] - s);
     }
+    template <int VW, typename A>
+    __device__ void vec(long i, int c0, int k, const A (&s)[VW]) const {
+        TB bb[VW];
+        vload_ro<TB, VW>(b + i * k + c0, bb);
+        TY o[VW];
+#pragma unroll
+        for (int v = 0; v < VW; v++) o[v] = (TY)((A)bb[v] - s[v]);
+        vstore<TY, VW>(r + i * k + c0, o);
+    }
+    bool al16v() const { return al16(b) && al16(r); }
 };
 
 template <typename TY>
@@ -76,6 +152,15 @@ struct BAppend {
     __device__ void operator()(long i, int c, int k, A s) const {
         y[i * k + c] = (TY)((A)y[i * k + c] + s);
     }
+    template <int VW, typename A>
+    __device__ void vec(long i, int c0, int k, const A (&s)[VW]) const {
+        TY yy[VW];
+        vload<TY, VW>(y + i * k + c0, yy);
+#pragma unroll
+        for (int v = 0; v < VW; v++) yy[v] = (TY)((A)yy[v] + s[v]);
+        vstore<TY, VW>(y + i * k + c0, yy);
+    }
+    bool al16v() const { return al16(y); }
 };
 
 template <typename TY>
@@ -86,6 +171,15 @@ struct BAddTo {
     __device__ void operator()(long i, int c, int k, A s) const {
         y[i * k + c] = (TY)((A)x0[i * k + c] + s);
     }
+    template <int VW, typename A>
+    __device__ void vec(long i, int c0, int k, const A (&s)[VW]) const {
+        TY xx[VW];
+        vload_ro<TY, VW>(x0 + i * k + c0, xx);
+#pragma unroll
+        for (int v = 0; v < VW; v++) xx[v] = (TY)((A)xx[v] + s[v]);
+        vstore<TY, VW>(y + i * k + c0, xx);
+    }
+    bool al16v() const { return al16(x0) && al16(y); }
 };
 
 // xn = xo + dinv_i (b - A xo), dinv per row
@@ -100,6 +194,19 @@ struct BJacobi {
         const long e = i * k + c;
         xn[e] = (T)((A)xo[e] + (A)dinv[i] * ((A)b[e] - s));
     }
+    template <int VW, typename A>
+    __device__ void vec(long i, int c0, int k, const A (&s)[VW]) const {
+        const long e = i * k + c0;
+        T xx[VW], bb[VW];
+        vload_ro<T, VW>(xo + e, xx);
+        vload_ro<T, VW>(b + e, bb);
+        const A d = (A)__ldg(dinv + i);
+        T o[VW];
+#pragma unroll
+        for (int v = 0; v < VW; v++) o[v] = (T)((A)xx[v] + d * ((A)bb[v] - s[v]));
+        vstore<T, VW>(xn + e, o);
+    }
+    bool al16v() const { return al16(xo) && al16(b) && al16(xn); }
 };
 
 // ------------------------------------------------ per-column reductions --
@@ -108,17 +215,13 @@ struct BJacobi {
 // fixed order), writes partials[block * KP + c], and the last block to
 // finish sums the block partials per column in a fixed order and calls
 // fin(c, total) for c < k.  Bit-reproducible for a given grid.
+// The block's per-warp column sums wpart[w][c] onwards.
 template <int KP, class Fin>
-__device__ void block_reduce_cols(double v, int k, const ReduceSlot& rs, Fin fin) {
+__device__ void block_reduce_cols_tail(double (*wpart)[KP], int k, const ReduceSlot& rs, Fin fin) {
     constexpr int kWarps = 256 / 32;
     constexpr int kStrands = 256 / KP;
-    __shared__ double wpart[kWarps][KP];
     __shared__ double spart[256];
     __shared__ bool is_last;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = KP; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane < KP) wpart[wid][lane] = v;
     __syncthreads();
     if (threadIdx.x < KP) {
         double t = 0.0;
@@ -146,6 +249,34 @@ __device__ void block_reduce_cols(double v, int k, const ReduceSlot& rs, Fin fin
     }
     __syncthreads();
     if (threadIdx.x == 0) *rs.ticket = 0u;
+}
+
+template <int KP, class Fin>
+__device__ void block_reduce_cols(double v, int k, const ReduceSlot& rs, Fin fin) {
+    constexpr int kWarps = 256 / 32;
+    __shared__ double wpart[kWarps][KP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = KP; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane < KP) wpart[wid][lane] = v;
+    block_reduce_cols_tail<KP>(wpart, k, rs, fin);
+}
+
+// The same with VW columns a lane: lane l carries columns (l % LPR) VW + v.
+template <int LPR, int VW, class Fin>
+__device__ void block_reduce_cols_v(double (&v)[VW], int k, const ReduceSlot& rs, Fin fin) {
+    constexpr int KP = LPR * VW;
+    constexpr int kWarps = 256 / 32;
+    __shared__ double wpart[kWarps][KP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = LPR; o < 32; o <<= 1)
+#pragma unroll
+        for (int q = 0; q < VW; q++) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    if (lane < LPR)
+#pragma unroll
+        for (int q = 0; q < VW; q++) wpart[wid][lane * VW + q] = v[q];
+    block_reduce_cols_tail<KP>(wpart, k, rs, fin);
 }
 
 // ----------------------------------------------------------- CSR SpMM --
@@ -304,6 +435,106 @@ k_csr_block_dot(long n, int k, const int* __restrict__ rp, const int* __restrict
     block_reduce_cols<KP>(red, k, rsl, fin);
 }
 
+// ------------------------------------------------ vectorised CSR SpMM --
+// LPR = KP / VW lanes a row, each with VW columns (Vec16); 32 / LPR rows a
+// warp step.  The row's indices and values are broadcast loads (the LPR
+// lanes of a row read the same entry); every lane then has the 16-byte
+// gathers of up to RB_BLOCK_VEC_UN nonzeros in flight before it uses the
+// first.  Each column's products are added in increasing position, as in
+// k_csr_block with one row split.
+#ifndef RB_BLOCK_VEC_UN
+#define RB_BLOCK_VEC_UN 8
+#endif
+
+template <int LPR, typename TV, typename TX, typename Acc>
+__device__ __forceinline__ void csr_row_v(int rs, int re, bool on, const int* __restrict__ ci,
+                                          const TV* __restrict__ cv, const TX* __restrict__ X,
+                                          int k, int c0, Acc (&acc)[Vec16<TX>::n]) {
+    constexpr int VW = Vec16<TX>::n;
+    constexpr int UN = RB_BLOCK_VEC_UN;
+#pragma unroll
+    for (int v = 0; v < VW; v++) acc[v] = Acc(0);
+    for (int j = rs; j < re; j += UN) {
+        int cc[UN];
+        TV vv[UN];
+#pragma unroll
+        for (int u = 0; u < UN; u++) {
+            const bool in = j + u < re;
+            cc[u] = in ? __ldg(ci + j + u) : 0;
+            vv[u] = in ? __ldg(cv + j + u) : TV(0);
+        }
+        TX xx[UN][VW];
+#pragma unroll
+        for (int u = 0; u < UN; u++) {
+            if (on && j + u < re) {
+                vload_ro<TX, VW>(X + (long)cc[u] * k + c0, xx[u]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < VW; v++) xx[u][v] = TX(0);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UN; u++)
+            if (j + u < re)
+#pragma unroll
+                for (int v = 0; v < VW; v++) acc[v] += (Acc)vv[u] * (Acc)xx[u][v];
+    }
+}
+
+template <int LPR, typename TV, typename TX, typename Acc, class Epi>
+__global__ void __launch_bounds__(256)
+k_csr_block_v(long n, int k, const int* __restrict__ rp, const int* __restrict__ ci,
+              const TV* __restrict__ cv, const TX* __restrict__ X, Epi epi) {
+    constexpr int VW = Vec16<TX>::n;
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31;
+    const int c0 = (lane % LPR) * VW, sub = lane / LPR;
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        const bool on = row < n && c0 < k;
+        int rs = 0, re = 0;
+        if (row < n) { rs = __ldg(rp + row); re = __ldg(rp + row + 1); }
+        Acc acc[VW];
+        csr_row_v<LPR, TV, TX, Acc>(rs, re, on, ci, cv, X, k, c0, acc);
+        if (on) epi.template vec<VW>(row, c0, k, acc);
+    }
+}
+
+// Y = A P with the per-column dots p.y, VW columns a lane
+template <int LPR, typename TV, class Fin>
+__global__ void __launch_bounds__(256)
+k_csr_block_dot_v(long n, int k, const int* __restrict__ rp, const int* __restrict__ ci,
+                  const TV* __restrict__ cv, const double* __restrict__ P, double* __restrict__ Y,
+                  ReduceSlot rsl, Fin fin) {
+    constexpr int VW = Vec16<double>::n;
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31;
+    const int c0 = (lane % LPR) * VW, sub = lane / LPR;
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    double red[VW];
+#pragma unroll
+    for (int v = 0; v < VW; v++) red[v] = 0.0;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long row = base + sub;
+        const bool on = row < n && c0 < k;
+        int rs = 0, re = 0;
+        if (row < n) { rs = __ldg(rp + row); re = __ldg(rp + row + 1); }
+        double acc[VW];
+        csr_row_v<LPR, TV, double, double>(rs, re, on, ci, cv, P, k, c0, acc);
+        if (on) {
+            double pp[VW];
+            vload_ro<double, VW>(P + row * k + c0, pp);
+            vstore<double, VW>(Y + row * k + c0, acc);
+#pragma unroll
+            for (int v = 0; v < VW; v++) red[v] += pp[v] * acc[v];
+        }
+    }
+    block_reduce_cols_v<LPR, VW>(red, k, rsl, fin);
+}
+
 // ---------------------------------------------------- sliced DIA SpMM --
 // A warp step covers U groups of 32 / KP consecutive rows; every value and
 // gathered x of the step is loaded before the first product.
@@ -419,19 +650,135 @@ k_sdia_block_dot(long n, int k, DiaOff off, const TV* __restrict__ sv,
     block_reduce_cols<KP>(red, k, rsl, fin);
 }
 
-// ------------------------------------------------------- block BLAS-1 --
-// x = dinv .* b per column (first Jacobi sweep from a zero guess)
-template <typename T>
-__global__ void k_scale_first_block(long n, int k, const T* __restrict__ b,
-                                    const T* __restrict__ dinv, T* __restrict__ x) {
-    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < n * k) x[e] = b[e] * dinv[e / k];
+// ----------------------------------------------- vectorised DIA SpMM --
+// LPR lanes a row with VW columns each (Vec16), 32 / LPR consecutive rows a
+// warp step (their values of one diagonal share a 32-row slice); the
+// diagonals are taken DC at a time, all values and 16-byte gathers of a
+// group loaded before its products, which are added in diagonal order as
+// in k_sdia_block.
+template <int ND>
+struct DiaChunk {
+    static constexpr int DC = ND < 9 ? ND : 9;
+    static_assert(ND % DC == 0, "diagonal groups");
+};
+
+template <int ND, int LPR, typename TV, typename TX, typename Acc>
+__device__ __forceinline__ void sdia_row_v(long i, long n, bool on, const DiaOff& off,
+                                           const TV* __restrict__ sv, const TX* __restrict__ X,
+                                           int k, int c0, Acc (&acc)[Vec16<TX>::n]) {
+    constexpr int VW = Vec16<TX>::n;
+    constexpr int DC = DiaChunk<ND>::DC;
+    const TV* a = sv + (i >> 5) * ND * 32 + (i & 31);
+#pragma unroll
+    for (int v = 0; v < VW; v++) acc[v] = Acc(0);
+#pragma unroll
+    for (int d0 = 0; d0 < ND; d0 += DC) {
+        TV av[DC];
+        TX xv[DC][VW];
+#pragma unroll
+        for (int d = 0; d < DC; d++) {
+            const long j = i + off.o[d0 + d];
+            const bool in = on && j >= 0 && j < n;
+            av[d] = in ? __ldg(a + (d0 + d) * 32) : TV(0);
+            if (in) {
+                vload_ro<TX, VW>(X + j * k + c0, xv[d]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < VW; v++) xv[d][v] = TX(0);
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < DC; d++)
+#pragma unroll
+            for (int v = 0; v < VW; v++) acc[v] += (Acc)av[d] * (Acc)xv[d][v];
+    }
 }
 
-// Per-column dot a.b over n rows of k columns (FP64), through fin(c, t).
-template <int KP, class Fin>
+template <int ND, int LPR, typename TV, typename TX, typename Acc, class Epi>
 __global__ void __launch_bounds__(256)
-k_block_dot(long n, int k, const double* __restrict__ a, const double* __restrict__ b,
+k_sdia_block_v(long n, int k, DiaOff off, const TV* __restrict__ sv, const TX* __restrict__ X,
+               Epi epi) {
+    constexpr int VW = Vec16<TX>::n;
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31;
+    const int c0 = (lane % LPR) * VW, sub = lane / LPR;
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long i = base + sub;
+        const bool on = i < n && c0 < k;
+        Acc acc[VW];
+        sdia_row_v<ND, LPR, TV, TX, Acc>(i, n, on, off, sv, X, k, c0, acc);
+        if (on) epi.template vec<VW>(i, c0, k, acc);
+    }
+}
+
+template <int ND, int LPR, typename TV, class Fin>
+__global__ void __launch_bounds__(256)
+k_sdia_block_dot_v(long n, int k, DiaOff off, const TV* __restrict__ sv,
+                   const double* __restrict__ P, double* __restrict__ Y, ReduceSlot rsl, Fin fin) {
+    constexpr int VW = Vec16<double>::n;
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31;
+    const int c0 = (lane % LPR) * VW, sub = lane / LPR;
+    const long gwarp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    double red[VW];
+#pragma unroll
+    for (int v = 0; v < VW; v++) red[v] = 0.0;
+    for (long base = gwarp * RPW; base < n; base += nwarps * RPW) {
+        const long i = base + sub;
+        const bool on = i < n && c0 < k;
+        double acc[VW];
+        sdia_row_v<ND, LPR, TV, double, double>(i, n, on, off, sv, P, k, c0, acc);
+        if (on) {
+            double pp[VW];
+            vload_ro<double, VW>(P + i * k + c0, pp);
+            vstore<double, VW>(Y + i * k + c0, acc);
+#pragma unroll
+            for (int v = 0; v < VW; v++) red[v] += pp[v] * acc[v];
+        }
+    }
+    block_reduce_cols_v<LPR, VW>(red, k, rsl, fin);
+}
+
+// ------------------------------------------------------- block BLAS-1 --
+// x = dinv .* b per column (first Jacobi sweep from a zero guess)
+// VW columns a thread (Vec16): thread t takes row t / LPR, columns
+// (t % LPR) VW ..
+template <int LPR, typename T>
+__global__ void k_scale_first_block_v(long n, int k, const T* __restrict__ b,
+                                      const T* __restrict__ dinv, T* __restrict__ x) {
+    constexpr int VW = Vec16<T>::n;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long i = t / LPR;
+    const int c0 = (int)(t % LPR) * VW;
+    if (i >= n || c0 >= k) return;
+    T bb[VW];
+    vload_ro<T, VW>(b + i * k + c0, bb);
+    const T d = __ldg(dinv + i);
+#pragma unroll
+    for (int v = 0; v < VW; v++) bb[v] = bb[v] * d;
+    vstore<T, VW>(x + i * k + c0, bb);
+}
+
+// (thread t: row t / KP, column t % KP; no division by k per entry)
+template <int KP, typename T>
+__global__ void k_scale_first_block(long n, int k, const T* __restrict__ b,
+                                    const T* __restrict__ dinv, T* __restrict__ x) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long i = t / KP;
+    const int c = (int)(t % KP);
+    if (i >= n || c >= k) return;
+    const long e = i * k + c;
+    x[e] = b[e] * dinv[i];
+}
+
+// Per-column dot a.b over n rows of k columns (FP64 accumulation; b FP64 or
+// the FP32 output of a block cycle), through fin(c, t).
+template <int KP, typename TB, class Fin>
+__global__ void __launch_bounds__(256)
+k_block_dot(long n, int k, const double* __restrict__ a, const TB* __restrict__ b,
             ReduceSlot rsl, Fin fin) {
     constexpr int RPW = 32 / KP;
     const int lane = threadIdx.x & 31;
@@ -440,7 +787,8 @@ k_block_dot(long n, int k, const double* __restrict__ a, const double* __restric
     const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
     double t = 0.0;
     if (c < k)
-        for (long i = gwarp * RPW + sub; i < n; i += nwarps * RPW) t += a[i * k + c] * b[i * k + c];
+        for (long i = gwarp * RPW + sub; i < n; i += nwarps * RPW)
+            t += a[i * k + c] * (double)b[i * k + c];
     block_reduce_cols<KP>(t, k, rsl, fin);
 }
 
@@ -522,11 +870,39 @@ inline unsigned block_grid_gather(const void* fn, long n, int KP, int S) {
     }
 
 // CSR SpMM with tile shape (KP from k, S rows splits).
+// Lanes a row of the vectorised kernels (0: they do not apply): k a multiple
+// of VW and every vector on a 16-byte boundary.
+template <typename TX, class Epi>
+int vec_lanes(int k, const TX* X, const Epi& epi) {
+    constexpr int VW = Vec16<TX>::n;
+    static const bool off = grid_per_sm("RAPTOR_B200_BLOCK_SCALAR", 0) > 0;
+    if (off || k < VW || k % VW || !al16(X) || !epi.al16v()) return 0;
+    return pow2_at_least(k) / VW;
+}
+
+#define RB_BLOCK_LPR_SWITCH(LPR, ...)                              \
+    switch (LPR) {                                                  \
+        case 1: { constexpr int kL = 1; __VA_ARGS__; } break;      \
+        case 2: { constexpr int kL = 2; __VA_ARGS__; } break;      \
+        case 4: { constexpr int kL = 4; __VA_ARGS__; } break;      \
+        case 8: { constexpr int kL = 8; __VA_ARGS__; } break;      \
+        default: { constexpr int kL = 16; __VA_ARGS__; } break;    \
+    }
+
 template <typename TV, typename TX, class Epi>
 void launch_csr_block(const int* rp, const int* ci, const TV* cv, long n, int k, const TX* X,
                       Epi epi, int S) {
     if (n <= 0) return;
     using Acc = AccOf2<TV, TX>;
+    if (const int lpr = vec_lanes(k, X, epi)) {
+        RB_BLOCK_LPR_SWITCH(lpr, {
+            auto kern = k_csr_block_v<kL, TV, TX, Acc, Epi>;
+            const unsigned g = block_grid_gather((const void*)kern, n, kL, 1);
+            kern<<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, X, epi);
+        });
+        RB_CHECK_LAUNCH();
+        return;
+    }
     const int KP = pow2_at_least(k);
     if (KP * S > 32) S = 32 / KP;
     auto go = [&](auto kern, int s) {
@@ -551,6 +927,16 @@ void launch_csr_block(const int* rp, const int* ci, const TV* cv, long n, int k,
 template <typename TV, class Fin>
 void launch_csr_block_dot(const int* rp, const int* ci, const TV* cv, long n, int k,
                           const double* P, double* Y, int S, Fin fin) {
+    if (const int lpr = vec_lanes(k, P, BStore<double>{Y})) {
+        RB_BLOCK_LPR_SWITCH(lpr, {
+            auto kern = k_csr_block_dot_v<kL, TV, Fin>;
+            const unsigned g = block_grid_gather((const void*)kern, n, kL, 1);
+            ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+            kern<<<g, 256, 0, stream()>>>(n, k, rp, ci, cv, P, Y, rs, fin);
+        });
+        RB_CHECK_LAUNCH();
+        return;
+    }
     const int KP = pow2_at_least(k);
     if (KP * S > 32) S = 32 / KP;
     auto go = [&](auto kern, int s) {
@@ -577,6 +963,18 @@ template <typename TV, typename TX, class Epi>
 void launch_dia_block(const DiaOff& off, const TV* sv, long n, int k, const TX* X, Epi epi) {
     if (n <= 0) return;
     using Acc = AccOf2<TV, TX>;
+    if (off.nd == 7 || off.nd == 27) {
+        if (const int lpr = vec_lanes(k, X, epi)) {
+            RB_BLOCK_LPR_SWITCH(lpr, {
+                auto kern = off.nd == 7 ? k_sdia_block_v<7, kL, TV, TX, Acc, Epi>
+                                        : k_sdia_block_v<27, kL, TV, TX, Acc, Epi>;
+                const unsigned g = block_grid_gather((const void*)kern, n, kL, 1);
+                kern<<<g, 256, 0, stream()>>>(n, k, off, sv, X, epi);
+            });
+            RB_CHECK_LAUNCH();
+            return;
+        }
+    }
     const int KP = pow2_at_least(k);
     auto go = [&](auto kern) {
         const unsigned g = block_grid_gather((const void*)kern, n, KP, 1);
@@ -595,6 +993,19 @@ void launch_dia_block(const DiaOff& off, const TV* sv, long n, int k, const TX* 
 template <typename TV, class Fin>
 void launch_dia_block_dot(const DiaOff& off, const TV* sv, long n, int k, const double* P,
                           double* Y, Fin fin) {
+    if (off.nd == 7 || off.nd == 27) {
+        if (const int lpr = vec_lanes(k, P, BStore<double>{Y})) {
+            RB_BLOCK_LPR_SWITCH(lpr, {
+                auto kern = off.nd == 7 ? k_sdia_block_dot_v<7, kL, TV, Fin>
+                                        : k_sdia_block_dot_v<27, kL, TV, Fin>;
+                const unsigned g = block_grid_gather((const void*)kern, n, kL, 1);
+                ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
+                kern<<<g, 256, 0, stream()>>>(n, k, off, sv, P, Y, rs, fin);
+            });
+            RB_CHECK_LAUNCH();
+            return;
+        }
+    }
     const int KP = pow2_at_least(k);
     auto go = [&](auto kern) {
         const unsigned g = block_grid_gather((const void*)kern, n, KP, 1);
@@ -611,12 +1022,12 @@ void launch_dia_block_dot(const DiaOff& off, const TV* sv, long n, int k, const 
     RB_CHECK_LAUNCH();
 }
 
-template <class Fin>
-void launch_block_dot(long n, int k, const double* a, const double* b, Fin fin) {
+template <typename TB, class Fin>
+void launch_block_dot(long n, int k, const double* a, const TB* b, Fin fin) {
     const int KP = pow2_at_least(k);
     const unsigned g = block_grid(n, KP, 1);
     ReduceSlot rs = global_reduce_slot((int)g * kMaxBlockK);
-    RB_BLOCK_KP_SWITCH(KP, { k_block_dot<kKP><<<g, 256, 0, stream()>>>(n, k, a, b, rs, fin); });
+    RB_BLOCK_KP_SWITCH(KP, { k_block_dot<kKP, TB><<<g, 256, 0, stream()>>>(n, k, a, b, rs, fin); });
     RB_CHECK_LAUNCH();
 }
 
