@@ -205,9 +205,12 @@ class ClockSampler:
 # ------------------------------------------------------------------ b200 ----
 def a_bytes(ml, l, vbytes):
     """Bytes of one pass over A_l in its stored format: CSR z(v+4) + (n+1)4,
-    or the sliced diagonals nd * 32 ceil(n/32) v (no indices)."""
+    the sliced diagonals nd * 32 ceil(n/32) v (no indices), or, for
+    diagonals with constant coefficients, one 4-byte mask a row."""
     n, z, _ = ml.level_info(l)
     nd = ml.level_storage(l)
+    if nd and ml.level_const_coef(l):
+        return 4 * n
     if nd:
         return nd * 32 * ((n + 31) // 32) * vbytes
     return z * (vbytes + 4) + (n + 1) * 4
@@ -536,9 +539,10 @@ def run_b200(args, rank, world, local):
     x = rb.ParVector(n)
     bnorm = float(np.linalg.norm(bh))
 
-    def make(prec):
+    def make(prec, const_coef=1):
         ml = rb.ParRugeStubenSolver(0.25, rb.PMIS, rb.Extended, rb.Classical, rb.L1Jacobi)
         ml.precision = prec
+        ml.const_coef = const_coef
         ml.setup(A)
         return ml
 
@@ -609,8 +613,12 @@ def run_b200(args, rank, world, local):
         "first_sweep_A0_fp32": 3 * n0 * 4,
     }
     peak, peak_kind = peaks()
-    dom = "jacobi_A0_fp32"
+    # the dominant kernel: the longest of the level-0 operations an iteration
+    # runs once each
+    dom = max(("residual_A0_fp32", "jacobi_A0_fp32", "spmv_dot_A0_fp64", "restrict_R0_fp32",
+               "prolong_P0_fp32"), key=lambda k: op_ms[k])
     achieved = alg[dom] / (op_ms[dom] * 1e-3) / 1e9
+    a0_const = ml32.level_const_coef(0)
 
     # FP64 form
     fp64 = None
@@ -627,6 +635,20 @@ def run_b200(args, rank, world, local):
         ml = ml64
     else:
         ml = ml32
+
+    # both forms again with level 0's stored values read (no constant-
+    # coefficient mask): what a stencil with varying coefficients would cost
+    stored = None
+    if not args.no_fp64 and ml32.level_const_coef(0):
+        stored = {}
+        for name, prec in (("fp32_form", rb.FP32), ("fp64_form", rb.FP64)):
+            mls = make(prec, const_coef=0)
+            ts_, its_, _ = timed(mls, max(2, args.steps // 2), 2)
+            stored[name] = {"seconds": ts_, "iters": its_[-1],
+                            "cycle_ms": mls.time_operator(0, 5, reps=20)}
+            del mls
+        stored["speedup_fp32_over_fp64"] = (stored["fp64_form"]["seconds"] /
+                                            stored["fp32_form"]["seconds"])
 
     # end to end through the public API with host buffers
     import ctypes as C
@@ -692,10 +714,14 @@ def run_b200(args, rank, world, local):
                    "levels": [ml32.level_info(l) for l in range(ml32.num_levels)],
                    "lanes": [ml32.level_lanes(l) for l in range(ml32.num_levels)]},
         "fp64_form": fp64,
+        "stored_values_level0": stored,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic_for(dom),
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic_for(dom + ("_const" if a0_const else "")),
                      "peak_source": peak_kind, "ops_ms": op_ms, "alg_bytes": alg,
-                     "a0_storage": ("sliced-diagonals nd=%d" % ml32.level_storage(0))
+                     "a0_storage": (("constant-coefficient diagonals nd=%d (a 4-byte mask a "
+                                     "row)" if ml32.level_const_coef(0) else
+                                     "sliced-diagonals nd=%d") % ml32.level_storage(0))
                      if ml32.level_storage(0) else "csr"},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": n * 8, "pinned": pinned},

@@ -204,6 +204,9 @@ typedef struct rb_amg_opts {
                                  (none if no start beats separate launches); 0: never;
                                  k >= 2: from level k-1 if that level qualifies */
     int use_graphs;           /* 1: replay cycles / Krylov iterations from CUDA graphs */
+    int const_coef;           /* 1 (default): a diagonal-storage level whose diagonals each hold one
+                                 value is read as a mask a row plus those values (same results);
+                                 0: the stored values */
 } rb_amg_opts;
 
 void rb_amg_default_opts(rb_amg_opts* opts);
@@ -248,6 +251,13 @@ int rb_amg_level_lanes(rb_amg ml, int level, int* lanes_A, int* lanes_P, int* la
 /* Storage of A_l in the cycle: *ndiag = number of stored diagonals when the
  * autotuner picked the sliced-diagonal layout, 0 for CSR. */
 int rb_amg_level_storage(rb_amg ml, int level, int* ndiag);
+/* 1 when A_l is stored by diagonals with constant coefficients (every
+ * nonzero of a diagonal has one value, as in a constant-coefficient stencil):
+ * the cycle's kernels then read one 4-byte mask a row (which of the stencil's
+ * entries the row has) in place of the row's values, with the same products
+ * in the same order.  RAPTOR_B200_CONST_DIA=0 at setup keeps the values.  No
+ * counterpart in the reference. */
+int rb_amg_level_const_coef(rb_amg ml, int level, int* constant);
 /* 1 when level l's first sweep from zero runs fused with its residual (one
  * pass over A_l; the autotuner's pick), else 0.  No counterpart in the
  * reference. */

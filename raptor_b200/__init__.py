@@ -358,7 +358,7 @@ class ParMultilevel:
     _FIELDS = ("strong_threshold", "relax_weight", "num_smooth_sweeps", "max_coarse",
                "max_levels", "max_iterations", "solve_tol", "interp_filter")
     _EXTRA = ("precision", "jacobi_compat", "seed_offset", "relax_type", "strength_type",
-              "interp_type", "fuse_coarse", "use_graphs", "prolong_weight",
+              "interp_type", "fuse_coarse", "use_graphs", "const_coef", "prolong_weight",
               "prolong_smooth_steps", "solver")
 
     def __init__(self, strong_threshold=0.0, strength_type=Classical, relax_type=SOR):
@@ -475,6 +475,13 @@ class ParMultilevel:
         nd = C.c_int()
         check(lib().rb_amg_level_storage(self.h, l, C.byref(nd)))
         return nd.value
+
+    def level_const_coef(self, l):
+        """True when A_l's diagonals have constant coefficients and the cycle
+        reads a mask a row instead of the values (see the C ABI)."""
+        f = C.c_int()
+        check(lib().rb_amg_level_const_coef(self.h, l, C.byref(f)))
+        return bool(f.value)
 
     def level_fused_first(self, l):
         """True when level l's first sweep runs fused with its residual."""

@@ -40,7 +40,7 @@ class AmgOpts(C.Structure):
         ("relax_weight", C.c_double), ("solve_tol", C.c_double), ("interp_filter", C.c_double),
         ("prolong_weight", C.c_double), ("prolong_smooth_steps", C.c_int),
         ("precision", C.c_int), ("jacobi_compat", C.c_int), ("seed_offset", C.c_int),
-        ("fuse_coarse", C.c_int), ("use_graphs", C.c_int),
+        ("fuse_coarse", C.c_int), ("use_graphs", C.c_int), ("const_coef", C.c_int),
     ]
 
 
@@ -115,6 +115,7 @@ SIGNATURES = {
     "rb_amg_setup_seconds": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "rb_amg_level_lanes": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "rb_amg_level_storage": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "rb_amg_level_const_coef": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "rb_amg_tail_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "rb_amg_level_fused_first": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "rb_amg_tail_timings": (C.c_int, [_P, _D, C.c_int, C.POINTER(C.c_int)]),

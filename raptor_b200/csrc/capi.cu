@@ -611,6 +611,7 @@ void rb_amg_default_opts(rb_amg_opts* o) {
     o->seed_offset = 0;
     o->fuse_coarse = 1;
     o->use_graphs = 1;
+    o->const_coef = 1;
 }
 
 int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_amg* out) {
@@ -774,6 +775,21 @@ int rb_amg_level_storage(rb_amg ml, int level, int* ndiag) {
         } else {
             const auto& V = ml->h.lv64[level];
             *ndiag = V.dia ? V.off.nd : 0;
+        }
+        return RB_OK;
+    });
+}
+
+int rb_amg_level_const_coef(rb_amg ml, int level, int* constant) {
+    return guarded([&]() -> int {
+        NEED(ml); NEED(constant);
+        RB_REQUIRE(level >= 0 && level < ml->h.num_levels(), "level out of range");
+        if (ml->h.opts.precision == RB_PREC_FP32) {
+            const auto& V = ml->h.lv32[level];
+            *constant = V.dia && V.off.mask ? 1 : 0;
+        } else {
+            const auto& V = ml->h.lv64[level];
+            *constant = V.dia && V.off.mask ? 1 : 0;
         }
         return RB_OK;
     });

@@ -58,13 +58,50 @@ constexpr int kMaxDiag = 32;
 #define RB_DIA_EPI_PREFETCH 1
 #endif
 
+// Offsets of the diagonals; with mask set, the operator has constant
+// coefficients: every nonzero of diagonal d equals c[d], and bit d of
+// mask[i] says whether a(i, i + o[d]) is nonzero.  The kernels then read 4
+// bytes a row instead of nd values (the stored values stay for the kernels
+// that do not take this form).  The same products in the same order: the
+// results are those of the stored values bit for bit.
 struct DiaOff {
     int nd;
     long long o[kMaxDiag];
+    const unsigned* mask;
+    double c[kMaxDiag];
+    float cf[kMaxDiag];   // c in FP32 (exact: an FP32 level's values are FP32)
 };
 
-// SC: the gathered vector is x_j * xs_j (the fused first sweep, spmv.cuh)
-template <int ND, typename TV, typename TX, typename Acc, bool SC = false>
+// *p through the read-only path when `on`, else 0, as one predicated load
+// (the compiler otherwise branches around each conditional load; a diagonal
+// a row, those branches saturated the SM's branch unit).  p is only formed,
+// never read, when `on` is false.
+__device__ __forceinline__ float ldg_if(const float* p, bool on) {
+    float v;
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\tmov.b32 %0, 0;\n\t"
+        "@q ld.global.nc.f32 %0, [%1];\n\t}"
+        : "=f"(v) : "l"(p), "r"((unsigned)on));
+    return v;
+}
+__device__ __forceinline__ double ldg_if(const double* p, bool on) {
+    double v;
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\tmov.b64 %0, 0;\n\t"
+        "@q ld.global.nc.f64 %0, [%1];\n\t}"
+        : "=d"(v) : "l"(p), "r"((unsigned)on));
+    return v;
+}
+
+// Coefficient d of a constant-coefficient operator in the value type TV (no
+// conversion instruction for FP32 levels).
+template <typename TV>
+__device__ __forceinline__ TV dia_coef(const DiaOff& off, int d) {
+    if constexpr (std::is_same<TV, float>::value) return off.cf[d];
+    else return (TV)off.c[d];
+}
+
+// SC: the gathered vector is x_j * xs_j (the fused first sweep, spmv.cuh);
+// CC: constant coefficients (off.mask, off.c; base unused)
+template <int ND, typename TV, typename TX, typename Acc, bool SC = false, bool CC = false>
 __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const TV* __restrict__ base,
                                         const TX* __restrict__ x,
                                         const TX* __restrict__ xs = nullptr) {
@@ -73,6 +110,32 @@ __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const
 #if RB_DIA_TWO_PHASE
         // all loads first (values, then the gathered x), then the products:
         // the warp keeps 2 ND loads in flight instead of waiting on each
+        if constexpr (CC) {
+            // a set mask bit implies 0 <= i + o[d] < n; a clear one is an entry
+            // that is zero, whose product c_d * 0 adds nothing, as 0 * x does
+            // FP32 vectors: one predicated load a diagonal (ldg_if).  FP64
+            // vectors keep the compiler's conditional loads: with 27
+            // predicated FP64 loads in flight the kernel spills (measured
+            // 0.184 against 0.129 ms for the outer A p at 192^3).
+            const unsigned m = i < n ? __ldg(off.mask + i) : 0u;
+            TX xv[ND];
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+                const bool on = (m >> d) & 1u;
+                if constexpr (sizeof(TX) == 4) {
+                    xv[d] = ldg_if(x + i + off.o[d], on);
+                    if constexpr (SC) xv[d] = (TX)(xv[d] * ldg_if(xs + i + off.o[d], on));
+                } else {
+                    xv[d] = on ? __ldg(x + i + off.o[d]) : TX(0);
+                    if constexpr (SC) xv[d] = on ? (TX)(xv[d] * __ldg(xs + i + off.o[d])) : TX(0);
+                }
+            }
+            // (the coefficient in the accumulation type: the FP32 value
+            // widened at setup, no conversion instruction a diagonal)
+#pragma unroll
+            for (int d = 0; d < ND; d++) s += dia_coef<Acc>(off, d) * (Acc)xv[d];
+            return s;
+        }
         TV v[ND];
         TX xv[ND];
 #pragma unroll
@@ -88,7 +151,7 @@ __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const
 #pragma unroll
         for (int d = 0; d < ND; d++) s += (Acc)v[d] * (Acc)xv[d];
 #else
-        static_assert(!SC, "scaled gathers need the two-phase row loop");
+        static_assert(!SC && !CC, "scaled gathers and constant coefficients need the two-phase row loop");
         TV v[ND];
 #pragma unroll
         for (int d = 0; d < ND; d++) v[d] = __ldg(base + d * 32);
@@ -99,6 +162,7 @@ __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const
         }
 #endif
     } else {
+        static_assert(!CC, "constant coefficients need a compiled diagonal count");
 #pragma unroll 4
         for (int d = 0; d < off.nd; d++) {
             const long j = i + off.o[d];
@@ -112,7 +176,7 @@ __device__ __forceinline__ Acc sdia_row(long i, long n, const DiaOff& off, const
     return s;
 }
 
-template <int ND, typename TV, typename TX, typename Acc, class Epi>
+template <int ND, typename TV, typename TX, typename Acc, class Epi, bool CC = false>
 __global__ void __launch_bounds__(256, RB_DIA_MINB_ROWS)
 k_sdia_rows(long n, DiaOff off, const TV* __restrict__ sv, const TX* __restrict__ x, Epi epi) {
     constexpr bool SC = ScaledGather<Epi>::value;
@@ -129,19 +193,21 @@ k_sdia_rows(long n, DiaOff off, const TV* __restrict__ sv, const TX* __restrict_
             // the epilogue's operands are loaded with the row's values and x
             typename Epi::Pre pr{};
             if (i < n) pr = epi.pre(i);
-            const Acc s = sdia_row<ND, TV, TX, Acc, SC>(i, n, off, sv + sl * nd * 32 + lane, x, xs);
+            const Acc s = sdia_row<ND, TV, TX, Acc, SC, CC>(i, n, off, sv + sl * nd * 32 + lane, x, xs);
             if (i < n) epi.post(i, s, red, pr);
         } else
 #endif
         {
-            const Acc s = sdia_row<ND, TV, TX, Acc, SC>(i, n, off, sv + sl * nd * 32 + lane, x, xs);
+            const Acc s = sdia_row<ND, TV, TX, Acc, SC, CC>(i, n, off, sv + sl * nd * 32 + lane, x, xs);
             if (i < n) epi(i, s, red);
         }
     }
 }
 
-template <int ND, typename TV, class Fin>
-__global__ void __launch_bounds__(256, RB_DIA_MINB)
+// (constant coefficients: 3 resident blocks, so that the 27 gathered FP64
+// values of a row fit the register budget without spilling)
+template <int ND, typename TV, class Fin, bool CC = false>
+__global__ void __launch_bounds__(256, CC ? 3 : RB_DIA_MINB)
 k_sdia_rows_dot(long n, DiaOff off, const TV* __restrict__ sv, const double* __restrict__ x,
                 EpiStoreDot epi, ReduceSlot rs, Fin fin) {
     const int lane = threadIdx.x & 31;
@@ -151,7 +217,7 @@ k_sdia_rows_dot(long n, DiaOff off, const TV* __restrict__ sv, const double* __r
     for (long sl = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < nslices;
          sl += ((long)gridDim.x * blockDim.x) >> 5) {
         const long i = (sl << 5) + lane;
-        const double s = sdia_row<ND, TV, double, double>(i, n, off, sv + sl * nd * 32 + lane, x);
+        const double s = sdia_row<ND, TV, double, double, false, CC>(i, n, off, sv + sl * nd * 32 + lane, x);
         if (i < n) epi(i, s, red);
     }
     block_reduce_finish(red, rs, fin);
@@ -172,6 +238,16 @@ void launch_dia(const DiaOff& off, const TV* sv, long n, const TX* x, Epi epi) {
     if (n <= 0) return;
     using Acc = AccOf2<TV, TX>;
     const unsigned g = dia_grid(n, false);
+    if (off.mask) {
+        switch (off.nd) {
+            case 5: k_sdia_rows<5, TV, TX, Acc, Epi, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;
+            case 7: k_sdia_rows<7, TV, TX, Acc, Epi, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;
+            case 9: k_sdia_rows<9, TV, TX, Acc, Epi, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;
+            default: k_sdia_rows<27, TV, TX, Acc, Epi, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;
+        }
+        RB_CHECK_LAUNCH();
+        return;
+    }
     switch (off.nd) {
         case 5: k_sdia_rows<5, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;
         case 7: k_sdia_rows<7, TV, TX, Acc, Epi><<<g, 256, 0, stream()>>>(n, off, sv, x, epi); break;
@@ -187,6 +263,16 @@ void launch_dia_dot(const DiaOff& off, const TV* sv, long n, const double* x, do
     const unsigned g = dia_grid(n, true);
     ReduceSlot rs = global_reduce_slot(g);
     EpiStoreDot epi{x, y};
+    if (off.mask) {
+        switch (off.nd) {
+            case 5: k_sdia_rows_dot<5, TV, Fin, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi, rs, fin); break;
+            case 7: k_sdia_rows_dot<7, TV, Fin, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi, rs, fin); break;
+            case 9: k_sdia_rows_dot<9, TV, Fin, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi, rs, fin); break;
+            default: k_sdia_rows_dot<27, TV, Fin, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi, rs, fin); break;
+        }
+        RB_CHECK_LAUNCH();
+        return;
+    }
     switch (off.nd) {
         case 5: k_sdia_rows_dot<5, TV><<<g, 256, 0, stream()>>>(n, off, sv, x, epi, rs, fin); break;
         case 7: k_sdia_rows_dot<7, TV><<<g, 256, 0, stream()>>>(n, off, sv, x, epi, rs, fin); break;
@@ -195,6 +281,36 @@ void launch_dia_dot(const DiaOff& off, const TV* sv, long n, const double* x, do
         default: k_sdia_rows_dot<0, TV><<<g, 256, 0, stream()>>>(n, off, sv, x, epi, rs, fin); break;
     }
     RB_CHECK_LAUNCH();
+}
+
+// Whether every nonzero stored on diagonal d has one value: lo/hi[d] end as
+// the least and greatest bit pattern (as FP64) of its nonzeros.
+template <typename T>
+__global__ void k_dia_const_range(long n, int nd, const T* __restrict__ dv,
+                                  unsigned long long* lo, unsigned long long* hi) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T* base = dv + (i >> 5) * nd * 32 + (i & 31);
+    for (int d = 0; d < nd; d++) {
+        const T v = base[d * 32];
+        if (v != T(0)) {
+            const unsigned long long b = (unsigned long long)__double_as_longlong((double)v);
+            atomicMin(lo + d, b);
+            atomicMax(hi + d, b);
+        }
+    }
+}
+
+// bit d of mask[i]: a(i, i + o[d]) is nonzero
+template <typename T>
+__global__ void k_dia_mask(long n, int nd, const T* __restrict__ dv, unsigned* __restrict__ mask) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T* base = dv + (i >> 5) * nd * 32 + (i & 31);
+    unsigned m = 0u;
+    for (int d = 0; d < nd; d++)
+        if (base[d * 32] != T(0)) m |= 1u << d;
+    mask[i] = m;
 }
 
 // Sliced storage size (entries) for n rows and nd diagonals.

@@ -8,6 +8,7 @@
 // l1 row norms, a multicolour row ordering for the Gauss-Seidel stand-in, the
 // row-kernel width chosen by timing, and the LU of A_c^T.
 #include <algorithm>
+#include <cstring>
 #include <climits>
 #include <chrono>
 #include <cmath>
@@ -442,14 +443,58 @@ static DiaOff find_diagonals(const rb_csr_s& M) {
     return off;
 }
 
+// The constant-coefficient form of V's diagonals (DiaOff::mask) when every
+// diagonal holds one nonzero value (a constant-coefficient stencil, as every
+// stencil_grid operator is): the kernels then read a 4-byte mask a row in
+// place of nd values.  allow = rb_amg_opts::const_coef;
+// RAPTOR_B200_CONST_DIA=0 keeps the stored values in every hierarchy.
 template <typename T>
-static void build_dia(Level<T>& V, const rb_csr_s& M, const DiaOff& off) {
+static void const_dia(Level<T>& V, bool allow) {
+    V.off.mask = nullptr;
+    V.dmask.release();
+    const int nd = V.off.nd;
+    static const bool disabled = [] {
+        const char* e = getenv("RAPTOR_B200_CONST_DIA");
+        return e && e[0] == '0';
+    }();
+    if (!allow || disabled || V.n <= 0 || !(nd == 5 || nd == 7 || nd == 9 || nd == 27)) return;
+    DevArray<unsigned long long> lo((size_t)nd), hi((size_t)nd);
+    RB_CUDA(cudaMemsetAsync(lo.get(), 0xff, sizeof(unsigned long long) * nd, stream()));
+    hi.zero();
+    k_dia_const_range<T><<<grid_for(V.n, 256), 256, 0, stream()>>>(V.n, nd, V.Adia.get(), lo.get(),
+                                                                   hi.get());
+    RB_CHECK_LAUNCH();
+    std::vector<unsigned long long> l = lo.to_host(), h = hi.to_host();
+    double c[kMaxDiag];
+    for (int d = 0; d < nd; d++) {
+        if (l[d] == ~0ull && h[d] == 0ull) {
+            c[d] = 0.0;   // no nonzero on this diagonal
+        } else if (l[d] != h[d]) {
+            return;       // two different values: not constant
+        } else {
+            long long b = (long long)l[d];
+            std::memcpy(&c[d], &b, sizeof(double));
+        }
+    }
+    for (int d = 0; d < nd; d++) {
+        V.off.c[d] = c[d];
+        V.off.cf[d] = (float)c[d];
+    }
+    V.dmask.alloc((size_t)V.n);
+    k_dia_mask<T><<<grid_for(V.n, 256), 256, 0, stream()>>>(V.n, nd, V.Adia.get(), V.dmask.get());
+    RB_CHECK_LAUNCH();
+    V.off.mask = V.dmask.get();
+}
+
+template <typename T>
+static void build_dia(Level<T>& V, const rb_csr_s& M, const DiaOff& off, bool const_coef) {
     V.off = off;
     V.Adia.alloc(sdia_size(V.n, off.nd));
     V.Adia.zero();
     k_csr_to_dia<T><<<grid_for(V.n, 256), 256, 0, stream()>>>(V.n, M.rowptr.get(), M.cols.get(),
                                                               M.vals.get(), off, V.Adia.get());
     RB_CHECK_LAUNCH();
+    const_dia(V, const_coef);
 }
 
 // ------------------------------------------------------------------ setup --
@@ -581,7 +626,7 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
         V.gA = autotune_group(V.A, V.x.get(), V.r.get(), "A", strided_only);
         const DiaOff off = strided_only ? DiaOff{} : find_diagonals(*master[l].A);
         if (off.nd > 0) {
-            build_dia(V, *master[l].A, off);
+            build_dia(V, *master[l].A, off, opts.const_coef != 0);
             const std::string key = tune_key("A_dia", V.n, V.A.nnz, (int)sizeof(T));
             auto& c = tune_cache();
             auto it = c.m.find(key);
@@ -600,7 +645,11 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
                 c.m[key] = V.dia ? 1 : 0;
                 tune_save();
             }
-            if (!V.dia) V.Adia.release();
+            if (!V.dia) {
+                V.Adia.release();
+                V.dmask.release();
+                V.off.mask = nullptr;
+            }
         }
         if (l < L - 1) {
             V.gP = autotune_group(V.P, lv[l + 1].x.get(), V.xt.get(), "P", strided_only);
@@ -694,7 +743,7 @@ void Hierarchy::build_cycle_data() {
         a0_64.Adia.release();
         if (!a0_fp32_exact && lv32[0].dia) {
             a0_64.n = A0.n_rows;
-            build_dia(a0_64, A0, lv32[0].off);
+            build_dia(a0_64, A0, lv32[0].off, opts.const_coef != 0);
             a0_64.dia = true;
         }
     } else {

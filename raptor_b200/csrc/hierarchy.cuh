@@ -123,6 +123,7 @@ struct Level {
     bool fuse_first = false;           // first sweep fused with the residual (timed pick)
     DiaOff off{};
     DevArray<T> Adia;
+    DevArray<unsigned> dmask;          // constant-coefficient form (DiaOff::mask)
     void alloc_vectors();
 
     // y-epilogue over the rows of A_l times x, in whichever format was picked
