@@ -131,6 +131,11 @@ int rb_mm_write_host(const char* path, int n_rows, int n_cols, int64_t nnz, cons
 #define RB_INTERP_DIRECT 0       /* interp_t Direct (core/types.hpp:161) */
 #define RB_INTERP_MODCLASSICAL 1 /* interp_t ModClassical */
 #define RB_INTERP_EXTENDED 2     /* interp_t Extended */
+#define RB_COARSEN_RS 0          /* coarsen_t RS (core/types.hpp:160) */
+#define RB_COARSEN_CLJP 1        /* coarsen_t CLJP */
+#define RB_COARSEN_FALGOUT 2     /* coarsen_t Falgout */
+#define RB_COARSEN_PMIS 3        /* coarsen_t PMIS */
+#define RB_COARSEN_HMIS 4        /* coarsen_t HMIS */
 
 /* ParCSRMatrix::strength (par_strength.cpp:536-546 -> :8-339 / :342-531).
  * A must have its diagonal first (rb_csr_sort_diag_first). */
@@ -138,6 +143,14 @@ int rb_strength(rb_csr A, int kind, double theta, rb_csr* S);
 /* split_pmis (ruge_stuben/par_cf_splitting.cpp:75-89, 1229-1381); weights has
  * n_rows entries; states (host, n_rows) receive 1 = C, 0 = F, -2 = isolated. */
 int rb_split_pmis(rb_csr S, const double* weights, int* states);
+/* The C/F splittings at one rank (par_cf_splitting.cpp): split_rs (:7-30,
+ * the Ruge-Stuben passes of cf_splitting.cpp:9-328, run on the host),
+ * split_cljp (:32-48, 1383-1607), split_falgout (:50-73), split_pmis
+ * (:75-89), split_hmis (:91-112), chosen by kind = RB_COARSEN_*.  weights
+ * (n_rows, or NULL for the reference's glibc rand() weights) are used by the
+ * CLJP and PMIS loops; states (host, n_rows) receive 1 = C, 0 = F, -2 =
+ * isolated. */
+int rb_split(rb_csr S, int kind, const double* weights, int* states);
 /* mod_classical_interpolation (par_interpolation.cpp:991-1451) and
  * extended_interpolation + filter_interp (:280-989, :175-278). */
 int rb_interpolation(rb_csr A, rb_csr S, const int* states, int kind, double filter,
@@ -207,6 +220,8 @@ typedef struct rb_amg_opts {
     int const_coef;           /* 1 (default): a diagonal-storage level whose diagonals each hold one
                                  value is read as a mask a row plus those values (same results);
                                  0: the stored values */
+    int coarsen_type;         /* RB_COARSEN_* (RS solver): PMIS (default), RS, CLJP, Falgout, HMIS
+                                 (par_ruge_stuben_solver.hpp:75-104; RS uses Falgout from level 3) */
 } rb_amg_opts;
 
 void rb_amg_default_opts(rb_amg_opts* opts);

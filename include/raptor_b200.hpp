@@ -219,14 +219,14 @@ class ParMultilevel {
 /* ruge_stuben/par_ruge_stuben_solver.hpp:24 */
 class ParRugeStubenSolver : public ParMultilevel {
   public:
-    ParRugeStubenSolver(double strong_threshold = 0.0, coarsen_t coarsen_type = PMIS,
+    ParRugeStubenSolver(double strong_threshold = 0.0, coarsen_t coarsen_type = RS,
                         interp_t interp_type = Direct, strength_t strength_type = Classical,
                         relax_t relax_type = SOR)
         : ParMultilevel(strong_threshold, strength_type, relax_type) {
-        if (coarsen_type != PMIS) throw error(RB_ERR_INVALID, "raptor_b200: only PMIS coarsening");
         if (interp_type != Direct && interp_type != ModClassical && interp_type != Extended)
             throw error(RB_ERR_INVALID, "raptor_b200: interpolation is Direct, ModClassical or Extended");
         opts.solver = RB_SOLVER_RS;
+        opts.coarsen_type = (int)coarsen_type;
         opts.interp_type = interp_type;
     }
     double& interp_filter = opts.interp_filter;

@@ -24,7 +24,7 @@ from ._capi import (AmgOpts, Breakdown, NotConverged, RaptorError, check, lib,  
 
 # enums (core/types.hpp:158-164) --------------------------------------------
 Classical, Symmetric = 0, 1                 # strength_t
-RS, CLJP, Falgout, PMIS, HMIS = 0, 1, 2, 3, 4   # coarsen_t (PMIS is built)
+RS, CLJP, Falgout, PMIS, HMIS = 0, 1, 2, 3, 4   # coarsen_t
 Direct, ModClassical, Extended = 0, 1, 2    # interp_t
 Jacobi, SOR, SSOR, L1Jacobi = 0, 1, 2, 3    # relax_t (+ L1-Jacobi)
 MIS = 0                                     # agg_t
@@ -287,6 +287,32 @@ def split_pmis(S, weights=None):
     return st[:n]
 
 
+def split(S, coarsen_type, weights=None):
+    """The C/F splittings at one rank (split_rs, split_cljp, split_falgout,
+    split_pmis, split_hmis of par_cf_splitting.cpp), by coarsen_t."""
+    n = S.global_num_rows
+    st = np.zeros(max(n, 1), np.int32)
+    w = None if weights is None else np.ascontiguousarray(weights[:n], np.float64)
+    check(lib().rb_split(S.h, int(coarsen_type), _ptr(w) if w is not None else None, st))
+    return st[:n]
+
+
+def split_rs(S):
+    return split(S, RS)
+
+
+def split_cljp(S, weights=None):
+    return split(S, CLJP, weights)
+
+
+def split_falgout(S, weights=None):
+    return split(S, Falgout, weights)
+
+
+def split_hmis(S, weights=None):
+    return split(S, HMIS, weights)
+
+
 def interpolation(A, S, states, interp_type=ModClassical, filter_threshold=0.0):
     h = C.c_void_p()
     st = np.ascontiguousarray(states, np.int32)
@@ -358,7 +384,7 @@ class ParMultilevel:
     _FIELDS = ("strong_threshold", "relax_weight", "num_smooth_sweeps", "max_coarse",
                "max_levels", "max_iterations", "solve_tol", "interp_filter")
     _EXTRA = ("precision", "jacobi_compat", "seed_offset", "relax_type", "strength_type",
-              "interp_type", "fuse_coarse", "use_graphs", "const_coef", "prolong_weight",
+              "interp_type", "fuse_coarse", "use_graphs", "const_coef", "coarsen_type", "prolong_weight",
               "prolong_smooth_steps", "solver")
 
     def __init__(self, strong_threshold=0.0, strength_type=Classical, relax_type=SOR):
@@ -513,11 +539,12 @@ class ParMultilevel:
 class ParRugeStubenSolver(ParMultilevel):
     """ParRugeStubenSolver (ruge_stuben/par_ruge_stuben_solver.hpp:12-170)."""
 
-    def __init__(self, strong_threshold=0.0, coarsen_type=PMIS, interp_type=Direct,
+    def __init__(self, strong_threshold=0.0, coarsen_type=RS, interp_type=Direct,
                  strength_type=Classical, relax_type=SOR):
         super().__init__(strong_threshold, strength_type, relax_type)
-        if coarsen_type != PMIS:
-            raise RaptorError(-1, "only PMIS coarsening is built")
+        if coarsen_type not in (RS, CLJP, Falgout, PMIS, HMIS):
+            raise RaptorError(-1, "coarsening must be RS, CLJP, Falgout, PMIS or HMIS")
+        self.opts.coarsen_type = coarsen_type
         if interp_type not in (Direct, ModClassical, Extended):
             raise RaptorError(-1, "interpolation must be Direct, ModClassical or Extended")
         self.opts.interp_type = interp_type

@@ -41,6 +41,7 @@ class AmgOpts(C.Structure):
         ("prolong_weight", C.c_double), ("prolong_smooth_steps", C.c_int),
         ("precision", C.c_int), ("jacobi_compat", C.c_int), ("seed_offset", C.c_int),
         ("fuse_coarse", C.c_int), ("use_graphs", C.c_int), ("const_coef", C.c_int),
+        ("coarsen_type", C.c_int),
     ]
 
 
@@ -94,6 +95,7 @@ SIGNATURES = {
                                    C.c_void_p, C.c_void_p]),
     "rb_strength": (C.c_int, [_P, C.c_int, C.c_double, _PP]),
     "rb_split_pmis": (C.c_int, [_P, _P, _I]),
+    "rb_split": (C.c_int, [_P, C.c_int, _P, _I]),
     "rb_interpolation": (C.c_int, [_P, _P, _I, C.c_int, C.c_double, _PP]),
     "rb_mis2": (C.c_int, [_P, _P, _I]),
     "rb_aggregate": (C.c_int, [_P, _P, _I, _P, _I, C.POINTER(C.c_int)]),

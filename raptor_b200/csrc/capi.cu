@@ -497,6 +497,34 @@ int rb_split_pmis(rb_csr S, const double* weights, int* states) {
     });
 }
 
+int rb_split(rb_csr S, int kind, const double* weights, int* states) {
+    return guarded([&]() -> int {
+        NEED(S); NEED(states);
+        RB_REQUIRE(kind >= RB_COARSEN_RS && kind <= RB_COARSEN_HMIS, "unknown coarsening kind");
+        const int n = S->n_rows;
+        std::vector<double> w = weights ? std::vector<double>(weights, weights + n) : rand_weights(n, 0);
+        DevArray<double> wd((size_t)std::max(n, 1));
+        wd.upload(w.data(), n);
+        DevArray<int> st((size_t)std::max(n, 1));
+        switch (kind) {
+            case RB_COARSEN_RS: split_rs(*S, st.get(), true); break;
+            case RB_COARSEN_CLJP: split_cljp(*S, wd.get(), st.get(), false); break;
+            case RB_COARSEN_FALGOUT:
+                split_rs(*S, st.get(), true);
+                split_cljp(*S, wd.get(), st.get(), true);
+                break;
+            case RB_COARSEN_HMIS:
+                split_rs(*S, st.get(), false);
+                split_pmis(*S, wd.get(), st.get(), true);
+                break;
+            default: split_pmis(*S, wd.get(), st.get()); break;
+        }
+        st.download(states, n);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
 int rb_interpolation(rb_csr A, rb_csr S, const int* states, int kind, double filter, rb_csr* P) {
     return guarded([&]() -> int {
         NEED(A); NEED(S); NEED(states); NEED(P);
@@ -612,6 +640,7 @@ void rb_amg_default_opts(rb_amg_opts* o) {
     o->fuse_coarse = 1;
     o->use_graphs = 1;
     o->const_coef = 1;
+    o->coarsen_type = RB_COARSEN_PMIS;
 }
 
 int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_amg* out) {
@@ -632,6 +661,8 @@ int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_am
                        o.relax_type == RB_RELAX_SSOR || o.relax_type == RB_RELAX_L1JACOBI,
                    "unknown relaxation type");
         RB_REQUIRE(o.precision == RB_PREC_FP64 || o.precision == RB_PREC_FP32, "unknown precision");
+        RB_REQUIRE(o.coarsen_type >= RB_COARSEN_RS && o.coarsen_type <= RB_COARSEN_HMIS,
+                   "unknown coarsening type");
         RB_REQUIRE(o.prolong_smooth_steps >= 0, "prolong_smooth_steps < 0");
         RB_REQUIRE(o.num_smooth_sweeps >= 0, "num_smooth_sweeps < 0");
         RB_REQUIRE(o.max_levels >= 1 && o.max_coarse >= 1, "max_levels and max_coarse must be >= 1");

@@ -556,7 +556,31 @@ void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* we
             L.P.reset(jacobi_prolongation(A, *T, o.prolong_weight, o.prolong_smooth_steps));
             cand = std::move(R);
         } else {
-            split_pmis(*S, wdev.get(), L.states.get());
+            // C/F splitting (par_ruge_stuben_solver.hpp:75-104); at one rank
+            // Falgout and HMIS are the Ruge-Stuben passes followed by a CLJP
+            // / PMIS loop over whatever is left unassigned
+            const int lvl = (int)master.size() - 1;
+            int* st = L.states.get();
+            switch (o.coarsen_type) {
+                case RB_COARSEN_RS:
+                    split_rs(*S, st, true);
+                    if (lvl >= 3) split_cljp(*S, wdev.get(), st, true);   // Falgout below level 3
+                    break;
+                case RB_COARSEN_CLJP:
+                    split_cljp(*S, wdev.get(), st, false);
+                    break;
+                case RB_COARSEN_FALGOUT:
+                    split_rs(*S, st, true);
+                    split_cljp(*S, wdev.get(), st, true);
+                    break;
+                case RB_COARSEN_HMIS:
+                    split_rs(*S, st, false);
+                    split_pmis(*S, wdev.get(), st, true);
+                    break;
+                default:
+                    split_pmis(*S, wdev.get(), st);
+                    break;
+            }
             L.P.reset(interpolation(A, *S, L.states.get(), o.interp_type, o.interp_filter));
         }
         S.reset();

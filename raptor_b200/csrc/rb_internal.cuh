@@ -89,7 +89,14 @@ void spmv_T64(rb_csr_s& A, const double* x, double* y);
 
 // Setup components (setup.cu).
 rb_csr_s* strength(const rb_csr_s& A, int kind, double theta);
-void split_pmis(const rb_csr_s& S, const double* weights_dev, int* states_dev);
+// keep_states: the states are already set (HMIS / Falgout after the
+// Ruge-Stuben passes); otherwise set_initial_states first.
+void split_pmis(const rb_csr_s& S, const double* weights_dev, int* states_dev,
+                bool keep_states = false);
+void split_cljp(const rb_csr_s& S, const double* weights_dev, int* states_dev,
+                bool keep_states = false);
+// Ruge-Stuben first pass (and second pass) on the host (coarsen_rs.cu).
+void split_rs(const rb_csr_s& S, int* states_dev, bool second_pass);
 rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* states_dev, int kind,
                         double filter);
 rb_csr_s* spgemm(const rb_csr_s& A, const rb_csr_s& B);

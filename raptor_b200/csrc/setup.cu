@@ -245,21 +245,72 @@ __global__ void k_pmis_update(int n, double* w, int* st, int* remaining) {
     if (threadIdx.x == 0 && keep) atomicAdd(remaining, keep);
 }
 
-void split_pmis(const rb_csr_s& S, const double* weights_dev, int* states_dev) {
+// pmis_main_loop's start when the states are already set (HMIS after the
+// Ruge-Stuben first pass, par_cf_splitting.cpp:1272-1306): the unassigned
+// rows that depend on a selected row become unselected, then the weight
+// filter; each influence adds 1.0 in sequence, as in k_pmis_init.
+__global__ void k_pmis_keep_mark(int n, const int* __restrict__ tp, const int* __restrict__ tci,
+                                 int* st) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || st[c] != kSelected) return;
+    for (int j = tp[c]; j < tp[c + 1]; j++)
+        if (st[tci[j]] == kUnassigned) st[tci[j]] = kUnselected;
+}
+
+__global__ void k_pmis_keep_init(int n, const int* __restrict__ tp, const double* __restrict__ rnd,
+                                 double* w, int* st) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double wi = rnd[i];
+    for (int k = tp[i]; k < tp[i + 1]; k++) wi = dadd(wi, 1.0);
+    if (st[i] == kUnassigned && wi < 1) { st[i] = kUnselected; wi = 0.0; }
+    else if (st[i] != kUnassigned) wi = 0.0;
+    w[i] = wi;
+}
+
+__global__ void k_fill_ones(long long n, int* p) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = 1;
+}
+
+__global__ void k_count_state(int n, const int* __restrict__ st, int want, int* count) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int hit = i < n && st[i] == want;
+    hit = __syncthreads_count(hit);
+    if (threadIdx.x == 0 && hit) atomicAdd(count, hit);
+}
+
+// Off-diagonal column lists of S (tp, tci).
+static void s_transpose(const rb_csr_s& S, DevArray<int>& tp, DevArray<int>& tci) {
     const int n = S.n_rows;
-    if (n == 0) return;
     const unsigned g = grid_for(n, 256);
-    DevArray<int> cnt((size_t)n + 1), tp((size_t)n + 1);
+    DevArray<int> cnt((size_t)n + 1);
+    tp.alloc((size_t)n + 1);
     cnt.zero();
     k_s_colcount<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), cnt.get());
     RB_CHECK_LAUNCH();
     long long tn = exclusive_scan(cnt.get(), tp.get(), n);
-    DevArray<int> tci((size_t)std::max(tn, 1LL));
+    tci.alloc((size_t)std::max(tn, 1LL));
     RB_CUDA(cudaMemcpyAsync(cnt.get(), tp.get(), sizeof(int) * n, cudaMemcpyDeviceToDevice, stream()));
     k_s_colfill<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), cnt.get(), tci.get());
     RB_CHECK_LAUNCH();
+}
+
+void split_pmis(const rb_csr_s& S, const double* weights_dev, int* states_dev, bool keep_states) {
+    const int n = S.n_rows;
+    if (n == 0) return;
+    const unsigned g = grid_for(n, 256);
+    DevArray<int> tp, tci;
+    s_transpose(S, tp, tci);
     DevArray<double> w((size_t)n);
-    k_pmis_init<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), tp.get(), weights_dev, w.get(), states_dev);
+    if (keep_states) {
+        k_pmis_keep_mark<<<g, 256, 0, stream()>>>(n, tp.get(), tci.get(), states_dev);
+        RB_CHECK_LAUNCH();
+        k_pmis_keep_init<<<g, 256, 0, stream()>>>(n, tp.get(), weights_dev, w.get(), states_dev);
+    } else {
+        k_pmis_init<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), tp.get(), weights_dev, w.get(),
+                                             states_dev);
+    }
     RB_CHECK_LAUNCH();
     DevArray<int> rem(1);
     for (int round = 0; round < 100000; round++) {
@@ -272,6 +323,117 @@ void split_pmis(const rb_csr_s& S, const double* weights_dev, int* states_dev) {
         if (read_scalar(rem.get()) == 0) return;
     }
     throw Error(RB_ERR_INVALID, "PMIS did not terminate");
+}
+
+// ================================================================ CLJP ===
+// split_cljp / cljp_main_loop at one rank (par_cf_splitting.cpp:32-48,
+// 246-309, 403-660, 1200-1227, 1383-1607).  A round selects the unassigned
+// rows whose weight no strong neighbour (either direction) exceeds (the
+// PMIS selection, k_pmis_select), then removes edges: for every new C point
+// c, the edge from each unassigned row of c's row (c depends on it), and the
+// edge i -> k between two rows that both depend on c (k unassigned, i not an
+// old C point), each removal taking 1.0 off the weight of the row at its
+// head; rows whose weight falls below 1 become F points.  Each edge is
+// removed at most once (its mark is claimed atomically), and every removal
+// subtracts the same 1.0, so the weights, and hence the rounds, do not
+// depend on the order the C points are visited in: they are those of the
+// reference's sequential loops.
+
+// set_initial_states (:114-131) + initial_weights (:246-309); keep: the
+// states are already set (Falgout after Ruge-Stuben), only their weights
+// are zeroed.
+__global__ void k_cljp_init(int n, const int* __restrict__ rp, const int* __restrict__ tp,
+                            const double* __restrict__ rnd, double* w, int* st, int keep) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int state = keep ? st[i] : ((rp[i + 1] - rp[i] > 1) ? kUnassigned : kNoNeighbors);
+    double wi = rnd[i];
+    for (int k = tp[i]; k < tp[i + 1]; k++) wi = dadd(wi, 1.0);
+    w[i] = state == kUnassigned ? wi : 0.0;
+    st[i] = state;
+}
+
+// update_row_weights (:497-542): the edges of the C points' own rows
+__global__ void k_cljp_row_edges(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                 const int* __restrict__ st, int want, int* edge, double* w) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || st[c] != want) return;
+    int s = rp[c], e = rp[c + 1];
+    if (s < e && ci[s] == c) s++;
+    for (int j = s; j < e; j++) {
+        const int idx = ci[j];
+        if (st[idx] == kUnassigned && edge[j]) {
+            edge[j] = 0;
+            atomicAdd(w + idx, -1.0);
+        }
+    }
+}
+
+// update_local_dist2_weights (:544-660): for a C point c, the edges i -> k
+// with both i and k depending on c (k unassigned, i not an old C point)
+__global__ void k_cljp_dist2_edges(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                   const int* __restrict__ tp, const int* __restrict__ tci,
+                                   const int* __restrict__ st, int want, int* edge, double* w) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || st[c] != want) return;
+    for (int jj = tp[c]; jj < tp[c + 1]; jj++) {
+        const int idx = tci[jj];
+        if (st[idx] == kSelected) continue;
+        int s = rp[idx], e = rp[idx + 1];
+        if (s < e && ci[s] == idx) s++;
+        for (int k = s; k < e; k++) {
+            const int idk = ci[k];
+            if (st[idk] != kUnassigned || !edge[k]) continue;
+            // does idk depend on c (c in idk's row, diagonal excluded)?
+            int s2 = rp[idk], e2 = rp[idk + 1];
+            if (s2 < e2 && ci[s2] == idk) s2++;
+            bool dep = false;
+            for (int q = s2; q < e2 && !dep; q++) dep = ci[q] == c;
+            if (dep && atomicExch(edge + k, 0) == 1) atomicAdd(w + idk, -1.0);
+        }
+    }
+}
+
+void split_cljp(const rb_csr_s& S, const double* weights_dev, int* states_dev, bool keep_states) {
+    const int n = S.n_rows;
+    if (n == 0) return;
+    const unsigned g = grid_for(n, 256);
+    DevArray<int> tp, tci;
+    s_transpose(S, tp, tci);
+    DevArray<int> edge((size_t)std::max<long long>(S.nnz, 1));
+    k_fill_ones<<<grid_for(std::max<long long>(S.nnz, 1), 256), 256, 0, stream()>>>(
+        std::max<long long>(S.nnz, 1), edge.get());
+    RB_CHECK_LAUNCH();
+    DevArray<double> w((size_t)n);
+    k_cljp_init<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), tp.get(), weights_dev, w.get(),
+                                         states_dev, keep_states ? 1 : 0);
+    RB_CHECK_LAUNCH();
+    auto remove_edges = [&](int want) {
+        k_cljp_row_edges<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), states_dev,
+                                                  want, edge.get(), w.get());
+        RB_CHECK_LAUNCH();
+        k_cljp_dist2_edges<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), tp.get(),
+                                                    tci.get(), states_dev, want, edge.get(),
+                                                    w.get());
+        RB_CHECK_LAUNCH();
+    };
+    // C points already set (Falgout) remove their edges before the loop
+    if (keep_states) remove_edges(kSelected);
+    DevArray<int> rem(1);
+    for (int round = 0; round < 100000; round++) {
+        rem.zero();
+        k_count_state<<<g, 256, 0, stream()>>>(n, states_dev, kUnassigned, rem.get());
+        RB_CHECK_LAUNCH();
+        if (read_scalar(rem.get()) == 0) return;
+        rem.zero();
+        k_pmis_select<<<g, 256, 0, stream()>>>(n, S.rowptr.get(), S.cols.get(), tp.get(), tci.get(),
+                                               w.get(), states_dev);
+        RB_CHECK_LAUNCH();
+        remove_edges(kNewSelection);
+        k_pmis_update<<<g, 256, 0, stream()>>>(n, w.get(), states_dev, rem.get());
+        RB_CHECK_LAUNCH();
+    }
+    throw Error(RB_ERR_INVALID, "CLJP did not terminate");
 }
 
 // ======================================================= interpolation ===

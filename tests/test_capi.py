@@ -62,10 +62,14 @@ def test_default_opts_mirror_reference_defaults():
     assert ml.interp_type == rb.Extended
 
 
-def test_unbuilt_coarsenings_are_rejected():
+def test_unknown_coarsening_is_rejected():
     import raptor_b200 as rb
     with pytest.raises(rb.RaptorError):
-        rb.ParRugeStubenSolver(0.25, rb.CLJP, rb.ModClassical)
+        rb.ParRugeStubenSolver(0.25, 7, rb.ModClassical)
+    ml = rb.ParRugeStubenSolver(0.25, rb.CLJP, rb.ModClassical)
+    assert ml.coarsen_type == rb.CLJP
+    # the reference's default coarsening is Ruge-Stuben
+    assert rb.ParRugeStubenSolver().coarsen_type == rb.RS
 
 
 @pytest.mark.parametrize("field,value,message", [
@@ -73,6 +77,7 @@ def test_unbuilt_coarsenings_are_rejected():
     ("strength_type", 5, "strength"),
     ("relax_type", 9, "relaxation"),
     ("precision", 2, "precision"),
+    ("coarsen_type", 9, "coarsening"),
     ("max_levels", 0, "max_levels"),
     ("solver", 7, "solver"),
 ])
