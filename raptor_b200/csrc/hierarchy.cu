@@ -461,8 +461,8 @@ static void const_dia(Level<T>& V, bool allow) {
     DevArray<unsigned long long> lo((size_t)nd), hi((size_t)nd);
     RB_CUDA(cudaMemsetAsync(lo.get(), 0xff, sizeof(unsigned long long) * nd, stream()));
     hi.zero();
-    k_dia_const_range<T><<<grid_for(V.n, 256), 256, 0, stream()>>>(V.n, nd, V.Adia.get(), lo.get(),
-                                                                   hi.get());
+    k_dia_const_range<T><<<std::min<unsigned>(grid_for(V.n, 256), sm_count() * 4), 256, 0,
+                           stream()>>>(V.n, nd, V.Adia.get(), lo.get(), hi.get());
     RB_CHECK_LAUNCH();
     std::vector<unsigned long long> l = lo.to_host(), h = hi.to_host();
     double c[kMaxDiag];
