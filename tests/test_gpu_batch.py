@@ -150,3 +150,25 @@ def test_batch_stopped_systems_left_alone(prec):
         assert abs(int(iters[s]) - (len(res) - 1)) <= 1, (s, iters[s], len(res) - 1)
         ref = xs.numpy()
         assert np.linalg.norm(got[lo:hi] - ref) <= 1e-6 * np.linalg.norm(ref), s
+
+
+def test_batch_pcg_matches_oracle_pcg():
+    """Every system of a batch solve against the CPU restatement's own PCG
+    (true-residual mode) on the hierarchy the restatement builds for it: the
+    iterations (within one) and the solution (within 1e-6)."""
+    mats = systems(13, 5)
+    B = rb.Batch(mats, make_ml("rs", rb.FP64))
+    bh = np.random.default_rng(17).uniform(-1, 1, B.total_rows)
+    x = rb.ParVector(B.total_rows)
+    rc, iters, relres = B.pcg(x, rb.ParVector(B.total_rows, values=bh), tol=1e-8, max_iter=400)
+    assert rc == 0
+    got = x.numpy()
+    for s, A in enumerate(mats):
+        lo, hi = B.offsets[s], B.offsets[s + 1]
+        n = hi - lo
+        rp, ci, cv = A.arrays()
+        Ao = O.CSR.from_arrays(n, n, rp, ci, cv)
+        om = O.Hierarchy(Ao, interp="mod_classical", relax="l1_jacobi")
+        xo, ho, _ = O.pcg(Ao, om, np.zeros(n), bh[lo:hi], tol=1e-8, max_iter=400, mode=1)
+        assert abs(int(iters[s]) - (len(ho) - 1)) <= 1, (s, iters[s], len(ho) - 1)
+        assert np.linalg.norm(got[lo:hi] - xo) <= 1e-6 * np.linalg.norm(xo), s

@@ -118,3 +118,26 @@ def test_block_path_rejects_sor_smoothing():
     ml = make_ml(A, "rs", rb.FP64, relax=rb.SOR)
     with pytest.raises(rb.RaptorError):
         rb.PCG_block(A, ml, rb.ParVector(n * 4), rb.ParVector(n * 4, values=np.ones(n * 4)), 4)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_block_pcg_columns_match_oracle_pcg(prec):
+    """Each column of a block solve against the CPU restatement's own PCG
+    (true-residual mode) on the same hierarchy, which the restatement builds
+    itself: the iterations of the restatement's solve (within one) and its
+    solution (within 1e-6)."""
+    Ao = lap27(14)
+    A = to_rb(Ao)
+    n = Ao.shape[0]
+    ml = make_ml(A, "rs", prec)
+    om = O.Hierarchy(Ao, interp="extended", interp_filter=0.3, relax="l1_jacobi")
+    k = 4
+    Bh = np.random.default_rng(41).uniform(-1, 1, (n, k))
+    Xb = rb.ParVector(n * k)
+    rc, iters, relres = rb.PCG_block(A, ml, Xb, block(Bh), k, tol=1e-8, max_iter=300)
+    assert rc == 0
+    X = Xb.numpy().reshape(n, k)
+    for c in range(k):
+        xo, ho, _ = O.pcg(Ao, om, np.zeros(n), Bh[:, c], tol=1e-8, max_iter=300, mode=1)
+        assert abs(int(iters[c]) - (len(ho) - 1)) <= 1, (c, iters[c], len(ho) - 1)
+        assert np.linalg.norm(X[:, c] - xo) <= 1e-6 * np.linalg.norm(xo), c
