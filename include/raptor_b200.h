@@ -222,6 +222,10 @@ typedef struct rb_amg_opts {
                                  0: the stored values */
     int coarsen_type;         /* RB_COARSEN_* (RS solver): PMIS (default), RS, CLJP, Falgout, HMIS
                                  (par_ruge_stuben_solver.hpp:75-104; RS uses Falgout from level 3) */
+    int num_variables;        /* 1 (default); k > 1: the unknown-based systems form of the RS solver
+                                 (row i is variable i % k; classical strength and ModClassical /
+                                 Extended interpolation couple only rows of one variable,
+                                 par_strength.cpp:8-339, par_interpolation.cpp:811,918,1308,1390) */
 } rb_amg_opts;
 
 void rb_amg_default_opts(rb_amg_opts* opts);

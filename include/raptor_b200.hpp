@@ -230,6 +230,7 @@ class ParRugeStubenSolver : public ParMultilevel {
         opts.interp_type = interp_type;
     }
     double& interp_filter = opts.interp_filter;
+    int& num_variables = opts.num_variables;   /* ParMultilevel::num_variables */
 };
 
 /* aggregation/par_smoothed_aggregation_solver.hpp:17 */

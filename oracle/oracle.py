@@ -468,6 +468,7 @@ class RefOpts(C.Structure):
         ("interp", C.c_int), ("strength", C.c_int), ("relax", C.c_int),
         ("relax_weight", C.c_double), ("num_smooth_sweeps", C.c_int),
         ("interp_filter", C.c_double), ("max_coarse", C.c_int), ("max_levels", C.c_int),
+        ("num_variables", C.c_int),
     ]
 
 

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <exception>
 #include <string>
+#include <vector>
 
 #include "core/types.hpp"
 #include "core/par_matrix.hpp"
@@ -50,6 +51,7 @@ struct rp_opts {
     double interp_filter;
     int max_coarse;
     int max_levels;
+    int num_variables;    // ParMultilevel::num_variables (RS solver: the systems form)
 };
 
 }  // extern "C"
@@ -214,6 +216,7 @@ void rp_default_opts(rp_opts* o) {
     o->interp_filter = 0.3;
     o->max_coarse = 50;
     o->max_levels = 25;
+    o->num_variables = 1;
 }
 
 const char* rp_last_error(void) { return g_error.c_str(); }
@@ -241,6 +244,7 @@ void* rp_setup(void* pA, const rp_opts* o) {
     s->ml->num_smooth_sweeps = o->num_smooth_sweeps;
     s->ml->max_coarse = o->max_coarse;
     s->ml->max_levels = o->max_levels;
+    if (o->solver == 0) s->ml->num_variables = o->num_variables;
     try {
         s->ml->setup(A);
     } catch (const std::exception& e) {
@@ -308,24 +312,45 @@ void* rp_level(void* p, int l, int which) {
 int rp_level_states(void* p, int l, int* states_out) {
     Solver* s = (Solver*)p;
     if (s->o.solver != 0 || l < 0 || l >= s->ml->num_levels - 1) return -1;
-    ParCSRMatrix* A = s->ml->levels[l]->A;
     double* w = new double[s->n0 > 0 ? s->n0 : 1];
     srand(2448422 + 0);
     for (int i = 0; i < s->n0; i++) w[i] = double(rand()) / RAND_MAX;
-    ParCSRMatrix* S = A->strength((strength_t)s->o.strength, s->o.theta, false, 1, NULL);
-    aligned_vector<int> states, off_proc_states;
-    switch (s->o.coarsen) {
-    case RS:
-        if (l < 3) split_rs(S, states, off_proc_states, false);
-        else split_falgout(S, states, off_proc_states, false, w);
-        break;
-    case CLJP: split_cljp(S, states, off_proc_states, false, w); break;
-    case Falgout: split_falgout(S, states, off_proc_states, false, w); break;
-    case PMIS: split_pmis(S, states, off_proc_states, false, w); break;
-    case HMIS: split_hmis(S, states, off_proc_states, false, w); break;
+    // the solver's variable list (form_variable_list: row i of level 0 is
+    // variable i % num_variables), compacted to the C points after every
+    // level as extend_hierarchy does (par_ruge_stuben_solver.hpp:124-133):
+    // the levels below l are split again to follow it
+    const int nv = s->o.num_variables > 1 ? s->o.num_variables : 1;
+    std::vector<int> vars;
+    if (nv > 1) {
+        vars.resize(s->n0 > 0 ? s->n0 : 1);
+        for (int i = 0; i < s->n0; i++) vars[i] = i % nv;
     }
+    aligned_vector<int> states;
+    for (int lv = (nv > 1 ? 0 : l); lv <= l; lv++) {
+        ParCSRMatrix* A = s->ml->levels[lv]->A;
+        ParCSRMatrix* S = A->strength((strength_t)s->o.strength, s->o.theta, false, nv,
+                                      nv > 1 ? vars.data() : NULL);
+        aligned_vector<int> off_proc_states;
+        states.clear();
+        switch (s->o.coarsen) {
+        case RS:
+            if (lv < 3) split_rs(S, states, off_proc_states, false);
+            else split_falgout(S, states, off_proc_states, false, w);
+            break;
+        case CLJP: split_cljp(S, states, off_proc_states, false, w); break;
+        case Falgout: split_falgout(S, states, off_proc_states, false, w); break;
+        case PMIS: split_pmis(S, states, off_proc_states, false, w); break;
+        case HMIS: split_hmis(S, states, off_proc_states, false, w); break;
+        }
+        delete S;
+        if (nv > 1 && lv < l) {
+            int ctr = 0;
+            for (int i = 0; i < A->local_num_rows; i++)
+                if (states[i] == 1) vars[ctr++] = vars[i];
+        }
+    }
+    ParCSRMatrix* A = s->ml->levels[l]->A;
     for (int i = 0; i < A->local_num_rows; i++) states_out[i] = states[i];
-    delete S;
     delete[] w;
     return A->local_num_rows;
 }

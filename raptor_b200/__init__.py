@@ -384,7 +384,8 @@ class ParMultilevel:
     _FIELDS = ("strong_threshold", "relax_weight", "num_smooth_sweeps", "max_coarse",
                "max_levels", "max_iterations", "solve_tol", "interp_filter")
     _EXTRA = ("precision", "jacobi_compat", "seed_offset", "relax_type", "strength_type",
-              "interp_type", "fuse_coarse", "use_graphs", "const_coef", "coarsen_type", "prolong_weight",
+              "interp_type", "fuse_coarse", "use_graphs", "const_coef", "coarsen_type", "num_variables",
+              "prolong_weight",
               "prolong_smooth_steps", "solver")
 
     def __init__(self, strong_threshold=0.0, strength_type=Classical, relax_type=SOR):

@@ -41,7 +41,7 @@ class AmgOpts(C.Structure):
         ("prolong_weight", C.c_double), ("prolong_smooth_steps", C.c_int),
         ("precision", C.c_int), ("jacobi_compat", C.c_int), ("seed_offset", C.c_int),
         ("fuse_coarse", C.c_int), ("use_graphs", C.c_int), ("const_coef", C.c_int),
-        ("coarsen_type", C.c_int),
+        ("coarsen_type", C.c_int), ("num_variables", C.c_int),
     ]
 
 

@@ -641,6 +641,7 @@ void rb_amg_default_opts(rb_amg_opts* o) {
     o->use_graphs = 1;
     o->const_coef = 1;
     o->coarsen_type = RB_COARSEN_PMIS;
+    o->num_variables = 1;
 }
 
 int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_amg* out) {
@@ -663,6 +664,7 @@ int rb_amg_setup(rb_csr A, const rb_amg_opts* opts, const double* weights, rb_am
         RB_REQUIRE(o.precision == RB_PREC_FP64 || o.precision == RB_PREC_FP32, "unknown precision");
         RB_REQUIRE(o.coarsen_type >= RB_COARSEN_RS && o.coarsen_type <= RB_COARSEN_HMIS,
                    "unknown coarsening type");
+        RB_REQUIRE(o.num_variables >= 1, "num_variables must be >= 1");
         RB_REQUIRE(o.prolong_smooth_steps >= 0, "prolong_smooth_steps < 0");
         RB_REQUIRE(o.num_smooth_sweeps >= 0, "num_smooth_sweeps < 0");
         RB_REQUIRE(o.max_levels >= 1 && o.max_coarse >= 1, "max_levels and max_coarse must be >= 1");

@@ -537,11 +537,16 @@ void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* we
         cand.upload(ones.data(), ones.size());
     }
 
+    DevArray<int> vars;   // the systems form's variable list of the current level
+    if (!sa && o.num_variables > 1) variables_init(master[0].A->n_rows, o.num_variables, vars);
     while (master.back().A->n_rows > o.max_coarse &&
            (o.max_levels == -1 || (int)master.size() < o.max_levels)) {
         MasterLevel& L = master.back();
         const rb_csr_s& A = *L.A;
-        std::unique_ptr<rb_csr_s> S(strength(A, o.strength_type, o.strong_threshold));
+        // (the systems form applies to the RS solver's classical strength
+        // and interpolation, par_ruge_stuben_solver.hpp:69-70, 112-120)
+        const int* vp = (!sa && o.num_variables > 1) ? vars.get() : nullptr;
+        std::unique_ptr<rb_csr_s> S(strength(A, o.strength_type, o.strong_threshold, vp));
         L.states.alloc((size_t)std::max(A.n_rows, 1));
         if (sa) {
             // par_smoothed_aggregation_solver.hpp:51-129: mis2, aggregate,
@@ -581,7 +586,8 @@ void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* we
                     split_pmis(*S, wdev.get(), st);
                     break;
             }
-            L.P.reset(interpolation(A, *S, L.states.get(), o.interp_type, o.interp_filter));
+            L.P.reset(interpolation(A, *S, L.states.get(), o.interp_type, o.interp_filter, vp));
+            if (vp) variables_coarsen(A.n_rows, L.states.get(), vars);
         }
         S.reset();
         L.R.reset(transpose(*L.P));
@@ -590,13 +596,19 @@ void Hierarchy::setup(const rb_csr_s& Af, const rb_amg_opts& o, const double* we
         // relaxation) moves the diagonal first, which is the same thing
         rb_csr_s* Ac = rap(A, *L.P, L.R.get(), !sa);
         if (sa) sort_rows_diag_first(*Ac, true);
-        if (Ac->n_rows == 0 || Ac->n_rows == A.n_rows) {
-            // no coarsening possible: keep this level as the coarsest
+        if (Ac->n_rows == A.n_rows) {
+            // every point a C point: the next level would be this one again
+            // (the reference would repeat it until max_levels); keep this
+            // level as the coarsest
             delete Ac;
             L.P.reset();
             L.R.reset();
             break;
         }
+        // no C point at all (a splitting with no strong connections, as the
+        // systems form can produce): the reference keeps the empty coarse
+        // level, and so does this loop (its size then ends the loop); its
+        // coarse solve is empty and P_l has no columns
         master.emplace_back();
         master.back().A.reset(Ac);
     }

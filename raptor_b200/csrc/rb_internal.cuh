@@ -88,7 +88,15 @@ int handle_lanes(rb_csr_s& A, const double* x);
 void spmv_T64(rb_csr_s& A, const double* x, double* y);
 
 // Setup components (setup.cu).
-rb_csr_s* strength(const rb_csr_s& A, int kind, double theta);
+// vars (the unknown-based systems form, num_variables > 1; NULL otherwise):
+// each row's variable; classical strength and ModClassical / Extended
+// interpolation couple only rows of one variable (the reference's symmetric
+// strength and Direct ignore it)
+rb_csr_s* strength(const rb_csr_s& A, int kind, double theta, const int* vars = nullptr);
+// the finest level's variable list (row i: i % nv), and the next level's
+// (the C points' variables, in order)
+void variables_init(int n, int nv, DevArray<int>& vars);
+void variables_coarsen(int n, const int* states_dev, DevArray<int>& vars);
 // keep_states: the states are already set (HMIS / Falgout after the
 // Ruge-Stuben passes); otherwise set_initial_states first.
 void split_pmis(const rb_csr_s& S, const double* weights_dev, int* states_dev,
@@ -98,7 +106,7 @@ void split_cljp(const rb_csr_s& S, const double* weights_dev, int* states_dev,
 // Ruge-Stuben first pass (and second pass) on the host (coarsen_rs.cu).
 void split_rs(const rb_csr_s& S, int* states_dev, bool second_pass);
 rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* states_dev, int kind,
-                        double filter);
+                        double filter, const int* vars = nullptr);
 rb_csr_s* spgemm(const rb_csr_s& A, const rb_csr_s& B);
 rb_csr_s* rap(const rb_csr_s& A, const rb_csr_s& P, const rb_csr_s* R_in, bool diag_first);
 int colour_rows(const rb_csr_s& A, int* colour_dev);

@@ -34,12 +34,18 @@ std::vector<double> rand_weights(int n, int first_row) {
 }
 
 // ============================================================ strength ===
-// classical_strength, par_strength.cpp:8-339 (num_variables = 1).
+// classical_strength, par_strength.cpp:8-339.  vars (the unknown-based
+// systems form, num_variables > 1; NULL otherwise): only entries between rows
+// of one variable take part in the row's scale and can be strong.
+__device__ __forceinline__ bool same_var(int i, int j, const int* vars) {
+    return vars == nullptr || vars[i] == vars[j];
+}
+
 template <bool FILL>
 __global__ void k_classical_strength(int n, const int* __restrict__ rp,
                                      const int* __restrict__ ci, const double* __restrict__ cv,
                                      double theta, int* cnt, const int* srp, int* sci,
-                                     double* scv) {
+                                     double* scv, const int* __restrict__ nv) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int rs = rp[i], re = rp[i + 1];
@@ -51,17 +57,19 @@ __global__ void k_classical_strength(int n, const int* __restrict__ rp,
         double row_scale;
         if (diag < 0.0) {
             row_scale = -kRandMax;
-            for (int j = rs; j < re; j++) if (cv[j] > row_scale) row_scale = cv[j];
+            for (int j = rs; j < re; j++)
+                if (same_var(i, ci[j], nv) && cv[j] > row_scale) row_scale = cv[j];
         } else {
             row_scale = kRandMax;
-            for (int j = rs; j < re; j++) if (cv[j] < row_scale) row_scale = cv[j];
+            for (int j = rs; j < re; j++)
+                if (same_var(i, ci[j], nv) && cv[j] < row_scale) row_scale = cv[j];
         }
         double thr = dmul(row_scale, theta);
         if (FILL) { sci[out] = i; scv[out] = diag; }
         k = 1;
         for (int j = rs; j < re; j++) {
             double v = cv[j];
-            if (diag < 0 ? (v > thr) : (v < thr)) {
+            if (same_var(i, ci[j], nv) && (diag < 0 ? (v > thr) : (v < thr))) {
                 if (FILL) { sci[out + k] = ci[j]; scv[out + k] = v; }
                 k++;
             }
@@ -128,14 +136,15 @@ __global__ void k_sym_strength(int n, const int* __restrict__ rp, const int* __r
     if (!FILL) cnt[i] = k;
 }
 
-rb_csr_s* strength(const rb_csr_s& A, int kind, double theta) {
+rb_csr_s* strength(const rb_csr_s& A, int kind, double theta, const int* nv) {
     const int n = A.n_rows;
     DevArray<int> cnt((size_t)n + 1);
     const unsigned g = grid_for(n, 256);
     rb_csr_s* S = nullptr;
     if (kind == RB_STRENGTH_CLASSICAL) {
         if (n) k_classical_strength<false><<<g, 256, 0, stream()>>>(
-            n, A.rowptr.get(), A.cols.get(), A.vals.get(), theta, cnt.get(), nullptr, nullptr, nullptr);
+            n, A.rowptr.get(), A.cols.get(), A.vals.get(), theta, cnt.get(), nullptr, nullptr, nullptr,
+            nv);
         RB_CHECK_LAUNCH();
         DevArray<int> rp((size_t)n + 1);
         long long nnz = exclusive_scan(cnt.get(), rp.get(), n);
@@ -143,7 +152,7 @@ rb_csr_s* strength(const rb_csr_s& A, int kind, double theta) {
         S->rowptr = std::move(rp);
         if (n) k_classical_strength<true><<<g, 256, 0, stream()>>>(
             n, A.rowptr.get(), A.cols.get(), A.vals.get(), theta, nullptr, S->rowptr.get(),
-            S->cols.get(), S->vals.get());
+            S->cols.get(), S->vals.get(), nv);
         RB_CHECK_LAUNCH();
     } else {
         DevArray<double> sc((size_t)n + 1);
@@ -165,6 +174,44 @@ rb_csr_s* strength(const rb_csr_s& A, int kind, double theta) {
         RB_CHECK_LAUNCH();
     }
     return S;
+}
+
+// The variable list of the systems form: row i of the finest level is
+// variable i % nv (form_variable_list, par_ruge_stuben_solver.hpp:44-53); the
+// next level's list is the C points' variables in order
+// (par_ruge_stuben_solver.hpp:124-133).
+__global__ void k_vars_init(int n, int nv, int* vars) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) vars[i] = i % nv;
+}
+
+__global__ void k_c_flags(int n, const int* __restrict__ st, int* f) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) f[i] = st[i] == 1 ? 1 : 0;
+}
+
+__global__ void k_vars_compact(int n, const int* __restrict__ st, const int* __restrict__ pos,
+                               const int* __restrict__ vin, int* vout) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && st[i] == 1) vout[pos[i]] = vin[i];
+}
+
+void variables_init(int n, int nv, DevArray<int>& vars) {
+    vars.alloc((size_t)std::max(n, 1));
+    if (n) k_vars_init<<<grid_for(n, 256), 256, 0, stream()>>>(n, nv, vars.get());
+    RB_CHECK_LAUNCH();
+}
+
+void variables_coarsen(int n, const int* states_dev, DevArray<int>& vars) {
+    DevArray<int> f((size_t)n + 1), pos((size_t)n + 1);
+    if (n) k_c_flags<<<grid_for(n, 256), 256, 0, stream()>>>(n, states_dev, f.get());
+    RB_CHECK_LAUNCH();
+    const long long nc = exclusive_scan(f.get(), pos.get(), n);
+    DevArray<int> out((size_t)std::max<long long>(nc, 1));
+    if (n) k_vars_compact<<<grid_for(n, 256), 256, 0, stream()>>>(n, states_dev, pos.get(),
+                                                                  vars.get(), out.get());
+    RB_CHECK_LAUNCH();
+    vars = std::move(out);
 }
 
 // ================================================================ PMIS ===
@@ -480,7 +527,7 @@ __global__ void k_modclass_fill(int n, const int* __restrict__ arp, const int* _
                                 const double* __restrict__ acv, const int* __restrict__ srp,
                                 const int* __restrict__ sci, const double* __restrict__ scv,
                                 const int* __restrict__ st, const int* __restrict__ prp,
-                                int* pcols, double* pvals) {
+                                int* pcols, double* pvals, const int* __restrict__ nv) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int p0 = prp[i];
@@ -527,7 +574,7 @@ __global__ void k_modclass_fill(int n, const int* __restrict__ arp, const int* _
                     }
                 }
             }
-        } else if (st[col] != kNoNeighbors) {
+        } else if (st[col] != kNoNeighbors && same_var(i, col, nv)) {
             weak_sum = dadd(weak_sum, val);
         }
     }
@@ -599,7 +646,7 @@ __global__ void k_ext_fill(int n, const int* __restrict__ arp, const int* __rest
                            const double* __restrict__ acv, const int* __restrict__ srp,
                            const int* __restrict__ sci, const int* __restrict__ st,
                            const int* __restrict__ prp, int* pcols, double* pvals, double filter,
-                           int* kept) {
+                           int* kept, const int* __restrict__ nv) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int p0 = prp[i], p1 = prp[i + 1];
@@ -650,7 +697,7 @@ __global__ void k_ext_fill(int n, const int* __restrict__ arp, const int* __rest
                     }
                 }
             } else {
-                if (st[col] != kNoNeighbors) weak_sum = dadd(weak_sum, val);
+                if (st[col] != kNoNeighbors && same_var(i, col, nv)) weak_sum = dadd(weak_sum, val);
             }
         }
         if (fabs(weak_sum) > kZeroTol)
@@ -798,7 +845,7 @@ k_ext_fill_warp(int n, const int* __restrict__ arp, const int* __restrict__ aci,
                 const double* __restrict__ acv, const int* __restrict__ srp,
                 const int* __restrict__ sci, const int* __restrict__ st,
                 const int* __restrict__ prp, int* pcols, double* pvals, double filter,
-                int* kept) {
+                int* kept, const int* __restrict__ nv) {
     extern __shared__ unsigned char ext_smem[];
     ExtWarpMem& w = reinterpret_cast<ExtWarpMem*>(ext_smem)[threadIdx.x >> 5];
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -880,7 +927,7 @@ k_ext_fill_warp(int n, const int* __restrict__ arp, const int* __restrict__ aci,
                     __syncwarp();
                 }
             } else {
-                if (st[col] != kNoNeighbors) weak_sum = dadd(weak_sum, val);
+                if (st[col] != kNoNeighbors && same_var(i, col, nv)) weak_sum = dadd(weak_sum, val);
             }
         }
         if (fabs(weak_sum) > kZeroTol)
@@ -947,7 +994,7 @@ __global__ void k_compact_rows(int n, const int* __restrict__ srcp, const int* _
 }
 
 rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* st, int kind,
-                        double filter) {
+                        double filter, const int* nv) {
     const int n = A.n_rows;
     RB_REQUIRE(S.n_rows == n, "strength matrix does not match A");
     const unsigned g = grid_for(n, 256);
@@ -988,7 +1035,7 @@ rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* st, int
         DevArray<int> fine_cols((size_t)std::max(nnz, 1LL));
         if (n) k_modclass_fill<<<g, 256, 0, stream()>>>(
             n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(),
-            S.vals.get(), st, P->rowptr.get(), fine_cols.get(), P->vals.get());
+            S.vals.get(), st, P->rowptr.get(), fine_cols.get(), P->vals.get(), nv);
         RB_CHECK_LAUNCH();
         // map to coarse indices (rows are already in increasing column order)
         DevArray<double> tmpv((size_t)std::max(nnz, 1LL));
@@ -1058,11 +1105,11 @@ rb_csr_s* interpolation(const rb_csr_s& A, const rb_csr_s& S, const int* st, int
         k_ext_fill_warp<<<grid_for((long)n * 32, kExtWarps * 32), kExtWarps * 32,
                           kExtWarps * sizeof(ExtWarpMem), stream()>>>(
             n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(), st,
-            prp.get(), pcols.get(), pvals.get(), filter, kept.get());
+            prp.get(), pcols.get(), pvals.get(), filter, kept.get(), nv);
         RB_CHECK_LAUNCH();
         k_ext_fill<<<g, 256, 0, stream()>>>(
             n, A.rowptr.get(), A.cols.get(), A.vals.get(), S.rowptr.get(), S.cols.get(), st,
-            prp.get(), pcols.get(), pvals.get(), filter, kept.get());
+            prp.get(), pcols.get(), pvals.get(), filter, kept.get(), nv);
     }
     RB_CHECK_LAUNCH();
     DevArray<int> frp((size_t)n + 1);
