@@ -206,10 +206,14 @@ class ClockSampler:
 def a_bytes(ml, l, vbytes):
     """Bytes of one pass over A_l in its stored format: CSR z(v+4) + (n+1)4,
     the sliced diagonals nd * 32 ceil(n/32) v (no indices), or, for
-    diagonals with constant coefficients, one 4-byte mask a row."""
+    diagonals with constant coefficients, one 4-byte mask a row (none in the
+    box-grid form, whose kernels read only the vectors)."""
     n, z, _ = ml.level_info(l)
     nd = ml.level_storage(l)
-    if nd and ml.level_const_coef(l):
+    cc = ml.level_const_coef(l) if nd else 0
+    if cc == 2:
+        return 0
+    if cc:
         return 4 * n
     if nd:
         return nd * 32 * ((n + 31) // 32) * vbytes
@@ -717,11 +721,14 @@ def run_b200(args, rank, world, local):
         "stored_values_level0": stored,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic_for(dom + ("_const" if a0_const else "")),
+                     "traffic": traffic_for(dom + {0: "", 1: "_const", 2: "_grid"}[a0_const]),
                      "peak_source": peak_kind, "ops_ms": op_ms, "alg_bytes": alg,
-                     "a0_storage": (("constant-coefficient diagonals nd=%d (a 4-byte mask a "
-                                     "row)" if ml32.level_const_coef(0) else
-                                     "sliced-diagonals nd=%d") % ml32.level_storage(0))
+                     "a0_storage": ({0: "sliced-diagonals nd=%d",
+                                     1: "constant-coefficient diagonals nd=%d (a 4-byte mask a "
+                                        "row)",
+                                     2: "constant-coefficient stencil nd=%d on a box (x staged "
+                                        "in shared memory by planes, no mask)"}[a0_const]
+                                    % ml32.level_storage(0))
                      if ml32.level_storage(0) else "csr"},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": n * 8, "pinned": pinned},

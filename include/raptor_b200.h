@@ -274,7 +274,12 @@ int rb_amg_level_storage(rb_amg ml, int level, int* ndiag);
  * nonzero of a diagonal has one value, as in a constant-coefficient stencil):
  * the cycle's kernels then read one 4-byte mask a row (which of the stencil's
  * entries the row has) in place of the row's values, with the same products
- * in the same order.  RAPTOR_B200_CONST_DIA=0 at setup keeps the values.  No
+ * in the same order.  2 when, in addition, A_l is a 27-, 7-, 9- or 5-point
+ * stencil on a box whose rows hold exactly their in-box neighbours: the
+ * kernels then stage x in shared memory plane by plane and read no mask
+ * (the same products in the same order again), where the autotuner timed
+ * that faster.  RAPTOR_B200_CONST_DIA=0 at setup keeps the values;
+ * RAPTOR_B200_GRID_DIA=0 keeps the mask, =1 takes the box form untimed.  No
  * counterpart in the reference. */
 int rb_amg_level_const_coef(rb_amg ml, int level, int* constant);
 /* 1 when level l's first sweep from zero runs fused with its residual (one

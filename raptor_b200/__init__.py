@@ -504,11 +504,13 @@ class ParMultilevel:
         return nd.value
 
     def level_const_coef(self, l):
-        """True when A_l's diagonals have constant coefficients and the cycle
-        reads a mask a row instead of the values (see the C ABI)."""
+        """0: A_l's values are read; 1: its diagonals have constant
+        coefficients and the cycle reads a mask a row instead; 2: in
+        addition it is a stencil on a box and the cycle stages x in shared
+        memory, reading no mask (see the C ABI)."""
         f = C.c_int()
         check(lib().rb_amg_level_const_coef(self.h, l, C.byref(f)))
-        return bool(f.value)
+        return int(f.value)
 
     def level_fused_first(self, l):
         """True when level l's first sweep runs fused with its residual."""

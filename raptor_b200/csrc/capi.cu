@@ -819,10 +819,10 @@ int rb_amg_level_const_coef(rb_amg ml, int level, int* constant) {
         RB_REQUIRE(level >= 0 && level < ml->h.num_levels(), "level out of range");
         if (ml->h.opts.precision == RB_PREC_FP32) {
             const auto& V = ml->h.lv32[level];
-            *constant = V.dia && V.off.mask ? 1 : 0;
+            *constant = V.dia && V.off.mask ? (V.off.grid ? 2 : 1) : 0;
         } else {
             const auto& V = ml->h.lv64[level];
-            *constant = V.dia && V.off.mask ? 1 : 0;
+            *constant = V.dia && V.off.mask ? (V.off.grid ? 2 : 1) : 0;
         }
         return RB_OK;
     });

@@ -70,6 +70,9 @@ struct DiaOff {
     const unsigned* mask;
     double c[kMaxDiag];
     float cf[kMaxDiag];   // c in FP32 (exact: an FP32 level's values are FP32)
+    // box-grid form (grid.cuh; needs mask): the stencil shape (GridShape,
+    // 0 = none), the box nx x ny x nz (rows x fastest) and planes per block
+    int grid, nx, ny, nz, gzc;
 };
 
 // *p through the read-only path when `on`, else 0, as one predicated load
@@ -98,6 +101,12 @@ __device__ __forceinline__ TV dia_coef(const DiaOff& off, int d) {
     if constexpr (std::is_same<TV, float>::value) return off.cf[d];
     else return (TV)off.c[d];
 }
+
+}  // namespace rb
+
+#include "grid.cuh"
+
+namespace rb {
 
 // SC: the gathered vector is x_j * xs_j (the fused first sweep, spmv.cuh);
 // CC: constant coefficients (off.mask, off.c; base unused)
@@ -237,6 +246,10 @@ template <typename TV, typename TX, class Epi>
 void launch_dia(const DiaOff& off, const TV* sv, long n, const TX* x, Epi epi) {
     if (n <= 0) return;
     using Acc = AccOf2<TV, TX>;
+    if (off.mask && off.grid) {
+        launch_grid<TX, Acc, Epi, false>(off, x, epi, NoFinish{});
+        return;
+    }
     const unsigned g = dia_grid(n, false);
     if (off.mask) {
         switch (off.nd) {
@@ -260,9 +273,13 @@ void launch_dia(const DiaOff& off, const TV* sv, long n, const TX* x, Epi epi) {
 
 template <typename TV, class Fin>
 void launch_dia_dot(const DiaOff& off, const TV* sv, long n, const double* x, double* y, Fin fin) {
+    EpiStoreDot epi{x, y};
+    if (off.mask && off.grid) {
+        launch_grid<double, double, EpiStoreDot, true>(off, x, epi, fin);
+        return;
+    }
     const unsigned g = dia_grid(n, true);
     ReduceSlot rs = global_reduce_slot(g);
-    EpiStoreDot epi{x, y};
     if (off.mask) {
         switch (off.nd) {
             case 5: k_sdia_rows_dot<5, TV, Fin, true><<<g, 256, 0, stream()>>>(n, off, sv, x, epi, rs, fin); break;

@@ -451,6 +451,7 @@ static DiaOff find_diagonals(const rb_csr_s& M) {
 template <typename T>
 static void const_dia(Level<T>& V, bool allow) {
     V.off.mask = nullptr;
+    V.off.grid = kGridNone;
     V.dmask.release();
     const int nd = V.off.nd;
     static const bool disabled = [] {
@@ -484,6 +485,124 @@ static void const_dia(Level<T>& V, bool allow) {
     k_dia_mask<T><<<grid_for(V.n, 256), 256, 0, stream()>>>(V.n, nd, V.Adia.get(), V.dmask.get());
     RB_CHECK_LAUNCH();
     V.off.mask = V.dmask.get();
+    find_grid(V.off, V.n);
+}
+
+// ---------------------------------------------------------- box grids --
+// Whether the offsets are those of shape S on an nx x ny box.
+template <int S>
+static bool grid_offsets_match(const DiaOff& off, long long nx, long long ny) {
+    if (off.nd != Shape<S>::nd) return false;
+    for (int d = 0; d < off.nd; d++)
+        if (off.o[d] != Shape<S>::dz(d) * nx * ny + Shape<S>::dy(d) * nx + Shape<S>::dx(d))
+            return false;
+    return true;
+}
+
+// Whether every row's mask is the in-box bits of its coordinates.
+template <int S>
+static bool grid_rows_match(const DiaOff& off, long n, int nx, int ny, int nz) {
+    DevArray<int> bad(1);
+    bad.zero();
+    k_grid_mask_check<S><<<std::min<unsigned>(grid_for(n, 256), sm_count() * 8), 256, 0,
+                           stream()>>>(n, nx, ny, nz, off.mask, bad.get());
+    RB_CHECK_LAUNCH();
+    return read_scalar(bad.get()) == 0;
+}
+
+// Most blocks of a box-grid launch (its dot reduces one partial a block).
+constexpr long kGridMaxBlocks = 1 << 16;
+
+// Planes per block for a launch of at most kGridMaxBlocks blocks.
+static int grid_zc(const DiaOff& off, int want) {
+    const bool is3d = off.grid == kBox27 || off.grid == kStar7;
+    const long txw = is3d ? 32 : 256, tyh = is3d ? 8 : 1;
+    const long tiles = ((off.nx + txw - 1) / txw) * ((off.ny + tyh - 1) / tyh);
+    const long per = kGridMaxBlocks / tiles;
+    const long least = (off.nz + per - 1) / per;
+    return (int)std::max<long>(want, least);
+}
+
+// The box-grid form of a masked operator (grid.cuh): its diagonals must be
+// one of the GridShape stencils on some nx x ny x nz box (nx, ny read off
+// the offsets), and every row's mask its in-box bits (checked on the
+// device; the reference's stencil_grid on a box that is not a cube leaves
+// some in-box neighbours out along the fastest axis, and such an operator
+// keeps the mask).  RAPTOR_B200_GRID_DIA=0 keeps the masked kernels.
+static void find_grid(DiaOff& off, long n) {
+    off.grid = kGridNone;
+    static const char* env = getenv("RAPTOR_B200_GRID_DIA");
+    if (!off.mask || n <= 0 || (env && env[0] == '0')) return;
+    long long nx = 0, ny = 0;
+    int S = kGridNone;
+    switch (off.nd) {
+        case 27: S = kBox27; nx = off.o[16]; ny = nx > 0 && off.o[22] % nx == 0 ? off.o[22] / nx : 0; break;
+        case 7: S = kStar7; nx = off.o[5]; ny = nx > 0 && off.o[6] % nx == 0 ? off.o[6] / nx : 0; break;
+        case 9: S = kBox9; nx = off.o[7]; ny = 1; break;
+        case 5: S = kStar5; nx = off.o[4]; ny = 1; break;
+        default: return;
+    }
+    const bool is3d = S == kBox27 || S == kStar7;
+    if (nx < 3 || ny < 1 || (is3d && ny < 3) || nx * ny > n || n % (nx * ny)) return;
+    const long long nz = n / (nx * ny);
+    if (nx > INT_MAX || ny > INT_MAX || nz > INT_MAX) return;
+    const long txw = is3d ? 32 : 256, tyh = is3d ? 8 : 1;
+    if (((nx + txw - 1) / txw) * ((ny + tyh - 1) / tyh) > kGridMaxBlocks) return;
+    bool ok = false;
+    switch (S) {
+        case kBox27: ok = grid_offsets_match<kBox27>(off, nx, ny) && grid_rows_match<kBox27>(off, n, nx, ny, nz); break;
+        case kStar7: ok = grid_offsets_match<kStar7>(off, nx, ny) && grid_rows_match<kStar7>(off, n, nx, ny, nz); break;
+        case kBox9: ok = grid_offsets_match<kBox9>(off, nx, ny) && grid_rows_match<kBox9>(off, n, nx, ny, nz); break;
+        case kStar5: ok = grid_offsets_match<kStar5>(off, nx, ny) && grid_rows_match<kStar5>(off, n, nx, ny, nz); break;
+    }
+    if (!ok) return;
+    off.grid = S;
+    off.nx = (int)nx;
+    off.ny = (int)ny;
+    off.nz = (int)nz;
+    off.gzc = grid_zc(off, 16);
+}
+
+// Masked or box-grid kernels, and the planes a block marches, by timing
+// y = A x cold (RAPTOR_B200_GRID_DIA=1: the box-grid form, 16 planes,
+// untimed).
+template <typename T>
+static void tune_grid(Level<T>& V) {
+    if (!V.off.grid) return;
+    static const char* env = getenv("RAPTOR_B200_GRID_DIA");
+    if (env && env[0] == '1') return;
+    const std::string key = tune_key("A_grid", V.n, V.off.nd, (int)sizeof(T));
+    auto& c = tune_cache();
+    auto it = c.m.find(key);
+    if (it != c.m.end()) {
+        if (it->second > 0) V.off.gzc = grid_zc(V.off, it->second);
+        else V.off.grid = kGridNone;
+        return;
+    }
+    DevArray<T> x((size_t)V.n), y((size_t)V.n);
+    x.zero();
+    const size_t xb = sizeof(T) * (size_t)V.n;
+    DiaOff masked = V.off;
+    masked.grid = kGridNone;
+    float best = time_launch([&] {
+        launch_dia(masked, V.Adia.get(), V.n, x.get(), EpiStore<T>{y.get()});
+    }, x.get(), xb);
+    int pick = 0;
+    for (int zc : {8, 16, 32}) {
+        DiaOff g = V.off;
+        g.gzc = grid_zc(g, zc);
+        const float t = time_launch([&] {
+            launch_dia(g, V.Adia.get(), V.n, x.get(), EpiStore<T>{y.get()});
+        }, x.get(), xb);
+        if (t < best) {
+            best = t;
+            pick = zc;
+        }
+    }
+    if (pick > 0) V.off.gzc = grid_zc(V.off, pick);
+    else V.off.grid = kGridNone;
+    c.m[key] = pick;
+    tune_save();
 }
 
 template <typename T>
@@ -495,6 +614,7 @@ static void build_dia(Level<T>& V, const rb_csr_s& M, const DiaOff& off, bool co
                                                               M.vals.get(), off, V.Adia.get());
     RB_CHECK_LAUNCH();
     const_dia(V, const_coef);
+    tune_grid(V);
 }
 
 // ------------------------------------------------------------------ setup --
@@ -685,6 +805,7 @@ void Hierarchy::build_levels(std::vector<Level<T>>& lv) {
                 V.Adia.release();
                 V.dmask.release();
                 V.off.mask = nullptr;
+                V.off.grid = kGridNone;
             }
         }
         if (l < L - 1) {
