@@ -279,7 +279,8 @@ int rb_amg_level_storage(rb_amg ml, int level, int* ndiag);
  * kernels then stage x in shared memory plane by plane and read no mask
  * (the same products in the same order again), where the autotuner timed
  * that faster.  RAPTOR_B200_CONST_DIA=0 at setup keeps the values;
- * RAPTOR_B200_GRID_DIA=0 keeps the mask, =1 takes the box form untimed.  No
+ * RAPTOR_B200_GRID_DIA=0 keeps the mask, =1 or =2 take the box form untimed
+ * with one or two rows in x a thread.  No
  * counterpart in the reference. */
 int rb_amg_level_const_coef(rb_amg ml, int level, int* constant);
 /* 1 when level l's first sweep from zero runs fused with its residual (one

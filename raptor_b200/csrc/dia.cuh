@@ -71,8 +71,9 @@ struct DiaOff {
     double c[kMaxDiag];
     float cf[kMaxDiag];   // c in FP32 (exact: an FP32 level's values are FP32)
     // box-grid form (grid.cuh; needs mask): the stencil shape (GridShape,
-    // 0 = none), the box nx x ny x nz (rows x fastest) and planes per block
-    int grid, nx, ny, nz, gzc;
+    // 0 = none), the box nx x ny x nz (rows x fastest), planes per block and
+    // rows in x a thread
+    int grid, nx, ny, nz, gzc, gvx;
 };
 
 // *p through the read-only path when `on`, else 0, as one predicated load

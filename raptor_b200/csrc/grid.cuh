@@ -15,11 +15,12 @@
 // offset the compiler knows (the stencil shape and tile are template
 // parameters), and each plane tile is loaded from global memory once.
 //
-// Schedule: one block of TXW x TYH threads owns an x-y tile and marches zc
-// planes in z.  Four plane buffers form a ring: while the block computes
-// output plane z from planes z-1, z, z+1, it loads plane z+2 into registers
-// and stores it into the fourth buffer after its products, then one barrier.
-// The z loop is unrolled by four so every buffer index is a constant.
+// Schedule: one block owns an x-y tile of TXW x TYH rows (VX adjacent rows
+// in x a thread) and marches zc planes in z.  Four plane buffers form a
+// ring: while the block computes output plane z from planes z-1, z, z+1, it
+// loads plane z+2 into registers and stores it into the fourth buffer after
+// its products, then one barrier.  The z loop is unrolled by four so every
+// buffer index is a constant.
 //
 // Which operators take this form is decided at setup (find_grid, verified
 // row by row on the device by k_grid_mask_check); 2D shapes run with the
@@ -63,16 +64,23 @@ template <> struct Shape<kStar5> {
     __host__ __device__ static constexpr int dx(int d) { return d == 1 ? -1 : d == 3 ? 1 : 0; }
 };
 
-// Tile of a shape: TXW x TYH threads, plane buffers of H rows of W values.
-template <int S>
+// Tile of a shape with VX adjacent rows in x a thread: TXW x TYH rows on
+// NT threads, plane buffers of H rows of W values (W even, so that a pair of
+// values at an even column is 2 TX aligned).
+template <int S, int VX>
 struct GridTile {
     static constexpr bool is3d = Shape<S>::hy == 1;
-    static constexpr int TXW = is3d ? 32 : 256, TYH = is3d ? 8 : 1;
+    static constexpr int TXT = is3d ? 32 : 256;   // threads along x
+    static constexpr int TXW = TXT * VX, TYH = is3d ? 8 : 1;
     static constexpr int HY = Shape<S>::hy;
     static constexpr int W = TXW + 2, H = TYH + 2 * HY, P = W * H;
-    static constexpr int NT = TXW * TYH;
+    static constexpr int NT = TXT * TYH;
     static constexpr int LPT = (P + NT - 1) / NT;   // plane values a thread loads
 };
+
+template <typename T> struct Pair;
+template <> struct Pair<float> { using type = float2; };
+template <> struct Pair<double> { using type = double2; };
 
 // The in-box bits of row i's diagonals (x fastest).
 template <int S>
@@ -97,6 +105,13 @@ __global__ void k_grid_mask_check(long n, int nx, int ny, int nz, const unsigned
         if (mask[i] != grid_in_box_bits<S>(i, nx, ny, nz)) *bad = 1;
 }
 
+// The epilogue's operand record (an empty one when it has none).
+struct NoPre {};
+template <class Epi, class = void>
+struct PreOf { using type = NoPre; };
+template <class Epi>
+struct PreOf<Epi, std::void_t<typename Epi::Pre>> { using type = typename Epi::Pre; };
+
 template <typename Acc>
 __device__ __forceinline__ Acc fma_acc(Acc a, Acc b, Acc c);
 template <>
@@ -106,14 +121,18 @@ __device__ __forceinline__ double fma_acc<double>(double a, double b, double c) 
 
 // y-epilogue of A x on the box grid (DOT: the epilogue accumulates a dot,
 // reduced over the grid into fin).  One block per (x tile, y tile, z chunk),
-// flattened into blockIdx.x with x fastest.
-template <int S, typename TX, typename Acc, class Epi, bool DOT, class Fin>
-__global__ void __launch_bounds__(GridTile<S>::NT)
+// flattened into blockIdx.x with x fastest.  VX = 2: a thread computes rows
+// x and x + 1 and reads, for each (plane, dy) its diagonals touch, the four
+// values at x - 1 .. x + 2 as two aligned pairs; each row's products and
+// their order are still those of VX = 1.
+template <int S, int VX, typename TX, typename Acc, class Epi, bool DOT, class Fin>
+__global__ void __launch_bounds__(GridTile<S, VX>::NT)
 k_grid_rows(DiaOff off, const TX* __restrict__ x, Epi epi, ReduceSlot rs, Fin fin) {
-    using G = GridTile<S>;
+    using G = GridTile<S, VX>;
     using Sh = Shape<S>;
+    using TX2 = typename Pair<TX>::type;
     constexpr bool SC = ScaledGather<Epi>::value;
-    __shared__ TX buf[4][G::P];
+    __shared__ __align__(16) TX buf[4][G::P];
     if constexpr (!DOT && HasGate<Epi>::value) {
         if (!epi.open()) return;
     }
@@ -124,7 +143,7 @@ k_grid_rows(DiaOff off, const TX* __restrict__ x, Epi epi, ReduceSlot rs, Fin fi
     const int bt = (int)(blockIdx.x / (unsigned)ntx);
     const int by = bt % nty, bz = bt / nty;
     const int x0 = bx * G::TXW, y0 = by * G::TYH, z0 = bz * zc;
-    const int tx = threadIdx.x % G::TXW, ty = threadIdx.x / G::TXW;
+    const int tx = threadIdx.x % G::TXT, ty = threadIdx.x / G::TXT;
     const long plane = (long)nx * ny;
 
     // this thread's share of a plane tile: in-plane offset and whether it is
@@ -158,45 +177,69 @@ k_grid_rows(DiaOff off, const TX* __restrict__ x, Epi epi, ReduceSlot rs, Fin fi
             if (u < G::LPT - 1 || e < G::P) buf[slot][e] = v[u];
         }
     };
+    const int zend = min(z0 + zc, nz);
+    // buffer index of the value left of this thread's first row
+    const int left = (ty + G::HY) * G::W + tx * VX;
+    const int xr = x0 + tx * VX;
+    const bool in_y = y0 + ty < ny;
+    bool in_r[VX];
+#pragma unroll
+    for (int r = 0; r < VX; r++) in_r[r] = in_y && xr + r < nx;
+    const long row_xy = (long)(y0 + ty) * nx + xr;
     {
-        TX v[G::LPT];
-        load(z0 - 1, v);
-        store(0, v);
-        load(z0, v);
-        store(1, v);
-        load(z0 + 1, v);
-        store(2, v);
+        TX w[3][G::LPT];
+        load(z0 - 1, w[0]);
+        load(z0, w[1]);
+        load(z0 + 1, w[2]);
+        store(0, w[0]);
+        store(1, w[1]);
+        store(2, w[2]);
     }
     __syncthreads();
 
-    const int zend = min(z0 + zc, nz);
-    const int ctr = (ty + G::HY) * G::W + tx + 1;
-    const bool in_xy = x0 + tx < nx && y0 + ty < ny;
-    const long row_xy = (long)(y0 + ty) * nx + x0 + tx;
     double red = 0.0;
-    // output plane z from the buffers (K, K+1, K+2) mod 4; plane z + 2 into
-    // buffer (K + 3) mod 4 when step z + 1 will need it
+    // step K (output plane z): reads the buffers (K, K+1, K+2) mod 4 and
+    // stores plane z + 2 (loaded at the step's start) into buffer (K + 3) mod
+    // 4 when step z + 1 will need it
     auto step = [&](auto kc, int z) {
         constexpr int K = decltype(kc)::value;
         TX v[G::LPT];
         const bool more = z + 1 < zend;
         if (more) load(z + 2, v);
         const long i = (long)z * plane + row_xy;
-        Acc s = Acc(0);
+        using Pre = typename PreOf<Epi>::type;
+        Pre pr[VX] = {};
         if constexpr (HasPre<Epi>::value) {
-            typename Epi::Pre pr{};
-            if (in_xy) pr = epi.pre(i);
 #pragma unroll
-            for (int d = 0; d < Sh::nd; d++)
-                s = fma_acc<Acc>(dia_coef<Acc>(off, d),
-                                 (Acc)buf[(K + 1 + Sh::dz(d)) & 3][ctr + Sh::dy(d) * G::W + Sh::dx(d)], s);
-            if (in_xy) epi.post(i, s, red, pr);
-        } else {
+            for (int r = 0; r < VX; r++)
+                if (in_r[r]) pr[r] = epi.pre(i + r);
+        }
+        Acc s[VX];
 #pragma unroll
-            for (int d = 0; d < Sh::nd; d++)
-                s = fma_acc<Acc>(dia_coef<Acc>(off, d),
-                                 (Acc)buf[(K + 1 + Sh::dz(d)) & 3][ctr + Sh::dy(d) * G::W + Sh::dx(d)], s);
-            if (in_xy) epi(i, s, red);
+        for (int r = 0; r < VX; r++) s[r] = Acc(0);
+#pragma unroll
+        for (int d = 0; d < Sh::nd; d++) {
+            const TX* row = &buf[(K + 1 + Sh::dz(d)) & 3][left + Sh::dy(d) * G::W];
+            const Acc c = dia_coef<Acc>(off, d);
+            if constexpr (VX == 1) {
+                s[0] = fma_acc<Acc>(c, (Acc)row[1 + Sh::dx(d)], s[0]);
+            } else {
+                // values at x - 1, x, x + 1, x + 2 (the same loads for every
+                // diagonal of one (plane, dy), which the compiler merges)
+                const TX2 a = *reinterpret_cast<const TX2*>(row);
+                const TX2 b = *reinterpret_cast<const TX2*>(row + 2);
+                const TX v0 = Sh::dx(d) < 0 ? a.x : Sh::dx(d) == 0 ? a.y : b.x;
+                const TX v1 = Sh::dx(d) < 0 ? a.y : Sh::dx(d) == 0 ? b.x : b.y;
+                s[0] = fma_acc<Acc>(c, (Acc)v0, s[0]);
+                s[1] = fma_acc<Acc>(c, (Acc)v1, s[1]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < VX; r++) {
+            if (in_r[r]) {
+                if constexpr (HasPre<Epi>::value) epi.post(i + r, s[r], red, pr[r]);
+                else epi(i + r, s[r], red);
+            }
         }
         if (more) store((K + 3) & 3, v);
         __syncthreads();
@@ -217,14 +260,20 @@ inline long grid_blocks(const DiaOff& off, int txw, int tyh) {
     return ntx * nty * nzc;
 }
 
-template <int S, typename TX, typename Acc, class Epi, bool DOT, class Fin>
-void launch_grid_shape(const DiaOff& off, const TX* x, Epi epi, Fin fin) {
-    using G = GridTile<S>;
+template <int S, int VX, typename TX, typename Acc, class Epi, bool DOT, class Fin>
+void launch_grid_vx(const DiaOff& off, const TX* x, Epi epi, Fin fin) {
+    using G = GridTile<S, VX>;
     const long nb = grid_blocks(off, G::TXW, G::TYH);
     ReduceSlot rs{nullptr, nullptr};
     if constexpr (DOT) rs = global_reduce_slot((int)nb);
-    k_grid_rows<S, TX, Acc, Epi, DOT, Fin><<<(unsigned)nb, G::NT, 0, stream()>>>(off, x, epi, rs, fin);
+    k_grid_rows<S, VX, TX, Acc, Epi, DOT, Fin><<<(unsigned)nb, G::NT, 0, stream()>>>(off, x, epi, rs, fin);
     RB_CHECK_LAUNCH();
+}
+
+template <int S, typename TX, typename Acc, class Epi, bool DOT, class Fin>
+void launch_grid_shape(const DiaOff& off, const TX* x, Epi epi, Fin fin) {
+    if (off.gvx == 2) launch_grid_vx<S, 2, TX, Acc, Epi, DOT, Fin>(off, x, epi, fin);
+    else launch_grid_vx<S, 1, TX, Acc, Epi, DOT, Fin>(off, x, epi, fin);
 }
 
 template <typename TX, typename Acc, class Epi, bool DOT, class Fin>

@@ -516,7 +516,7 @@ constexpr long kGridMaxBlocks = 1 << 16;
 // Planes per block for a launch of at most kGridMaxBlocks blocks.
 static int grid_zc(const DiaOff& off, int want) {
     const bool is3d = off.grid == kBox27 || off.grid == kStar7;
-    const long txw = is3d ? 32 : 256, tyh = is3d ? 8 : 1;
+    const long txw = (is3d ? 32 : 256) * std::max(off.gvx, 1), tyh = is3d ? 8 : 1;
     const long tiles = ((off.nx + txw - 1) / txw) * ((off.ny + tyh - 1) / tyh);
     const long per = kGridMaxBlocks / tiles;
     const long least = (off.nz + per - 1) / per;
@@ -560,47 +560,63 @@ static void find_grid(DiaOff& off, long n) {
     off.nx = (int)nx;
     off.ny = (int)ny;
     off.nz = (int)nz;
+    off.gvx = (env && env[0] == '2') ? 2 : 1;
     off.gzc = grid_zc(off, 16);
 }
 
-// Masked or box-grid kernels, and the planes a block marches, by timing
-// y = A x cold (RAPTOR_B200_GRID_DIA=1: the box-grid form, 16 planes,
-// untimed).
+// Masked or box-grid kernels, the rows a thread takes in x and the planes a
+// block marches, by timing the residual r = b - A x cold (the cycle's most
+// frequent product; its epilogue sets the register count, and with it how
+// many blocks an SM holds, as the sweeps' does) (RAPTOR_B200_GRID_DIA=1 or 2: the
+// box-grid form with that many rows a thread, 16 planes, untimed).  The
+// record is planes | rows << 8, 0 for the masked kernels.
 template <typename T>
 static void tune_grid(Level<T>& V) {
     if (!V.off.grid) return;
     static const char* env = getenv("RAPTOR_B200_GRID_DIA");
-    if (env && env[0] == '1') return;
+    if (env && (env[0] == '1' || env[0] == '2')) return;
     const std::string key = tune_key("A_grid", V.n, V.off.nd, (int)sizeof(T));
     auto& c = tune_cache();
     auto it = c.m.find(key);
     if (it != c.m.end()) {
-        if (it->second > 0) V.off.gzc = grid_zc(V.off, it->second);
-        else V.off.grid = kGridNone;
+        if (it->second > 0) {
+            V.off.gvx = std::max(1, it->second >> 8);
+            V.off.gzc = grid_zc(V.off, it->second & 255);
+        } else {
+            V.off.grid = kGridNone;
+        }
         return;
     }
-    DevArray<T> x((size_t)V.n), y((size_t)V.n);
+    DevArray<T> x((size_t)V.n), b((size_t)V.n), y((size_t)V.n);
     x.zero();
+    b.zero();
     const size_t xb = sizeof(T) * (size_t)V.n;
     DiaOff masked = V.off;
     masked.grid = kGridNone;
     float best = time_launch([&] {
-        launch_dia(masked, V.Adia.get(), V.n, x.get(), EpiStore<T>{y.get()});
+        launch_dia(masked, V.Adia.get(), V.n, x.get(), EpiResidual<T, T>{b.get(), y.get()});
     }, x.get(), xb);
     int pick = 0;
-    for (int zc : {8, 16, 32}) {
-        DiaOff g = V.off;
-        g.gzc = grid_zc(g, zc);
-        const float t = time_launch([&] {
-            launch_dia(g, V.Adia.get(), V.n, x.get(), EpiStore<T>{y.get()});
-        }, x.get(), xb);
-        if (t < best) {
-            best = t;
-            pick = zc;
+    for (int vx : {1, 2}) {
+        for (int zc : {8, 16, 32}) {
+            DiaOff g = V.off;
+            g.gvx = vx;
+            g.gzc = grid_zc(g, zc);
+            const float t = time_launch([&] {
+                launch_dia(g, V.Adia.get(), V.n, x.get(), EpiResidual<T, T>{b.get(), y.get()});
+            }, x.get(), xb);
+            if (t < best) {
+                best = t;
+                pick = zc | vx << 8;
+            }
         }
     }
-    if (pick > 0) V.off.gzc = grid_zc(V.off, pick);
-    else V.off.grid = kGridNone;
+    if (pick > 0) {
+        V.off.gvx = pick >> 8;
+        V.off.gzc = grid_zc(V.off, pick & 255);
+    } else {
+        V.off.grid = kGridNone;
+    }
     c.m[key] = pick;
     tune_save();
 }

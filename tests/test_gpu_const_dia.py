@@ -7,8 +7,8 @@ in-box neighbours, no mask at all: x is staged in shared memory plane by
 plane with a zero halo (the box-grid form).  Every row's products, and their
 order, are those of the stored values, so one V-cycle must give the same
 result bit for bit in all three forms (RAPTOR_B200_CONST_DIA=0: stored
-values; RAPTOR_B200_GRID_DIA=0: the mask; RAPTOR_B200_GRID_DIA=1: the box
-grid).  The outer A p of PCG sums its p.Ap over rows in another grouping in
+values; RAPTOR_B200_GRID_DIA=0: the mask; RAPTOR_B200_GRID_DIA=1 or 2: the
+box grid with one or two rows in x a thread).  The outer A p of PCG sums its p.Ap over rows in another grouping in
 each form, so a whole solve agrees to rounding: iterations within one,
 residual histories within 1e-9 relative (1e-13 absolute: the histories are
 relative to the first residual, and the dots' rounding reaches about 1e-14
@@ -68,7 +68,7 @@ np.savez(out, rc=rc, res=np.array(res), x=x.numpy(), z=z.numpy(), const=ml.level
 """
 
 
-FORMS = {"stored": ("0", "0"), "masked": ("1", "0"), "grid": ("1", "1")}
+FORMS = {"stored": ("0", "0"), "masked": ("1", "0"), "grid": ("1", "1"), "grid2": ("1", "2")}
 
 
 def run_child(tmp_path, tag, m, prec, stencil):
@@ -89,7 +89,7 @@ def test_constant_coefficients_bit_identical(tmp_path, stencil, m, prec):
     assert int(off["nd"]) > 0 and int(off["const"]) == 0 and int(off["rc"]) == 0
     rtol = 1e-6 if stencil == "aniso2d" else 1e-9
     grid_code = 1 if stencil == "aniso7_uneven" else 2
-    for form, code in (("masked", 1), ("grid", grid_code)):
+    for form, code in (("masked", 1), ("grid", grid_code), ("grid2", grid_code)):
         on = run_child(tmp_path, form, m, prec, stencil)
         assert int(on["nd"]) == int(off["nd"])
         assert int(on["const"]) == code, form
