@@ -78,6 +78,27 @@ struct GridTile {
     static constexpr int LPT = (P + NT - 1) / NT;   // plane values a thread loads
 };
 
+// The epilogue's operand record (an empty one when it has none).
+struct NoPre {};
+template <class Epi, class = void>
+struct PreOf { using type = NoPre; };
+template <class Epi>
+struct PreOf<Epi, std::void_t<typename Epi::Pre>> { using type = typename Epi::Pre; };
+
+// Resident blocks the compiler must allow for: the FP32 sweeps with two rows
+// a thread (three operands a row: old iterate, b, inverse diagonal) are held
+// to RB_GRID_MINB2 blocks of 256 threads (48 registers, no spills; the
+// compiler's own choice is 64 registers, 4 blocks); every other instance
+// keeps the compiler's choice (the residual spills at 48).
+#ifndef RB_GRID_MINB2
+#define RB_GRID_MINB2 5
+#endif
+template <int VX, typename TX, class Epi>
+constexpr int grid_min_blocks() {
+    return (VX == 2 && sizeof(TX) == 4 && sizeof(typename PreOf<Epi>::type) >= 3 * sizeof(TX))
+               ? RB_GRID_MINB2 : 0;
+}
+
 template <typename T> struct Pair;
 template <> struct Pair<float> { using type = float2; };
 template <> struct Pair<double> { using type = double2; };
@@ -105,13 +126,6 @@ __global__ void k_grid_mask_check(long n, int nx, int ny, int nz, const unsigned
         if (mask[i] != grid_in_box_bits<S>(i, nx, ny, nz)) *bad = 1;
 }
 
-// The epilogue's operand record (an empty one when it has none).
-struct NoPre {};
-template <class Epi, class = void>
-struct PreOf { using type = NoPre; };
-template <class Epi>
-struct PreOf<Epi, std::void_t<typename Epi::Pre>> { using type = typename Epi::Pre; };
-
 template <typename Acc>
 __device__ __forceinline__ Acc fma_acc(Acc a, Acc b, Acc c);
 template <>
@@ -126,7 +140,7 @@ __device__ __forceinline__ double fma_acc<double>(double a, double b, double c) 
 // values at x - 1 .. x + 2 as two aligned pairs; each row's products and
 // their order are still those of VX = 1.
 template <int S, int VX, typename TX, typename Acc, class Epi, bool DOT, class Fin>
-__global__ void __launch_bounds__(GridTile<S, VX>::NT)
+__global__ void __launch_bounds__(GridTile<S, VX>::NT, grid_min_blocks<VX, TX, Epi>())
 k_grid_rows(DiaOff off, const TX* __restrict__ x, Epi epi, ReduceSlot rs, Fin fin) {
     using G = GridTile<S, VX>;
     using Sh = Shape<S>;
