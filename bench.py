@@ -721,7 +721,8 @@ def run_b200(args, rank, world, local):
         "stored_values_level0": stored,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic_for(dom + {0: "", 1: "_const", 2: "_grid"}[a0_const]),
+                     "traffic": traffic_for(dom + ({0: "", 1: "_const", 2: "_grid"}[a0_const]
+                                                  if "_A0_" in dom else "")),
                      "peak_source": peak_kind, "ops_ms": op_ms, "alg_bytes": alg,
                      "a0_storage": ({0: "sliced-diagonals nd=%d",
                                      1: "constant-coefficient diagonals nd=%d (a 4-byte mask a "
