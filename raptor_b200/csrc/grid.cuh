@@ -93,10 +93,19 @@ struct PreOf<Epi, std::void_t<typename Epi::Pre>> { using type = typename Epi::P
 #ifndef RB_GRID_MINB2
 #define RB_GRID_MINB2 5
 #endif
+// The FP64 instances with two rows a thread and at most one operand a row
+// (the outer A p with its dot, the FP64 residual) are held to
+// RB_GRID_MINB_F64 blocks (64 registers, no spills; the compiler's choice
+// for the dot is 78, 3 blocks); the FP64 sweeps spill at 64 and keep theirs.
+#ifndef RB_GRID_MINB_F64
+#define RB_GRID_MINB_F64 4
+#endif
 template <int VX, typename TX, class Epi>
 constexpr int grid_min_blocks() {
-    return (VX == 2 && sizeof(TX) == 4 && sizeof(typename PreOf<Epi>::type) >= 3 * sizeof(TX))
-               ? RB_GRID_MINB2 : 0;
+    using Pre = typename PreOf<Epi>::type;
+    if (VX == 2 && sizeof(TX) == 4 && sizeof(Pre) >= 3 * sizeof(TX)) return RB_GRID_MINB2;
+    if (VX == 2 && sizeof(TX) == 8 && sizeof(Pre) <= sizeof(TX)) return RB_GRID_MINB_F64;
+    return 0;
 }
 
 template <typename T> struct Pair;
