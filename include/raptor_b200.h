@@ -76,6 +76,11 @@ int rb_vec_device_ptr(rb_vec v, double** ptr);
 int rb_vec_copy(rb_vec dst, rb_vec src);         /* ParVector::copy */
 int rb_vec_axpy(rb_vec y, rb_vec x, double a);   /* ParVector::axpy, vector.cpp:53-59 */
 int rb_vec_scale(rb_vec y, double a);            /* ParVector::scale, vector.cpp:89-95 */
+/* out[k] = x[idx[k]] for k < n, idx and out device pointers (ordered on the
+ * library stream): the send-buffer packing of a halo exchange, ParComm's
+ * init_comm / pack_values (core/comm_pkg.hpp:145-158, core/comm_data.hpp:
+ * 257-262, 584).  An index outside x writes NaN. */
+int rb_vec_gather(rb_vec x, const int* idx, int n, double* out);
 int rb_vec_dot(rb_vec a, rb_vec b, double* out); /* ParVector::inner_product, par_vector.cpp:101-121 */
 int rb_vec_norm2(rb_vec a, double* out);         /* ParVector::norm(2), par_vector.cpp:88-98 */
 

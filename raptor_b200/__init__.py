@@ -104,6 +104,25 @@ class ParVector:
         check(lib().rb_vec_device_ptr(self.h, C.byref(p)))
         return p.value
 
+    def torch_view(self):
+        """The vector's device memory as a torch CUDA tensor (no copy; the
+        vector must outlive the tensor).  Used to receive halo values
+        straight into a vector."""
+        import torch
+
+        class _Cai:
+            pass
+
+        o = _Cai()
+        o.__cuda_array_interface__ = {"shape": (self.local_n,), "typestr": "<f8",
+                                      "data": (self.device_ptr(), False), "version": 3}
+        return torch.as_tensor(o, device="cuda")
+
+    def gather(self, idx_dev, n, out_dev):
+        """out[k] = self[idx[k]] for k < n (device pointers), on the library
+        stream: a halo exchange's send-buffer packing."""
+        check(lib().rb_vec_gather(self.h, C.c_void_p(idx_dev), int(n), C.c_void_p(out_dev)))
+
 
 class ParCSRMatrix:
     """Device CSR matrix, FP64 values, int32 indices (core/par_matrix.hpp:481-611)."""
@@ -697,6 +716,17 @@ def launch_count():
 
 def init(device=0):
     check(lib().rb_init(int(device)))
+
+
+def set_stream(cuda_stream):
+    """Order all later library calls on a caller's CUDA stream (its handle as
+    an integer; 0 = the library's own stream)."""
+    check(lib().rb_set_stream(C.c_void_p(int(cuda_stream) or None)))
+
+
+def synchronize():
+    """Wait for all work queued on the library stream."""
+    check(lib().rb_synchronize())
 
 
 def version():

@@ -58,6 +58,7 @@ SIGNATURES = {
     "rb_init": (C.c_int, [C.c_int]),
     "rb_set_stream": (C.c_int, [_P]),
     "rb_synchronize": (C.c_int, []),
+    "rb_vec_gather": (C.c_int, [_P, _P, C.c_int, _P]),
     "rb_csr_create": (C.c_int, [C.c_int, C.c_int, _i64, _P, _P, _P, C.c_int, _PP]),
     "rb_csr_destroy": (C.c_int, [_P]),
     "rb_csr_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(_i64)]),

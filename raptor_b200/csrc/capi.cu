@@ -270,6 +270,27 @@ int rb_vec_axpy(rb_vec y, rb_vec x, double a) {
     });
 }
 
+// out[k] = x[idx[k]]: packing the values a halo exchange sends.  An index
+// outside x gives NaN instead of a read out of bounds.
+__global__ void k_vec_gather(int n, const double* __restrict__ x, int nx, const int* __restrict__ idx,
+                             double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int j = idx[k];
+    out[k] = (j >= 0 && j < nx) ? x[j] : __longlong_as_double(0x7ff8000000000000ll);
+}
+
+int rb_vec_gather(rb_vec x, const int* idx, int n, double* out) {
+    return guarded([&]() -> int {
+        NEED(x);
+        RB_REQUIRE(n >= 0, "negative count");
+        RB_REQUIRE(n == 0 || (idx && out), "null index or output pointer");
+        if (n) k_vec_gather<<<grid_for(n, 256), 256, 0, stream()>>>(n, x->v.get(), x->n, idx, out);
+        RB_CHECK_LAUNCH();
+        return RB_OK;
+    });
+}
+
 int rb_vec_scale(rb_vec y, double a) {
     return guarded([&]() -> int {
         NEED(y);

@@ -1,0 +1,351 @@
+"""Row-partitioned ParCSR across processes: RAPtor's halo exchange (ParComm)
+and its distributed products, one process per GPU.
+
+The reference distributes a matrix by contiguous row blocks
+(core/partition.hpp:52-64).  Each rank stores its rows as an ``on_proc``
+block (columns it owns, local numbering) and an ``off_proc`` block whose
+columns are condensed to the sorted ``off_proc_column_map``
+(core/par_matrix.cpp:76-157).  ``ParComm`` (core/comm_pkg.hpp:400-466) turns
+that map into receive messages, one per owning rank and contiguous in the map,
+and send lists.  Each rank tells the owners which of their rows it needs.
+``ParMatrix::mult`` (util/linalg/par_spmv.cpp:25-59) starts the exchange of
+x's halo values, multiplies ``on_proc`` meanwhile, waits, then appends
+``off_proc`` times the received values; dots add the local dots over all
+ranks (core/par_vector.cpp:88-121).
+
+Here the transport is torch.distributed point-to-point (NCCL over NVLink on
+GPUs; the same calls run on gloo CPU ranks, which is how the plan and the
+exchange are tested without several GPUs).  The local products, the send
+buffer packing (``rb_vec_gather``) and the vectors live in the CUDA library.
+The library and the module's torch calls share one CUDA stream (``stream()``;
+the library is switched to it), so that the pack, the NCCL transfer, the
+``on_proc`` product and the ``off_proc`` product follow one another on the
+device with no host wait.  The ``on_proc`` product runs while the transfer
+is in flight, as in the reference.
+
+Scope: the distributed products (mult, residual, mult_append), the distributed
+dot and norm.  The distributed AMG setup of the reference (C/F splitting
+across ranks, the P-row exchange of RAP, coarse agglomeration) is not built;
+partitions that share one process, such as several partitions on one GPU,
+exchange through device copies (``mult_in_process``).
+"""
+import numpy as np
+
+from . import ParCSRMatrix, ParVector, RaptorError, set_stream
+
+_STREAM = None
+
+
+def stream():
+    """The CUDA stream of the distributed products (created on first use;
+    the library's calls are ordered on it from then on)."""
+    global _STREAM
+    if _STREAM is None:
+        import torch
+
+        _STREAM = torch.cuda.Stream()
+        set_stream(_STREAM.cuda_stream)
+    return _STREAM
+
+
+def _on_stream():
+    import torch
+
+    return torch.cuda.stream(stream())
+
+
+class RowPartition:
+    """Contiguous row blocks: rank q owns global rows [first[q], first[q+1])."""
+
+    def __init__(self, first):
+        self.first = np.asarray(first, dtype=np.int64)
+        if self.first.ndim != 1 or self.first.size < 2 or np.any(np.diff(self.first) < 0):
+            raise RaptorError(-1, "row partition must be nondecreasing with world + 1 entries")
+        self.world = self.first.size - 1
+        self.global_num_rows = int(self.first[-1])
+
+    @classmethod
+    def even(cls, n, world):
+        """The reference's default partition (core/partition.hpp:52-64): n //
+        world rows a rank, one more on each of the first n % world ranks."""
+        avg, extra = divmod(int(n), int(world))
+        first = [avg * q + min(q, extra) for q in range(world + 1)]
+        return cls(first)
+
+    def local_range(self, rank):
+        return int(self.first[rank]), int(self.first[rank + 1])
+
+    def owner(self, cols):
+        """Rank owning each global column (row) index."""
+        return np.searchsorted(self.first, np.asarray(cols, dtype=np.int64), side="right") - 1
+
+
+def split_rows(rowptr, cols, vals, first, last):
+    """Split rows of a CSR matrix with global column indices into the
+    on_proc block (columns in [first, last), numbered from first) and the
+    off_proc block (columns condensed to the sorted unique off_proc column
+    map), each row sorted by column (par_matrix.cpp:76-157).  Returns
+    ((rowptr, cols, vals) on_proc, (rowptr, cols, vals) off_proc, colmap)."""
+    rowptr = np.asarray(rowptr, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    vals = np.asarray(vals, dtype=np.float64)
+    n = rowptr.size - 1
+    rows = np.repeat(np.arange(n), np.diff(rowptr))
+    on = (cols >= first) & (cols < last)
+    colmap = np.unique(cols[~on])
+
+    def block(mask, newcols):
+        r, c, v = rows[mask], newcols, vals[mask]
+        o = np.lexsort((c, r))
+        rp = np.zeros(n + 1, dtype=np.int64)
+        np.add.at(rp, r + 1, 1)
+        return (np.cumsum(rp).astype(np.int32), c[o].astype(np.int32), v[o])
+
+    on_blk = block(on, cols[on] - first)
+    off_blk = block(~on, np.searchsorted(colmap, cols[~on]))
+    return on_blk, off_blk, colmap.astype(np.int64)
+
+
+class ParComm:
+    """Halo-exchange plan of one rank (core/comm_pkg.hpp:400-466).
+
+    recv_procs[k] sends this rank ghost values recv_ptr[k]:recv_ptr[k+1] of
+    the off_proc column map (the map is sorted and owners hold contiguous
+    rows, so each owner's columns are one run); send_procs[k] receives this
+    rank's local rows send_idx[send_ptr[k]:send_ptr[k+1]], in the order the
+    receiver's map lists them."""
+
+    def __init__(self, recv_procs, recv_ptr, send_procs, send_ptr, send_idx):
+        self.recv_procs = [int(q) for q in recv_procs]
+        self.recv_ptr = np.asarray(recv_ptr, dtype=np.int64)
+        self.send_procs = [int(q) for q in send_procs]
+        self.send_ptr = np.asarray(send_ptr, dtype=np.int64)
+        self.send_idx = np.asarray(send_idx, dtype=np.int32)
+
+    @property
+    def num_recv(self):
+        return int(self.recv_ptr[-1])
+
+    @property
+    def num_send(self):
+        return int(self.send_ptr[-1])
+
+    @staticmethod
+    def _recv_runs(partition, colmap):
+        owners = partition.owner(colmap)
+        procs, ptr = [], [0]
+        for k in range(len(colmap)):
+            if not procs or owners[k] != procs[-1]:
+                if procs:
+                    ptr.append(k)
+                procs.append(int(owners[k]))
+        if procs:
+            ptr.append(len(colmap))
+        return procs, ptr
+
+    @classmethod
+    def plan_all(cls, partition, colmaps):
+        """Every rank's plan from every rank's column map, in one process (no
+        communication): what build() computes on each rank."""
+        runs = [cls._recv_runs(partition, np.asarray(m, dtype=np.int64)) for m in colmaps]
+        plans = []
+        for r in range(partition.world):
+            send_procs, send_ptr, send_idx = [], [0], []
+            first = partition.local_range(r)[0]
+            for q in range(partition.world):
+                procs, ptr = runs[q]
+                if r in procs:
+                    k = procs.index(r)
+                    seg = np.asarray(colmaps[q], dtype=np.int64)[ptr[k]:ptr[k + 1]]
+                    send_procs.append(q)
+                    send_idx.extend((seg - first).tolist())
+                    send_ptr.append(len(send_idx))
+            procs, ptr = runs[r]
+            plans.append(cls(procs, ptr, send_procs, send_ptr, send_idx))
+        return plans
+
+    @classmethod
+    def build(cls, partition, colmap, rank, group=None, device="cpu"):
+        """This rank's plan, exchanging index lists with the other ranks over
+        torch.distributed (``device``: where the messages live; CUDA for
+        NCCL).  Every rank of the group must call it."""
+        import torch
+        import torch.distributed as dist
+
+        colmap = np.asarray(colmap, dtype=np.int64)
+        world = partition.world
+        procs, ptr = cls._recv_runs(partition, colmap)
+        need = torch.zeros(world, dtype=torch.int64, device=device)
+        for k, q in enumerate(procs):
+            need[q] = ptr[k + 1] - ptr[k]
+        # recv sizes of every rank (the reference all-reduces them; gathering
+        # the whole table also tells each rank whom it sends to)
+        table = [torch.zeros(world, dtype=torch.int64, device=device) for _ in range(world)]
+        dist.all_gather(table, need, group=group)
+        counts = [int(table[q][rank]) for q in range(world)]
+        send_procs = [q for q in range(world) if counts[q] > 0 and q != rank]
+        ops, bufs = [], []
+        cm = torch.as_tensor(colmap, device=device)
+        for k, q in enumerate(procs):
+            ops.append(dist.P2POp(dist.isend, cm[ptr[k]:ptr[k + 1]].contiguous(), q, group=group))
+        for q in send_procs:
+            b = torch.empty(counts[q], dtype=torch.int64, device=device)
+            bufs.append(b)
+            ops.append(dist.P2POp(dist.irecv, b, q, group=group))
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+        first = partition.local_range(rank)[0]
+        send_ptr = [0]
+        send_idx = []
+        for b in bufs:
+            send_idx.extend((b.cpu().numpy() - first).tolist())
+            send_ptr.append(len(send_idx))
+        return cls(procs, ptr, send_procs, send_ptr, send_idx)
+
+    def exchange_packed(self, send_buf, recv_buf, group=None):
+        """Start the exchange: send_buf holds this rank's send_idx values
+        (packed), recv_buf receives the ghost values in column-map order.
+        Returns the requests to wait on (empty when nothing moves)."""
+        import torch.distributed as dist
+
+        ops = []
+        for k, q in enumerate(self.recv_procs):
+            a, b = int(self.recv_ptr[k]), int(self.recv_ptr[k + 1])
+            ops.append(dist.P2POp(dist.irecv, recv_buf[a:b], q, group=group))
+        for k, q in enumerate(self.send_procs):
+            a, b = int(self.send_ptr[k]), int(self.send_ptr[k + 1])
+            ops.append(dist.P2POp(dist.isend, send_buf[a:b], q, group=group))
+        return dist.batch_isend_irecv(ops) if ops else []
+
+
+class DistParCSRMatrix:
+    """This rank's rows of a row-partitioned matrix on its GPU
+    (core/par_matrix.hpp:78-343): the on_proc and off_proc blocks as device
+    CSR matrices, the halo plan, the packed send buffer and the ghost vector.
+    Vectors are ParVector of the local size (local_num_rows)."""
+
+    def __init__(self, partition, rank, rowptr, cols, vals, comm=None, group=None):
+        import torch
+
+        self.partition, self.rank, self.group = partition, int(rank), group
+        first, last = partition.local_range(rank)
+        self.local_num_rows = last - first
+        (orp, oci, ocv), (frp, fci, fcv), self.colmap = split_rows(rowptr, cols, vals, first, last)
+        self.on_proc = ParCSRMatrix.from_arrays(self.local_num_rows, self.local_num_rows, orp, oci, ocv)
+        self.off_proc_num_cols = len(self.colmap)
+        self.off_proc = (ParCSRMatrix.from_arrays(self.local_num_rows, self.off_proc_num_cols,
+                                                  frp, fci, fcv)
+                         if self.off_proc_num_cols else None)
+        if comm is None:
+            comm = ParComm.build(partition, self.colmap, rank, group=group, device="cuda")
+        self.comm = comm
+        with _on_stream():
+            self.send_idx = torch.as_tensor(comm.send_idx, device="cuda")
+            self.send_buf = torch.empty(max(comm.num_send, 1), dtype=torch.float64, device="cuda")
+        stream().synchronize()
+        self.ghost = ParVector(max(self.off_proc_num_cols, 1))
+        self.ghost_buf = self.ghost.torch_view()
+        self.tmp = ParVector(max(self.local_num_rows, 1))
+        stream()
+
+    @classmethod
+    def from_global(cls, rowptr, cols, vals, partition, rank, group=None, comm=None):
+        """This rank's rows of a global host CSR matrix."""
+        first, last = partition.local_range(rank)
+        rowptr = np.asarray(rowptr, dtype=np.int64)
+        a, b = int(rowptr[first]), int(rowptr[last])
+        return cls(partition, rank, rowptr[first:last + 1] - a, np.asarray(cols)[a:b],
+                   np.asarray(vals)[a:b], comm=comm, group=group)
+
+    # ---------------------------------------------------------------- halo
+    def pack(self, x):
+        if self.comm.num_send:
+            x.gather(self.send_idx.data_ptr(), self.comm.num_send, self.send_buf.data_ptr())
+
+    def start_halo(self, x):
+        self.pack(x)
+        with _on_stream():
+            return self.comm.exchange_packed(self.send_buf, self.ghost_buf, group=self.group)
+
+    @staticmethod
+    def _wait(reqs):
+        with _on_stream():
+            for w in reqs:
+                w.wait()
+
+    # ------------------------------------------------------------ products
+    def mult(self, x, b):
+        """b = A x (par_spmv.cpp:25-59): halo exchange in flight while the
+        on_proc product runs, then b += off_proc * ghost."""
+        reqs = self.start_halo(x)
+        self.on_proc.mult(x, b)
+        self._wait(reqs)
+        if self.off_proc is not None:
+            self.off_proc.mult_append(self.ghost, b)
+
+    def mult_append(self, x, b):
+        """b += A x (par_spmv.cpp:91-125)."""
+        reqs = self.start_halo(x)
+        self.on_proc.mult_append(x, b)
+        self._wait(reqs)
+        if self.off_proc is not None:
+            self.off_proc.mult_append(self.ghost, b)
+
+    def residual(self, x, b, r):
+        """r = b - A x (par_spmv.cpp:215-252)."""
+        reqs = self.start_halo(x)
+        self.on_proc.residual(x, b, r)
+        self._wait(reqs)
+        if self.off_proc is not None:
+            self.off_proc.mult(self.ghost, self.tmp)
+            r.axpy(self.tmp, -1.0)
+
+    # ---------------------------------------------------------------- dots
+    def inner_product(self, x, y):
+        """Global x.y: local dots summed over the ranks (par_vector.cpp:101-121)."""
+        import torch
+        import torch.distributed as dist
+
+        with _on_stream():
+            t = torch.tensor([x.inner_product(y)], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, group=self.group)
+            return float(t.item())
+
+    def norm(self, x):
+        return float(np.sqrt(self.inner_product(x, x)))
+
+    # ------------------------------------------- partitions in one process
+    @staticmethod
+    def exchange_in_process(mats, xs):
+        """The halo exchange between partitions held by one process (several
+        partitions on one GPU): each partition's packed values copied into
+        the ghost vectors of the partitions that need them."""
+        for m, x in zip(mats, xs):
+            m.pack(x)
+        with _on_stream():
+            for q, mq in enumerate(mats):
+                for k, r in enumerate(mq.comm.recv_procs):
+                    mr = mats[r]
+                    j = mr.comm.send_procs.index(q)
+                    a, b = int(mr.comm.send_ptr[j]), int(mr.comm.send_ptr[j + 1])
+                    c, d = int(mq.comm.recv_ptr[k]), int(mq.comm.recv_ptr[k + 1])
+                    mq.ghost_buf[c:d].copy_(mr.send_buf[a:b])
+
+    @staticmethod
+    def mult_in_process(mats, xs, bs):
+        """b_r = (A x)_r for every partition r held by this process."""
+        DistParCSRMatrix.exchange_in_process(mats, xs)
+        for m, x, b in zip(mats, xs, bs):
+            m.on_proc.mult(x, b)
+            if m.off_proc is not None:
+                m.off_proc.mult_append(m.ghost, b)
+
+    @staticmethod
+    def residual_in_process(mats, xs, bs, rs):
+        DistParCSRMatrix.exchange_in_process(mats, xs)
+        for m, x, b, r in zip(mats, xs, bs, rs):
+            m.on_proc.residual(x, b, r)
+            if m.off_proc is not None:
+                m.off_proc.mult(m.ghost, m.tmp)
+                r.axpy(m.tmp, -1.0)
