@@ -86,10 +86,11 @@ template <class Epi>
 struct PreOf<Epi, std::void_t<typename Epi::Pre>> { using type = typename Epi::Pre; };
 
 // Resident blocks the compiler must allow for: the FP32 sweeps with two rows
-// a thread (three operands a row: old iterate, b, inverse diagonal) are held
-// to RB_GRID_MINB2 blocks of 256 threads (48 registers, no spills; the
-// compiler's own choice is 64 registers, 4 blocks); every other instance
-// keeps the compiler's choice (the residual spills at 48).
+// a thread (two or three operands a row: old iterate, b, inverse diagonal;
+// the first sweep fused with the residual reads b and the inverse diagonal)
+// are held to RB_GRID_MINB2 blocks of 256 threads (48 registers, no spills;
+// the compiler's own choice is 64 registers, 4 blocks); the FP32 residual
+// spills at 48 and keeps the compiler's choice.
 #ifndef RB_GRID_MINB2
 #define RB_GRID_MINB2 5
 #endif
@@ -103,7 +104,7 @@ struct PreOf<Epi, std::void_t<typename Epi::Pre>> { using type = typename Epi::P
 template <int VX, typename TX, class Epi>
 constexpr int grid_min_blocks() {
     using Pre = typename PreOf<Epi>::type;
-    if (VX == 2 && sizeof(TX) == 4 && sizeof(Pre) >= 3 * sizeof(TX)) return RB_GRID_MINB2;
+    if (VX == 2 && sizeof(TX) == 4 && sizeof(Pre) >= 2 * sizeof(TX)) return RB_GRID_MINB2;
     if (VX == 2 && sizeof(TX) == 8 && sizeof(Pre) <= sizeof(TX)) return RB_GRID_MINB_F64;
     return 0;
 }

@@ -565,7 +565,8 @@ static void find_grid(DiaOff& off, long n) {
 }
 
 // Masked or box-grid kernels, the rows a thread takes in x and the planes a
-// block marches, by timing the residual r = b - A x cold (the cycle's most
+// block marches (4 to 32: the candidates differ in how the block count
+// fills the SMs' resident blocks), by timing the residual r = b - A x cold (the cycle's most
 // frequent product; its epilogue sets the register count, and with it how
 // many blocks an SM holds, as the sweeps' does) (RAPTOR_B200_GRID_DIA=1 or 2: the
 // box-grid form with that many rows a thread, 16 planes, untimed).  The
@@ -598,7 +599,7 @@ static void tune_grid(Level<T>& V) {
     }, x.get(), xb);
     int pick = 0;
     for (int vx : {1, 2}) {
-        for (int zc : {8, 16, 32}) {
+        for (int zc : {4, 6, 8, 12, 16, 24, 32}) {
             DiaOff g = V.off;
             g.gvx = vx;
             g.gzc = grid_zc(g, zc);
