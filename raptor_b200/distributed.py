@@ -24,10 +24,12 @@ device with no host wait.  The ``on_proc`` product runs while the transfer
 is in flight, as in the reference.
 
 Scope: the distributed products (mult, residual, mult_append), the distributed
-dot and norm.  The distributed AMG setup of the reference (C/F splitting
-across ranks, the P-row exchange of RAP, coarse agglomeration) is not built;
-partitions that share one process, such as several partitions on one GPU,
-exchange through device copies (``mult_in_process``).
+dot and norm, and the reference's CG and PCG over them (krylov/par_cg.cpp),
+the PCG preconditioned by one AMG cycle of each partition's own block (block
+Jacobi).  The distributed AMG setup of the reference (C/F splitting across
+ranks, the P-row exchange of RAP, coarse agglomeration) is not built.
+Partitions that share one process, such as several partitions on one GPU,
+exchange through device copies (``mult_in_process``, ``Partitions``).
 """
 import numpy as np
 
@@ -349,3 +351,201 @@ class DistParCSRMatrix:
             if m.off_proc is not None:
                 m.off_proc.mult(m.ghost, m.tmp)
                 r.axpy(m.tmp, -1.0)
+
+
+# ------------------------------------------------------------------ Krylov --
+class Partitions:
+    """The partitions of one row-partitioned matrix that this process holds:
+    one (a process per GPU; products exchange over the process group, dots
+    all_reduce) or all of them (several partitions in one process; products
+    exchange by device copies, dots add up locally).  Vectors are lists of
+    ParVector, one per held partition."""
+
+    def __init__(self, mats, in_process=None):
+        import torch.distributed as dist
+
+        self.mats = list(mats)
+        world = self.mats[0].partition.world
+        if in_process is None:
+            in_process = len(self.mats) == world and (world > 1 or not dist.is_initialized())
+        if in_process and len(self.mats) != world:
+            raise RaptorError(-1, "in-process partitions must be all %d partitions" % world)
+        if not in_process and len(self.mats) != 1:
+            raise RaptorError(-1, "a process of a process group holds one partition")
+        self.in_process = in_process
+        self.global_n = self.mats[0].partition.global_num_rows
+
+    def vectors(self, values=None):
+        """New vectors, from a global array of values (or zero)."""
+        out = []
+        for m in self.mats:
+            f, l = m.partition.local_range(m.rank)
+            v = ParVector(self.global_n, local_n=l - f, first_local=f)
+            if values is not None:
+                v.set_values(np.asarray(values, dtype=np.float64)[f:l])
+            else:
+                v.set_const_value(0.0)
+            out.append(v)
+        return out
+
+    def mult(self, xs, ys):
+        if self.in_process:
+            DistParCSRMatrix.mult_in_process(self.mats, xs, ys)
+        else:
+            self.mats[0].mult(xs[0], ys[0])
+
+    def residual(self, xs, bs, rs):
+        if self.in_process:
+            DistParCSRMatrix.residual_in_process(self.mats, xs, bs, rs)
+        else:
+            self.mats[0].residual(xs[0], bs[0], rs[0])
+
+    def dot(self, xs, ys):
+        if self.in_process:
+            return float(sum(x.inner_product(y) for x, y in zip(xs, ys)))
+        return self.mats[0].inner_product(xs[0], ys[0])
+
+    def norm(self, xs):
+        return float(np.sqrt(self.dot(xs, xs)))
+
+    @staticmethod
+    def axpy(ys, xs, a):
+        for y, x in zip(ys, xs):
+            y.axpy(x, a)
+
+    @staticmethod
+    def scale(ys, a):
+        for y in ys:
+            y.scale(a)
+
+    @staticmethod
+    def copy(ys, xs):
+        for y, x in zip(ys, xs):
+            y.copy(x)
+
+    @staticmethod
+    def set_const(ys, v):
+        for y in ys:
+            y.set_const_value(v)
+
+
+class BlockJacobiAMG:
+    """Preconditioner of the distributed PCG: one AMG V-cycle per partition
+    on its own on_proc block (block Jacobi over the partitions, an AMG solve
+    of each block).  The reference's PCG at several ranks cycles one
+    distributed hierarchy instead, whose setup is not built here; at one
+    partition the two are the same.  ``make_solver()`` returns an unset-up
+    ParMultilevel (for example ParRugeStubenSolver(...))."""
+
+    def __init__(self, parts, make_solver):
+        self.parts = parts
+        self.levels = []
+        for m in parts.mats:
+            ml = make_solver()
+            ml.setup(m.on_proc)
+            self.levels.append(ml)
+
+    def cycle(self, zs, rs):
+        """z = M^-1 r from z = 0, on every held partition."""
+        for ml, z, r in zip(self.levels, zs, rs):
+            z.set_const_value(0.0)
+            ml.cycle(z, r)
+
+
+def _breakdown():
+    from ._capi import Breakdown
+
+    return Breakdown(-4, "Indefinite matrix detected in CG")
+
+
+def CG(parts, xs, bs, res, tol=1e-5, max_iter=-1):
+    """Conjugate gradients over the partitions (krylov/par_cg.cpp:8-118): the
+    true residual every 8 iterations (and first), stopping when ||r|| <= tol
+    ||r_0||; res gets ||r|| / ||b|| per iteration.  Returns 0 when it
+    converged, -5 at the iteration limit; p.Ap < 0 raises Breakdown (the
+    reference exits)."""
+    P = parts
+    r, p, Ap = P.vectors(), P.vectors(), P.vectors()
+    b_norm = P.norm(bs)
+    if b_norm < 1e-16:
+        b_norm = 1.0
+    if max_iter <= 0:
+        max_iter = int(1.3 * P.global_n) + 2
+    P.residual(xs, bs, r)
+    P.copy(p, r)
+    rr = P.dot(r, r)
+    norm_r = float(np.sqrt(rr))
+    res.append(norm_r / b_norm)
+    if norm_r != 0.0:
+        tol = tol * norm_r
+    recompute_r, it = 8, 0
+    while norm_r > tol and it < max_iter:
+        P.mult(p, Ap)
+        app = P.dot(Ap, p)
+        if app < 0.0 or not np.isfinite(app):
+            raise _breakdown()
+        alpha = rr / app
+        P.axpy(xs, p, alpha)
+        if (it % recompute_r) and it > 0:
+            P.axpy(r, Ap, -alpha)
+        else:
+            P.residual(xs, bs, r)
+        nxt = P.dot(r, r)
+        beta = nxt / rr
+        P.scale(p, beta)
+        P.axpy(p, r, 1.0)
+        rr = nxt
+        norm_r = float(np.sqrt(rr))
+        res.append(norm_r / b_norm)
+        it += 1
+    return -5 if it == max_iter and norm_r > tol else 0
+
+
+def PCG(parts, precond, xs, bs, res, tol=1e-5, max_iter=-1):
+    """Preconditioned CG over the partitions (krylov/par_cg.cpp:121-263),
+    with the reference's stopping rule and history: the first entry is
+    sqrt(r.z), then (r.z) / (b.Mb) per iteration, stopping when r.z < tol
+    sqrt(b.Mb); the true residual every 8 iterations.  ``precond.cycle(z, r)``
+    applies M^-1 from z = 0 (BlockJacobiAMG).  Returns 0 or -5 as CG."""
+    P = parts
+    r, z, p, Ap = P.vectors(), P.vectors(), P.vectors(), P.vectors()
+    if max_iter <= 0:
+        max_iter = int(1.3 * P.global_n) + 2
+    precond.cycle(z, bs)
+    b_inner = P.dot(bs, z)
+    norm_b = float(np.sqrt(b_inner))
+    if norm_b > 1e-16:
+        tol = tol * norm_b
+    P.residual(xs, bs, r)
+    precond.cycle(z, r)
+    P.copy(p, z)
+    rz = P.dot(r, z)
+    res.append(float(np.sqrt(rz)))
+    recompute_r, it, converged = 8, 0, False
+    while it < max_iter:
+        it += 1
+        P.mult(p, Ap)
+        app = P.dot(Ap, p)
+        if app < 0.0 or not np.isfinite(app):
+            raise _breakdown()
+        alpha = rz / app
+        P.axpy(xs, p, alpha)
+        full_r = recompute_r and it % recompute_r == 0
+        if full_r:
+            P.residual(xs, bs, r)
+        else:
+            P.axpy(r, Ap, -alpha)
+        precond.cycle(z, r)
+        nxt = P.dot(r, z)
+        beta = nxt / rz
+        res.append(nxt / b_inner)
+        if nxt < tol:
+            converged = True
+            break
+        if full_r:
+            P.copy(p, z)
+        else:
+            P.scale(p, beta)
+            P.axpy(p, z, 1.0)
+        rz = nxt
+    return 0 if converged else -5

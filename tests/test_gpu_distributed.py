@@ -7,8 +7,14 @@ device copies with the plan every rank would build) must give the rows of
 A x and b - A x of the whole matrix: on_proc x_local + off_proc x_ghost sums
 a row in another grouping than the single product, so the check is to
 1e-14 of sum_j |a_ij x_j| against an FP64 numpy product and the library's
-own product of the whole matrix.  A one-rank NCCL group runs the
-communicating path itself (plan built by all_gather, dot by all_reduce).
+own product of the whole matrix.  CG over three partitions must follow the
+library's CG on the whole matrix (histories to 1e-8); PCG over one partition
+with its block-Jacobi AMG (then the whole matrix's AMG) must give the
+library's reference-mode PCG history to 1e-10 (to within one iteration),
+and over four uneven
+partitions must converge.  A one-rank NCCL group runs the communicating path
+itself (plan built by all_gather, dots by all_reduce, CG through it equal to
+CG in process).
 The NCCL point-to-point halo between several GPUs is not run here (one GPU
 per run); its plan and exchange are checked on gloo CPU ranks in
 tests/test_distributed.py.
@@ -121,6 +127,73 @@ def test_partitions_in_one_process_match_whole_matrix(name, parts):
     assert np.all(np.abs(r - (bvec - want)) <= tol + 1e-15 * np.abs(bvec))
 
 
+def partitions_of(rp, ci, cv, part):
+    maps = []
+    for r in range(part.world):
+        f, l = part.local_range(r)
+        maps.append(D.split_rows(rp[f:l + 1] - rp[f], ci[rp[f]:rp[l]], cv[rp[f]:rp[l]], f, l)[2])
+    plans = D.ParComm.plan_all(part, maps)
+    return D.Partitions([D.DistParCSRMatrix.from_global(rp, ci, cv, part, r, comm=plans[r])
+                         for r in range(part.world)])
+
+
+def test_cg_over_partitions_matches_whole_matrix_cg():
+    rp, ci, cv = csr_of(rb.par_stencil_grid(rb.laplace_stencil_27pt(), [12, 12, 12]))
+    n = len(rp) - 1
+    P = partitions_of(rp, ci, cv, D.RowPartition.even(n, 3))
+    b = np.random.default_rng(4).uniform(-1, 1, n)
+    xs, bs = P.vectors(), P.vectors(b)
+    res = []
+    assert D.CG(P, xs, bs, res, tol=1e-8, max_iter=400) == 0
+    A = rb.ParCSRMatrix.from_arrays(n, n, rp, ci, cv)
+    x2, res2 = rb.ParVector(n), []
+    assert rb.CG(A, x2, rb.ParVector(n, values=b), res2, tol=1e-8, max_iter=400) == 0
+    assert abs(len(res) - len(res2)) <= 1
+    k = min(len(res), len(res2))
+    np.testing.assert_allclose(res[:k], res2[:k], rtol=1e-8, atol=1e-15)
+    x = np.concatenate([v.numpy() for v in xs])
+    assert np.linalg.norm(x - x2.numpy()) <= 1e-7 * np.linalg.norm(x2.numpy())
+
+
+def make_amg():
+    return rb.ParRugeStubenSolver(0.25, rb.PMIS, rb.Extended, rb.Classical, rb.L1Jacobi)
+
+
+def test_pcg_one_partition_is_the_libraries_pcg():
+    rp, ci, cv = csr_of(rb.par_stencil_grid(rb.laplace_stencil_27pt(), [20, 20, 20]))
+    n = len(rp) - 1
+    P = partitions_of(rp, ci, cv, D.RowPartition.even(n, 1))
+    M = D.BlockJacobiAMG(P, make_amg)
+    b = np.random.default_rng(6).uniform(-1, 1, n)
+    xs, bs = P.vectors(), P.vectors(b)
+    res = []
+    assert D.PCG(P, M, xs, bs, res, tol=1e-8, max_iter=100) == 0
+    A = rb.ParCSRMatrix.from_arrays(n, n, rp, ci, cv)
+    ml = make_amg()
+    ml.setup(A)
+    x2, res2 = rb.ParVector(n), []
+    assert rb.PCG(A, ml, x2, rb.ParVector(n, values=b), res2, tol=1e-8, max_iter=100,
+                  mode=rb.PCG_REFERENCE) == 0
+    assert abs(len(res) - len(res2)) <= 1
+    k = min(len(res), len(res2))
+    np.testing.assert_allclose(res[:k], res2[:k], rtol=1e-10, atol=1e-18)
+
+
+def test_pcg_block_jacobi_amg_over_partitions_converges():
+    rp, ci, cv = csr_of(rb.par_stencil_grid(rb.laplace_stencil_27pt(), [20, 20, 20]))
+    n = len(rp) - 1
+    P = partitions_of(rp, ci, cv, D.RowPartition([0, 2000, 5000, 6500, n]))
+    M = D.BlockJacobiAMG(P, make_amg)
+    b = np.random.default_rng(8).uniform(-1, 1, n)
+    xs, bs = P.vectors(), P.vectors(b)
+    res = []
+    assert D.PCG(P, M, xs, bs, res, tol=1e-10, max_iter=300) == 0
+    x = np.concatenate([v.numpy() for v in xs])
+    r = b - product(rp, ci, cv, x)
+    assert np.linalg.norm(r) <= 1e-4 * np.linalg.norm(b)
+    assert len(res) < 120
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -148,6 +221,17 @@ def test_one_rank_nccl_group():
         assert np.all(np.abs(yv.numpy() - want) <= 1e-14 * scale_of(rp, ci, cv, x))
         assert abs(M.inner_product(xv, xv) - xv.inner_product(xv)) == 0.0
         assert abs(M.norm(xv) - np.linalg.norm(x)) <= 1e-12 * np.linalg.norm(x)
+        # CG through the process group (halo and dots over NCCL) against the
+        # same CG with the partition in process
+        P = D.Partitions([M])
+        assert not P.in_process
+        bvec = np.random.default_rng(3).uniform(-1, 1, n)
+        xs, res = P.vectors(), []
+        assert D.CG(P, xs, P.vectors(bvec), res, tol=1e-8, max_iter=400) == 0
+        Q = D.Partitions([M], in_process=True)
+        xq, resq = Q.vectors(), []
+        assert D.CG(Q, xq, Q.vectors(bvec), resq, tol=1e-8, max_iter=400) == 0
+        assert res == resq
     finally:
         rb.synchronize()
         dist.destroy_process_group()
