@@ -105,8 +105,24 @@ int rb_diffusion_stencil_2d(double eps, double theta, double* out9);
 int rb_laplace_stencil_27pt(double* out27);
 /* par_stencil_grid (gallery/par_stencil.hpp:16-236) */
 int rb_stencil_grid(const double* stencil, const int* grid, int dim, rb_csr* out);
-/* readParMatrix for PETSc binary AIJ files (gallery/par_matrix_IO.cpp:22+) */
+/* readParMatrix for PETSc binary AIJ files (gallery/par_matrix_IO.cpp:22+):
+ * big-endian int32 header (1211216, rows, columns, nonzeros), row lengths,
+ * column indices, float64 values; rows sorted diagonal first as finalize()
+ * does.  A file whose row lengths do not add up to the nonzero count, or
+ * with a column out of range, is refused (RB_ERR_INVALID). */
 int rb_read_petsc(const char* path, rb_csr* out);
+/* The same parsing into caller-owned host arrays in file order (no device
+ * needed; readMatrix, gallery/matrix_IO.cpp:24-110).  Call with rowptr,
+ * cols, vals NULL to learn the sizes, then with arrays of n_rows + 1, nnz
+ * and nnz entries. */
+int rb_petsc_read_host(const char* path, int* n_rows, int* n_cols, int64_t* nnz, int* rowptr,
+                       int* cols, double* vals);
+/* Write a PETSc binary AIJ file (what PETSc's MatLoad reads) from host CSR
+ * arrays, rows and entries in the given order; the reference reads this
+ * format but has no writer.  rb_write_petsc writes a device matrix. */
+int rb_petsc_write_host(const char* path, int n_rows, int n_cols, int64_t nnz, const int* rowptr,
+                        const int* cols, const double* vals);
+int rb_write_petsc(rb_csr A, const char* path);
 /* MatrixMarket coordinate files (real, integer or pattern; general,
  * symmetric or skew-symmetric).  read_mm (gallery/matrix_market.cpp:18-76):
  * entries in file order within each row, the symmetry field ignored (the

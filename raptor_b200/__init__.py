@@ -297,6 +297,37 @@ def mm_write_host(path, n_rows, n_cols, rowptr, cols, vals):
                                  _ptr(cv) if cv.size else None))
 
 
+def write_petsc(A, path):
+    """Write a device matrix as a PETSc binary AIJ file (what PETSc's MatLoad
+    and readParMatrix read), rows and entries in the matrix's order."""
+    check(lib().rb_write_petsc(A.h, str(path).encode()))
+
+
+def petsc_read_host(path):
+    """readMatrix's parsing of a PETSc binary AIJ file into host arrays in
+    file order (gallery/matrix_IO.cpp:24-110; no device): returns (n_rows,
+    n_cols, rowptr, cols, vals)."""
+    m, n, z = C.c_int(), C.c_int(), C.c_int64()
+    p = str(path).encode()
+    check(lib().rb_petsc_read_host(p, C.byref(m), C.byref(n), C.byref(z), None, None, None))
+    rp = np.zeros(m.value + 1, np.int32)
+    ci = np.zeros(max(z.value, 1), np.int32)
+    cv = np.zeros(max(z.value, 1), np.float64)
+    check(lib().rb_petsc_read_host(p, C.byref(m), C.byref(n), C.byref(z), _ptr(rp), _ptr(ci),
+                                   _ptr(cv)))
+    return m.value, n.value, rp, ci[:z.value], cv[:z.value]
+
+
+def petsc_write_host(path, n_rows, n_cols, rowptr, cols, vals):
+    """Write host CSR arrays as a PETSc binary AIJ file (no device)."""
+    rp = np.ascontiguousarray(rowptr, np.int32)
+    ci = np.ascontiguousarray(cols, np.int32)
+    cv = np.ascontiguousarray(vals, np.float64)
+    check(lib().rb_petsc_write_host(str(path).encode(), int(n_rows), int(n_cols), int(rp[-1]),
+                                    _ptr(rp), _ptr(ci) if ci.size else None,
+                                    _ptr(cv) if cv.size else None))
+
+
 # setup components ---------------------------------------------------------
 def split_pmis(S, weights=None):
     n = S.global_num_rows

@@ -59,6 +59,10 @@ SIGNATURES = {
     "rb_set_stream": (C.c_int, [_P]),
     "rb_synchronize": (C.c_int, []),
     "rb_vec_gather": (C.c_int, [_P, _P, C.c_int, _P]),
+    "rb_petsc_read_host": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(_i64), _P, _P, _P]),
+    "rb_petsc_write_host": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _i64, _P, _P, _P]),
+    "rb_write_petsc": (C.c_int, [_P, C.c_char_p]),
     "rb_csr_create": (C.c_int, [C.c_int, C.c_int, _i64, _P, _P, _P, C.c_int, _PP]),
     "rb_csr_destroy": (C.c_int, [_P]),
     "rb_csr_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(_i64)]),

@@ -403,35 +403,51 @@ int rb_read_petsc(const char* path, rb_csr* out) {
     return guarded([&]() -> int {
         ensure_device();
         NEED(path); NEED(out);
-        FILE* f = fopen(path, "rb");
-        RB_REQUIRE(f != nullptr, std::string("cannot open ") + path);
-        std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
-        auto be32 = [&](int* dst, size_t n) {
-            std::vector<unsigned char> buf(4 * n);
-            RB_REQUIRE(fread(buf.data(), 1, buf.size(), f) == buf.size(), "truncated PETSc file");
-            for (size_t i = 0; i < n; i++)
-                dst[i] = (int)((unsigned)buf[4 * i] << 24 | (unsigned)buf[4 * i + 1] << 16 |
-                               (unsigned)buf[4 * i + 2] << 8 | (unsigned)buf[4 * i + 3]);
-        };
-        int hdr[4];
-        be32(hdr, 4);
-        RB_REQUIRE(hdr[0] == 1211216, "not a PETSc binary AIJ matrix");
-        const int m = hdr[1], n = hdr[2], nnz = hdr[3];
-        std::vector<int> lens(m), rp(m + 1, 0), ci(nnz);
-        be32(lens.data(), m);
-        be32(ci.data(), nnz);
-        for (int i = 0; i < m; i++) rp[i + 1] = rp[i] + lens[i];
-        std::vector<double> cv(nnz);
-        std::vector<unsigned char> buf(8 * (size_t)nnz);
-        RB_REQUIRE(fread(buf.data(), 1, buf.size(), f) == buf.size(), "truncated PETSc file");
-        for (int j = 0; j < nnz; j++) {
-            uint64_t u = 0;
-            for (int k = 0; k < 8; k++) u = (u << 8) | buf[8 * (size_t)j + k];
-            memcpy(&cv[j], &u, 8);
-        }
-        int rc = rb_csr_create(m, n, nnz, rp.data(), ci.data(), cv.data(), 0, out);
+        HostCsr H = petsc_parse(path);
+        int rc = rb_csr_create(H.n_rows, H.n_cols, (int64_t)H.cols.size(), H.rowptr.data(),
+                               H.cols.data(), H.vals.data(), 0, out);
         if (rc != RB_OK) return rc;
         sort_rows_diag_first(**out, false);   // finalize() sorts rows
+        return RB_OK;
+    });
+}
+
+int rb_petsc_read_host(const char* path, int* n_rows, int* n_cols, int64_t* nnz, int* rowptr,
+                       int* cols, double* vals) {
+    return guarded([&]() -> int {
+        NEED(path); NEED(n_rows); NEED(n_cols); NEED(nnz);
+        HostCsr H = petsc_parse(path);
+        *n_rows = H.n_rows;
+        *n_cols = H.n_cols;
+        *nnz = (int64_t)H.cols.size();
+        if (rowptr) std::copy(H.rowptr.begin(), H.rowptr.end(), rowptr);
+        if (cols) std::copy(H.cols.begin(), H.cols.end(), cols);
+        if (vals) std::copy(H.vals.begin(), H.vals.end(), vals);
+        return RB_OK;
+    });
+}
+
+int rb_petsc_write_host(const char* path, int n_rows, int n_cols, int64_t nnz, const int* rowptr,
+                        const int* cols, const double* vals) {
+    return guarded([&]() -> int {
+        NEED(path);
+        petsc_write(path, n_rows, n_cols, (long long)nnz, rowptr, cols, vals);
+        return RB_OK;
+    });
+}
+
+int rb_write_petsc(rb_csr A, const char* path) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(path);
+        std::vector<int> rp((size_t)A->n_rows + 1), ci((size_t)A->nnz);
+        std::vector<double> cv((size_t)A->nnz);
+        A->rowptr.download(rp.data(), rp.size());
+        if (A->nnz) {
+            A->cols.download(ci.data(), ci.size());
+            A->vals.download(cv.data(), cv.size());
+        }
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        petsc_write(path, A->n_rows, A->n_cols, A->nnz, rp.data(), ci.data(), cv.data());
         return RB_OK;
     });
 }

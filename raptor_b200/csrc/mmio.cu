@@ -23,6 +23,7 @@
 #include <cctype>
 #include <cerrno>
 #include <climits>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -216,6 +217,100 @@ void mm_write(const char* path, int n_rows, int n_cols, long long nnz, const int
         for (int q = rowptr[i]; q < rowptr[i + 1]; q++)
             std::fprintf(f, "%d %d %2.15e\n", i + 1, cols[q] + 1, vals[q]);
     RB_REQUIRE(std::ferror(f) == 0, std::string("write failed: ") + path);
+}
+
+// ---------------------------------------------------------------- PETSc --
+// PETSc's binary AIJ matrix format (what MatView writes to a binary viewer
+// and MatLoad reads; the reference's readMatrix / readParMatrix input,
+// gallery/matrix_IO.cpp:24-110, gallery/par_matrix_IO.cpp:22+): big-endian
+// int32 header (1211216, rows, columns, nonzeros), int32 row lengths, int32
+// column indices, float64 values, rows in order and each row's entries as
+// stored.
+namespace {
+constexpr int kPetscMatCode = 1211216;
+
+void put_be32(unsigned char* p, unsigned v) {
+    p[0] = (unsigned char)(v >> 24);
+    p[1] = (unsigned char)(v >> 16);
+    p[2] = (unsigned char)(v >> 8);
+    p[3] = (unsigned char)v;
+}
+}  // namespace
+
+HostCsr petsc_parse(const char* path) {
+    FILE* f = std::fopen(path, "rb");
+    RB_REQUIRE(f != nullptr, std::string("cannot open ") + path);
+    std::unique_ptr<FILE, int (*)(FILE*)> guard(f, std::fclose);
+    auto be32 = [&](int* dst, size_t n) {
+        std::vector<unsigned char> buf(4 * n);
+        RB_REQUIRE(std::fread(buf.data(), 1, buf.size(), f) == buf.size(), "truncated PETSc file");
+        for (size_t i = 0; i < n; i++)
+            dst[i] = (int)((unsigned)buf[4 * i] << 24 | (unsigned)buf[4 * i + 1] << 16 |
+                           (unsigned)buf[4 * i + 2] << 8 | (unsigned)buf[4 * i + 3]);
+    };
+    int hdr[4];
+    be32(hdr, 4);
+    RB_REQUIRE(hdr[0] == kPetscMatCode, "not a PETSc binary AIJ matrix");
+    HostCsr A;
+    A.n_rows = hdr[1];
+    A.n_cols = hdr[2];
+    const int nnz = hdr[3];
+    RB_REQUIRE(A.n_rows >= 0 && A.n_cols >= 0 && nnz >= 0, "negative size in a PETSc header");
+    std::vector<int> lens((size_t)A.n_rows);
+    be32(lens.data(), lens.size());
+    A.rowptr.assign((size_t)A.n_rows + 1, 0);
+    for (int i = 0; i < A.n_rows; i++) {
+        RB_REQUIRE(lens[i] >= 0, "negative row length in a PETSc file");
+        A.rowptr[i + 1] = A.rowptr[i] + lens[i];
+        RB_REQUIRE(A.rowptr[i + 1] <= nnz, "PETSc row lengths exceed the nonzero count");
+    }
+    RB_REQUIRE(A.rowptr[A.n_rows] == nnz, "PETSc row lengths do not add up to the nonzero count");
+    A.cols.resize((size_t)nnz);
+    be32(A.cols.data(), A.cols.size());
+    for (int c : A.cols) RB_REQUIRE(c >= 0 && c < A.n_cols, "PETSc column index out of range");
+    A.vals.resize((size_t)nnz);
+    std::vector<unsigned char> buf(8 * (size_t)nnz);
+    RB_REQUIRE(std::fread(buf.data(), 1, buf.size(), f) == buf.size(), "truncated PETSc file");
+    for (int j = 0; j < nnz; j++) {
+        uint64_t u = 0;
+        for (int k = 0; k < 8; k++) u = (u << 8) | buf[8 * (size_t)j + k];
+        std::memcpy(&A.vals[j], &u, 8);
+    }
+    return A;
+}
+
+void petsc_write(const char* path, int n_rows, int n_cols, long long nnz, const int* rowptr,
+                 const int* cols, const double* vals) {
+    RB_REQUIRE(n_rows >= 0 && n_cols >= 0 && nnz >= 0, "negative matrix dimension");
+    RB_REQUIRE(nnz <= INT_MAX, "more nonzeros than a PETSc binary AIJ file holds");
+    RB_REQUIRE(n_rows == 0 || (rowptr && (nnz == 0 || (cols && vals))), "missing CSR arrays");
+    RB_REQUIRE(n_rows == 0 || (rowptr[0] == 0 && rowptr[n_rows] == nnz),
+               "row pointers do not span the nonzeros");
+    std::vector<unsigned char> out(16 + 4 * (size_t)n_rows + 12 * (size_t)nnz);
+    unsigned char* p = out.data();
+    put_be32(p, (unsigned)kPetscMatCode);
+    put_be32(p + 4, (unsigned)n_rows);
+    put_be32(p + 8, (unsigned)n_cols);
+    put_be32(p + 12, (unsigned)nnz);
+    p += 16;
+    for (int i = 0; i < n_rows; i++, p += 4) {
+        RB_REQUIRE(rowptr[i + 1] >= rowptr[i], "row pointers decrease");
+        put_be32(p, (unsigned)(rowptr[i + 1] - rowptr[i]));
+    }
+    for (long long j = 0; j < nnz; j++, p += 4) {
+        RB_REQUIRE(cols[j] >= 0 && cols[j] < n_cols, "column index out of range");
+        put_be32(p, (unsigned)cols[j]);
+    }
+    for (long long j = 0; j < nnz; j++, p += 8) {
+        uint64_t u;
+        std::memcpy(&u, &vals[j], 8);
+        for (int k = 0; k < 8; k++) p[k] = (unsigned char)(u >> (56 - 8 * k));
+    }
+    FILE* f = std::fopen(path, "wb");
+    RB_REQUIRE(f != nullptr, std::string("cannot write ") + path);
+    std::unique_ptr<FILE, int (*)(FILE*)> guard(f, std::fclose);
+    RB_REQUIRE(std::fwrite(out.data(), 1, out.size(), f) == out.size(),
+               std::string("write failed: ") + path);
 }
 
 }  // namespace rb

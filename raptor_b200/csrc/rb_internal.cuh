@@ -63,6 +63,10 @@ struct HostCsr {
 // off-diagonal entries of symmetric / skew-symmetric files, sort_rows sorts
 // each row by column (stable); otherwise file order within a row (mmio.cu)
 HostCsr mm_parse(const char* path, bool mirror, bool sort_rows);
+// PETSc binary AIJ file <-> host CSR, rows and entries in file order (mmio.cu)
+HostCsr petsc_parse(const char* path);
+void petsc_write(const char* path, int n_rows, int n_cols, long long nnz, const int* rowptr,
+                 const int* cols, const double* vals);
 void mm_write(const char* path, int n_rows, int n_cols, long long nnz, const int* rowptr,
               const int* cols, const double* vals);
 rb_csr_s* clone_csr(const rb_csr_s& M);

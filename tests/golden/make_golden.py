@@ -7,6 +7,7 @@ use and stores them, unchanged, as numpy arrays in one compressed file so the
 test suite never needs the reference checkout at run time.
 
 Run once in the build container:  python tests/golden/make_golden.py
+(``--digests``: only the SHA-256 digests of the PETSc files).
 """
 import os
 import sys
@@ -18,6 +19,9 @@ OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "raptor_golden.np
 # MatrixMarket files, kept byte for byte (the reader and writer tests parse
 # and rewrite them); sas_P0 and aniso_S have PETSc twins above
 OUT_MM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "raptor_mm.npz")
+# SHA-256 and size of each PETSc file above (the writer's output must equal
+# the reference's files byte for byte); --digests writes only this file
+OUT_DIGESTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "petsc_digests.json")
 MM_FILES = ["sas_P0", "aniso_S", "aniso"]
 
 MATRICES = [
@@ -56,10 +60,27 @@ def read_petsc(path):
     return m, n, rowptr, cols, vals
 
 
+def write_digests(td):
+    import hashlib
+    import json
+
+    out = {}
+    for name in MATRICES:
+        with open(os.path.join(td, name + ".pm"), "rb") as f:
+            data = f.read()
+        out[name] = {"sha256": hashlib.sha256(data).hexdigest(), "bytes": len(data)}
+    with open(OUT_DIGESTS, "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print("wrote", OUT_DIGESTS)
+
+
 def main():
     td = os.path.join(REF, "test_data")
     if not os.path.isdir(td):
         sys.exit("reference test_data not found at %s" % td)
+    write_digests(td)
+    if "--digests" in sys.argv[1:]:
+        return
     out = {}
     for name in MATRICES:
         m, n, rp, ci, cv = read_petsc(os.path.join(td, name + ".pm"))
