@@ -81,6 +81,11 @@ int rb_vec_scale(rb_vec y, double a);            /* ParVector::scale, vector.cpp
  * init_comm / pack_values (core/comm_pkg.hpp:145-158, core/comm_data.hpp:
  * 257-262, 584).  An index outside x writes NaN. */
 int rb_vec_gather(rb_vec x, const int* idx, int n, double* out);
+/* y[idx[k]] += vals[k] for k < n, idx and vals device pointers: adding the
+ * values a transpose halo exchange receives into the owner's rows, ParComm's
+ * complete_comm_T (core/comm_pkg.hpp:198-211).  The indices of one call must
+ * be distinct (call once per message); an index outside y is skipped. */
+int rb_vec_scatter_add(rb_vec y, const int* idx, const double* vals, int n);
 int rb_vec_dot(rb_vec a, rb_vec b, double* out); /* ParVector::inner_product, par_vector.cpp:101-121 */
 int rb_vec_norm2(rb_vec a, double* out);         /* ParVector::norm(2), par_vector.cpp:88-98 */
 

@@ -118,6 +118,11 @@ class ParVector:
                                       "data": (self.device_ptr(), False), "version": 3}
         return torch.as_tensor(o, device="cuda")
 
+    def scatter_add(self, idx_dev, vals_dev, n):
+        """self[idx[k]] += vals[k] for k < n (device pointers; distinct
+        indices), on the library stream."""
+        check(lib().rb_vec_scatter_add(self.h, C.c_void_p(idx_dev), C.c_void_p(vals_dev), int(n)))
+
     def gather(self, idx_dev, n, out_dev):
         """out[k] = self[idx[k]] for k < n (device pointers), on the library
         stream: a halo exchange's send-buffer packing."""

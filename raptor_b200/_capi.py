@@ -59,6 +59,7 @@ SIGNATURES = {
     "rb_set_stream": (C.c_int, [_P]),
     "rb_synchronize": (C.c_int, []),
     "rb_vec_gather": (C.c_int, [_P, _P, C.c_int, _P]),
+    "rb_vec_scatter_add": (C.c_int, [_P, _P, _P, C.c_int]),
     "rb_petsc_read_host": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(_i64), _P, _P, _P]),
     "rb_petsc_write_host": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _i64, _P, _P, _P]),

@@ -291,6 +291,28 @@ int rb_vec_gather(rb_vec x, const int* idx, int n, double* out) {
     });
 }
 
+// y[idx[k]] += v[k]: adding a transpose exchange's received values into the
+// owner's rows.  The indices of one call must be distinct (one message);
+// an index outside y is skipped.
+__global__ void k_vec_scatter_add(int n, double* __restrict__ y, int ny, const int* __restrict__ idx,
+                                  const double* __restrict__ v) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int j = idx[k];
+    if (j >= 0 && j < ny) y[j] += v[k];
+}
+
+int rb_vec_scatter_add(rb_vec y, const int* idx, const double* vals, int n) {
+    return guarded([&]() -> int {
+        NEED(y);
+        RB_REQUIRE(n >= 0, "negative count");
+        RB_REQUIRE(n == 0 || (idx && vals), "null index or value pointer");
+        if (n) k_vec_scatter_add<<<grid_for(n, 256), 256, 0, stream()>>>(n, y->v.get(), y->n, idx, vals);
+        RB_CHECK_LAUNCH();
+        return RB_OK;
+    });
+}
+
 int rb_vec_scale(rb_vec y, double a) {
     return guarded([&]() -> int {
         NEED(y);

@@ -23,7 +23,7 @@ the library is switched to it), so that the pack, the NCCL transfer, the
 device with no host wait.  The ``on_proc`` product runs while the transfer
 is in flight, as in the reference.
 
-Scope: the distributed products (mult, residual, mult_append), the distributed
+Scope: the distributed products (mult, residual, mult_append, mult_T), the distributed
 dot and norm, and the reference's CG and PCG over them (krylov/par_cg.cpp),
 the PCG preconditioned by one AMG cycle of each partition's own block (block
 Jacobi).  The distributed AMG setup of the reference (C/F splitting across
@@ -220,6 +220,22 @@ class ParComm:
             ops.append(dist.P2POp(dist.isend, send_buf[a:b], q, group=group))
         return dist.batch_isend_irecv(ops) if ops else []
 
+    def exchange_packed_T(self, ghost_buf, recv_buf, group=None):
+        """The transpose exchange (init_comm_T, core/comm_pkg.hpp:187-196):
+        ghost_buf holds values in column-map order, each owner's run sent
+        back to it; recv_buf receives, in send-list order, what the other
+        ranks send for this rank's rows.  Returns the requests."""
+        import torch.distributed as dist
+
+        ops = []
+        for k, q in enumerate(self.send_procs):
+            a, b = int(self.send_ptr[k]), int(self.send_ptr[k + 1])
+            ops.append(dist.P2POp(dist.irecv, recv_buf[a:b], q, group=group))
+        for k, q in enumerate(self.recv_procs):
+            a, b = int(self.recv_ptr[k]), int(self.recv_ptr[k + 1])
+            ops.append(dist.P2POp(dist.isend, ghost_buf[a:b], q, group=group))
+        return dist.batch_isend_irecv(ops) if ops else []
+
 
 class DistParCSRMatrix:
     """This rank's rows of a row-partitioned matrix on its GPU
@@ -245,6 +261,7 @@ class DistParCSRMatrix:
         with _on_stream():
             self.send_idx = torch.as_tensor(comm.send_idx, device="cuda")
             self.send_buf = torch.empty(max(comm.num_send, 1), dtype=torch.float64, device="cuda")
+            self.recv_T = torch.empty(max(comm.num_send, 1), dtype=torch.float64, device="cuda")
         stream().synchronize()
         self.ghost = ParVector(max(self.off_proc_num_cols, 1))
         self.ghost_buf = self.ghost.torch_view()
@@ -294,6 +311,26 @@ class DistParCSRMatrix:
         if self.off_proc is not None:
             self.off_proc.mult_append(self.ghost, b)
 
+    def _add_received_T(self, b):
+        """b[send_idx] += received values, one message after another (a row
+        can arrive from several ranks; within a message rows are distinct)."""
+        c = self.comm
+        for k in range(len(c.send_procs)):
+            a, e = int(c.send_ptr[k]), int(c.send_ptr[k + 1])
+            b.scatter_add(self.send_idx.data_ptr() + 4 * a, self.recv_T.data_ptr() + 8 * a, e - a)
+
+    def mult_T(self, x, b):
+        """b = A^T x (par_spmv.cpp:157-187; A square, x and b partitioned like
+        the rows): off_proc^T x goes back to the owners of those columns
+        while on_proc^T x is formed, then the received values are added."""
+        if self.off_proc is not None:
+            self.off_proc.mult_T(x, self.ghost)
+        with _on_stream():
+            reqs = self.comm.exchange_packed_T(self.ghost_buf, self.recv_T, group=self.group)
+        self.on_proc.mult_T(x, b)
+        self._wait(reqs)
+        self._add_received_T(b)
+
     def residual(self, x, b, r):
         """r = b - A x (par_spmv.cpp:215-252)."""
         reqs = self.start_halo(x)
@@ -342,6 +379,24 @@ class DistParCSRMatrix:
             m.on_proc.mult(x, b)
             if m.off_proc is not None:
                 m.off_proc.mult_append(m.ghost, b)
+
+    @staticmethod
+    def mult_T_in_process(mats, xs, bs):
+        """b_r = (A^T x)_r for every partition r held by this process."""
+        for m, x in zip(mats, xs):
+            if m.off_proc is not None:
+                m.off_proc.mult_T(x, m.ghost)
+        with _on_stream():
+            for q, mq in enumerate(mats):
+                for k, r in enumerate(mq.comm.send_procs):
+                    mr = mats[r]
+                    j = mr.comm.recv_procs.index(q)
+                    a, b = int(mr.comm.recv_ptr[j]), int(mr.comm.recv_ptr[j + 1])
+                    c, d = int(mq.comm.send_ptr[k]), int(mq.comm.send_ptr[k + 1])
+                    mq.recv_T[c:d].copy_(mr.ghost_buf[a:b])
+        for m, x, b in zip(mats, xs, bs):
+            m.on_proc.mult_T(x, b)
+            m._add_received_T(b)
 
     @staticmethod
     def residual_in_process(mats, xs, bs, rs):

@@ -6,7 +6,9 @@ halo exchange (core/comm_pkg.hpp:400-466) over torch.distributed with gloo,
 world sizes 2 and 3.  On every rank the plan built by exchanging index lists
 must equal the plan computed for all ranks in one process, the exchange must
 deliver x at the column map, and on_proc x_local + off_proc x_ghost (taken
-here with numpy, as a check) must be that rank's rows of A x.  The device
+here with numpy, as a check) must be that rank's rows of A x; the transpose
+exchange (off_proc^T x_local sent back to the owners and added into their
+rows) must give that rank's rows of A^T x.  The device
 products are covered by tests/test_gpu_distributed.py.
 """
 import os
@@ -137,8 +139,20 @@ def _rank_main(rank, world, port, kind, out):
         if len(colmap):
             y = y + dense(frp, fci, fcv, len(colmap)) @ ghost
         want = dense(rp, ci, cv, n)[f:l] @ x
+        # transpose: off_proc^T x_local back to the owners, added into their rows
+        t = (dense(frp, fci, fcv, len(colmap)).T @ x[f:l]) if len(colmap) else np.zeros(1)
+        recv_t = torch.zeros(max(plan.num_send, 1), dtype=torch.float64)
+        for w in plan.exchange_packed_T(torch.as_tensor(t), recv_t):
+            w.wait()
+        yt = dense(orp, oci, ocv, l - f).T @ x[f:l]
+        rt = recv_t.numpy()
+        for k in range(len(plan.send_procs)):
+            a, e = plan.send_ptr[k], plan.send_ptr[k + 1]
+            yt[plan.send_idx[a:e]] += rt[a:e]
+        want_t = dense(rp, ci, cv, n).T[f:l] @ x
         np.save(out % rank, np.array([float(same), float(np.array_equal(ghost, x[colmap])),
-                                      float(np.max(np.abs(y - want), initial=0.0))]))
+                                      float(np.max(np.abs(y - want), initial=0.0)),
+                                      float(np.max(np.abs(yt - want_t), initial=0.0))]))
     finally:
         dist.destroy_process_group()
 
@@ -151,7 +165,7 @@ def test_gloo_plan_and_exchange(tmp_path, world, kind):
     mp.start_processes(_rank_main, args=(world, _free_port(), kind, out), nprocs=world,
                        start_method="spawn", join=True)
     for r in range(world):
-        same, ghost_ok, err = np.load(out % r)
+        same, ghost_ok, err, err_t = np.load(out % r)
         assert same == 1.0, "plan differs on rank %d" % r
         assert ghost_ok == 1.0, "halo values wrong on rank %d" % r
-        assert err < 1e-13
+        assert err < 1e-13 and err_t < 1e-13

@@ -7,7 +7,8 @@ device copies with the plan every rank would build) must give the rows of
 A x and b - A x of the whole matrix: on_proc x_local + off_proc x_ghost sums
 a row in another grouping than the single product, so the check is to
 1e-14 of sum_j |a_ij x_j| against an FP64 numpy product and the library's
-own product of the whole matrix.  CG over three partitions must follow the
+own product of the whole matrix (and likewise A^T x, whose off_proc part
+goes back to the owners of the columns).  CG over three partitions must follow the
 library's CG on the whole matrix (histories to 1e-8); PCG over one partition
 with its block-Jacobi AMG (then the whole matrix's AMG) must give the
 library's reference-mode PCG history to 1e-10 (to within one iteration),
@@ -125,6 +126,17 @@ def test_partitions_in_one_process_match_whole_matrix(name, parts):
     D.DistParCSRMatrix.residual_in_process(mats, xs, bs, rs)
     r = np.concatenate([v.numpy() for v in rs])
     assert np.all(np.abs(r - (bvec - want)) <= tol + 1e-15 * np.abs(bvec))
+    # transpose product: off_proc^T x back to the column owners
+    D.DistParCSRMatrix.mult_T_in_process(mats, xs, ys)
+    yt = np.concatenate([v.numpy() for v in ys])
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    want_t = np.zeros(n)
+    np.add.at(want_t, ci, cv * x[rows])
+    scale_t = np.zeros(n)
+    np.add.at(scale_t, ci, np.abs(cv * x[rows]))
+    assert np.all(np.abs(yt - want_t) <= 1e-14 * scale_t + 1e-300)
+    A.mult_T(rb.ParVector(n, values=x), yw)
+    assert np.all(np.abs(yt - yw.numpy()) <= 1e-14 * scale_t + 1e-300)
 
 
 def partitions_of(rp, ci, cv, part):
