@@ -249,6 +249,12 @@ class DistParCSRMatrix:
         self.partition, self.rank, self.group = partition, int(rank), group
         first, last = partition.local_range(rank)
         self.local_num_rows = last - first
+        if self.local_num_rows <= 0:
+            # (the reference allows ranks without rows when n < p; here every
+            # rank's blocks and vectors are device arrays of its rows)
+            raise RaptorError(-1, "rank %d owns no rows: use fewer ranks than rows" % rank)
+        if len(rowptr) != self.local_num_rows + 1:
+            raise RaptorError(-1, "rowptr must have local_num_rows + 1 entries")
         (orp, oci, ocv), (frp, fci, fcv), self.colmap = split_rows(rowptr, cols, vals, first, last)
         self.on_proc = ParCSRMatrix.from_arrays(self.local_num_rows, self.local_num_rows, orp, oci, ocv)
         self.off_proc_num_cols = len(self.colmap)

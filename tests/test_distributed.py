@@ -79,6 +79,17 @@ def test_split_rows_rebuilds_the_rows(first, last):
             assert np.all(np.diff(cib[rpb[i]:rpb[i + 1]]) > 0)
 
 
+def test_rank_without_rows_is_refused():
+    from raptor_b200 import RaptorError
+    from raptor_b200.distributed import DistParCSRMatrix
+
+    part = RowPartition.even(2, 3)   # the last rank owns no rows
+    with pytest.raises(RaptorError):
+        DistParCSRMatrix(part, 2, np.zeros(1, np.int32), [], [])
+    with pytest.raises(RaptorError):   # rows of another size than the partition's
+        DistParCSRMatrix(RowPartition([0, 3]), 0, np.zeros(3, np.int32), [], [])
+
+
 def test_plan_all_sends_what_each_rank_needs():
     rp, ci, cv = stencil_csr(12)
     part = RowPartition.even(144, 3)
