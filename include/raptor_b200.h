@@ -35,6 +35,7 @@ typedef struct rb_csr_s* rb_csr;   /* device CSR matrix, FP64 values, int32 indi
 typedef struct rb_vec_s* rb_vec;   /* device FP64 vector */
 typedef struct rb_amg_s* rb_amg;   /* AMG hierarchy (ParMultilevel) */
 typedef struct rb_batch_s* rb_batch; /* independent systems solved together */
+typedef struct rb_bsr_s* rb_bsr;   /* device block CSR matrix, FP64 blocks, int32 block indices */
 
 /* Description of the last failure on this thread ("" when none). */
 const char* rb_last_error(void);
@@ -64,6 +65,36 @@ int rb_csr_sort_diag_first(rb_csr A);
 /* Transpose with rows of the result in increasing source-row order
  * (CSRMatrix::transpose / CSR_to_CSC, core/matrix.cpp:148-154, :492-538). */
 int rb_csr_transpose(rb_csr A, rb_csr* out);
+
+/* Block CSR (BSRMatrix, core/matrix.hpp:962-1060): n_block_rows x
+ * n_block_cols blocks of b_rows x b_cols values; rowptr (n_block_rows+1) and
+ * cols (nnz_blocks) index blocks, and block j's values are
+ * vals[j*b_rows*b_cols ...], row-major inside the block (the reference's
+ * block_vals[j][r*b_cols + c]).  Copies host (on_device=0, checked) or device
+ * (on_device=1) arrays.  Vectors of a product hold scalar entries:
+ * n_block_cols*b_cols for x, n_block_rows*b_rows for b. */
+int rb_bsr_create(int n_block_rows, int n_block_cols, int b_rows, int b_cols, int64_t nnz_blocks,
+                  const int* rowptr, const int* cols, const double* vals, int on_device,
+                  rb_bsr* out);
+int rb_bsr_destroy(rb_bsr A);
+int rb_bsr_info(rb_bsr A, int* n_block_rows, int* n_block_cols, int* b_rows, int* b_cols,
+                int64_t* nnz_blocks);
+/* Copy the matrix to host buffers of n_block_rows+1, nnz_blocks and
+ * nnz_blocks*b_rows*b_cols entries (a NULL buffer is skipped). */
+int rb_bsr_download(rb_bsr A, int* rowptr, int* cols, double* vals);
+/* b = A x: BSRMatrix::spmv / BSR_spmv (util/linalg/spmv.cpp:121-148, 343-346). */
+int rb_bsr_spmv(rb_bsr A, rb_vec x, rb_vec b);
+/* b += A x: BSRMatrix::spmv_append / BSR_append (spmv.cpp:105-119, 347-350). */
+int rb_bsr_spmv_append(rb_bsr A, rb_vec x, rb_vec b);
+/* r = b - A x: BSRMatrix::spmv_residual (spmv.cpp:363-368). */
+int rb_bsr_residual(rb_bsr A, rb_vec x, rb_vec b, rb_vec r);
+/* b = A^T x: Matrix::mult_T with the block append_T (core/matrix.hpp:342-348,
+ * 299-312).  The first call builds the transposed block pattern on the
+ * handle (host counting sort, then kept); later calls allocate nothing. */
+int rb_bsr_spmv_T(rb_bsr A, rb_vec x, rb_vec b);
+/* Scalar CSR of the matrix, entries with |v| > 1e-16 in the reference's
+ * order: BSRMatrix::to_CSR / BSR_to_CSR (core/matrix.cpp:1180-1185, 358-395). */
+int rb_bsr_to_csr(rb_bsr A, rb_csr* out);
 
 /* ParVector (core/par_vector.hpp:44-176) */
 int rb_vec_create(int n, rb_vec* out);

@@ -165,6 +165,53 @@ inline void write_par_mm(ParCSRMatrix* A, const char* fname) { write_mm(A, fname
 
 /* multilevel/par_multilevel.hpp: the option fields are the C options
  * themselves, so `ml->relax_weight = w` and friends work as in the reference */
+/* BSRMatrix (core/matrix.hpp:962-1060): n_rows x n_cols blocks of b_rows x
+ * b_cols values; block j's values at vals[j*b_rows*b_cols], row-major. */
+class BSRMatrix {
+  public:
+    explicit BSRMatrix(rb_bsr h) : h_(h) {
+        int64_t z = 0;
+        check(rb_bsr_info(h_, &n_rows, &n_cols, &b_rows, &b_cols, &z));
+        nnz = (long)z;
+    }
+    /* host block CSR arrays (copied to the device) */
+    BSRMatrix(int num_block_rows, int num_block_cols, int block_row_size, int block_col_size,
+              const int* rowptr, const int* cols, const double* vals) {
+        check(rb_bsr_create(num_block_rows, num_block_cols, block_row_size, block_col_size,
+                            rowptr[num_block_rows], rowptr, cols, vals, 0, &h_));
+        n_rows = num_block_rows;
+        n_cols = num_block_cols;
+        b_rows = block_row_size;
+        b_cols = block_col_size;
+        nnz = rowptr[num_block_rows];
+    }
+    BSRMatrix(const BSRMatrix&) = delete;
+    BSRMatrix& operator=(const BSRMatrix&) = delete;
+    ~BSRMatrix() { rb_bsr_destroy(h_); }
+
+    rb_bsr handle() const { return h_; }
+    void mult(ParVector& x, ParVector& b) { check(rb_bsr_spmv(h_, x.handle(), b.handle())); }
+    void mult_T(ParVector& x, ParVector& b) { check(rb_bsr_spmv_T(h_, x.handle(), b.handle())); }
+    void mult_append(ParVector& x, ParVector& b) {
+        check(rb_bsr_spmv_append(h_, x.handle(), b.handle()));
+    }
+    void residual(ParVector& x, ParVector& b, ParVector& r) {
+        check(rb_bsr_residual(h_, x.handle(), b.handle(), r.handle()));
+    }
+    /* BSRMatrix::to_CSR (core/matrix.cpp:1180-1185); the caller owns it */
+    ParCSRMatrix* to_CSR() {
+        rb_csr C = nullptr;
+        check(rb_bsr_to_csr(h_, &C));
+        return new ParCSRMatrix(C);
+    }
+
+    int n_rows = 0, n_cols = 0, b_rows = 1, b_cols = 1;
+    long nnz = 0;
+
+  private:
+    rb_bsr h_ = nullptr;
+};
+
 class ParMultilevel {
   public:
     virtual ~ParMultilevel() {

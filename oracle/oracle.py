@@ -65,6 +65,12 @@ def lib():
         for f in ("oc_spmv", "oc_spmv_T", "oc_spmv_append"):
             getattr(L, f).argtypes = [_P, _D, _D]
         L.oc_residual.argtypes = [_P, _D, _D, _D]
+        L.oc_bsr_spmv.argtypes = [C.c_int, C.c_int, C.c_int, _I, _I, _D, _D, _D]
+        L.oc_bsr_append.argtypes = [C.c_int, C.c_int, C.c_int, _I, _I, _D, _D, _D]
+        L.oc_bsr_residual.argtypes = [C.c_int, C.c_int, C.c_int, _I, _I, _D, _D, _D, _D]
+        L.oc_bsr_spmv_T.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _D, _D, _D]
+        L.oc_bsr_to_csr.restype = _P
+        L.oc_bsr_to_csr.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _D]
         L.oc_classical_strength.restype = _P
         L.oc_classical_strength.argtypes = [_P, C.c_double]
         L.oc_symmetric_strength.restype = _P
@@ -216,6 +222,61 @@ def residual(A, x, b):
     lib().oc_residual(A.ptr, np.ascontiguousarray(x, np.float64),
                       np.ascontiguousarray(b, np.float64), r)
     return r
+
+
+class BSR:
+    """Host block CSR: n_rows x n_cols blocks of b_rows x b_cols values,
+    blocks as an (nnz, b_rows, b_cols) array (core/matrix.hpp:962-1060)."""
+
+    def __init__(self, n_rows, n_cols, b_rows, b_cols, rowptr, cols, blocks):
+        self.n_rows, self.n_cols = int(n_rows), int(n_cols)
+        self.b_rows, self.b_cols = int(b_rows), int(b_cols)
+        self.rowptr = np.ascontiguousarray(rowptr, np.int32)
+        self.cols = np.ascontiguousarray(cols, np.int32)
+        self.blocks = np.ascontiguousarray(blocks, np.float64).reshape(
+            len(self.cols), self.b_rows, self.b_cols)
+
+    @property
+    def shape(self):
+        return self.n_rows * self.b_rows, self.n_cols * self.b_cols
+
+    def _args(self):
+        v = self.blocks.reshape(-1) if self.blocks.size else np.zeros(1)
+        c = self.cols if self.cols.size else np.zeros(1, np.int32)
+        return self.rowptr, c, np.ascontiguousarray(v)
+
+
+def bsr_spmv(A, x):
+    b = np.zeros(A.shape[0])
+    lib().oc_bsr_spmv(A.n_rows, A.b_rows, A.b_cols, *A._args(),
+                      np.ascontiguousarray(x, np.float64), b)
+    return b
+
+
+def bsr_append(A, x, b):
+    out = np.array(b, dtype=np.float64)
+    lib().oc_bsr_append(A.n_rows, A.b_rows, A.b_cols, *A._args(),
+                        np.ascontiguousarray(x, np.float64), out)
+    return out
+
+
+def bsr_residual(A, x, b):
+    r = np.zeros(A.shape[0])
+    lib().oc_bsr_residual(A.n_rows, A.b_rows, A.b_cols, *A._args(),
+                          np.ascontiguousarray(x, np.float64),
+                          np.ascontiguousarray(b, np.float64), r)
+    return r
+
+
+def bsr_spmv_T(A, x):
+    b = np.zeros(A.shape[1])
+    lib().oc_bsr_spmv_T(A.n_rows, A.n_cols, A.b_rows, A.b_cols, *A._args(),
+                        np.ascontiguousarray(x, np.float64), b)
+    return b
+
+
+def bsr_to_csr(A):
+    return CSR(lib().oc_bsr_to_csr(A.n_rows, A.n_cols, A.b_rows, A.b_cols, *A._args()))
 
 
 def sort_diag_first(A):
@@ -434,6 +495,12 @@ def ref_lib():
         L.rs_split_cljp.argtypes = [C.c_int, _I, _I, _D, _D, _I]
         L.rs_split_rs.argtypes = [C.c_int, _I, _I, _D, C.c_int, _I]
         L.rs_mis2.argtypes = [C.c_int, _I, _I, _D, _D, _I]
+        L.rs_bsr_apply.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _D, C.c_int, _D,
+                                   _D, _D]
+        L.rs_bsr_to_csr.restype = _P
+        L.rs_bsr_to_csr.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _D]
+        L.rs_bcoo_to_bsr.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _D, _I,
+                                     _I, _D]
         L.rs_interp.restype = _P
         L.rs_interp.argtypes = [C.c_int, _I, _I, _D, _I, _I, _D, _I, C.c_int]
         _ref = L

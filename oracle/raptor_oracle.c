@@ -321,6 +321,98 @@ void oc_spmv_append(const oc_csr* A, const double* x, double* b) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* block CSR (BSRMatrix, core/matrix.hpp:962-1060)                          */
+/* nbr x nbc blocks of br x bc values; block j's values at vals[j*br*bc],   */
+/* row-major (the reference's block_vals[j][r*bc + c]).                     */
+/* ------------------------------------------------------------------------ */
+
+/* BSR_spmv, spmv.cpp:121-148 */
+void oc_bsr_spmv(int nbr, int br, int bc, const int* rowptr, const int* cols,
+                 const double* vals, const double* x, double* b) {
+    const size_t bs = (size_t)br * bc;
+    for (int i = 0; i < nbr; i++) {
+        const int first_row = i * br;
+        for (int row = 0; row < br; row++) {
+            double val = 0;
+            const size_t idx = (size_t)row * bc;
+            for (int j = rowptr[i]; j < rowptr[i + 1]; j++) {
+                const size_t first_col = (size_t)cols[j] * bc;
+                const double* block = vals + (size_t)j * bs;
+                for (int col = 0; col < bc; col++) val += block[idx + col] * x[first_col + col];
+            }
+            b[first_row + row] = val;
+        }
+    }
+}
+
+/* BSR_append with the block Matrix::append, spmv.cpp:105-119,
+ * matrix.hpp:287-298; neg != 0: the block append_neg (matrix.hpp:313-324) */
+static void bsr_append_sign(int nbr, int br, int bc, const int* rowptr, const int* cols,
+                            const double* vals, const double* x, double* b, int neg) {
+    const size_t bs = (size_t)br * bc;
+    for (int i = 0; i < nbr; i++)
+        for (int j = rowptr[i]; j < rowptr[i + 1]; j++) {
+            const size_t first_row = (size_t)i * br, first_col = (size_t)cols[j] * bc;
+            const double* block = vals + (size_t)j * bs;
+            for (int row = 0; row < br; row++)
+                for (int col = 0; col < bc; col++) {
+                    if (neg)
+                        b[first_row + row] -= block[row * bc + col] * x[first_col + col];
+                    else
+                        b[first_row + row] += block[row * bc + col] * x[first_col + col];
+                }
+        }
+}
+
+void oc_bsr_append(int nbr, int br, int bc, const int* rowptr, const int* cols,
+                   const double* vals, const double* x, double* b) {
+    bsr_append_sign(nbr, br, bc, rowptr, cols, vals, x, b, 0);
+}
+
+/* BSRMatrix::spmv_residual, spmv.cpp:363-368 */
+void oc_bsr_residual(int nbr, int br, int bc, const int* rowptr, const int* cols,
+                     const double* vals, const double* x, const double* b, double* r) {
+    for (size_t i = 0; i < (size_t)nbr * br; i++) r[i] = b[i];
+    bsr_append_sign(nbr, br, bc, rowptr, cols, vals, x, r, 1);
+}
+
+/* Matrix::mult_T zero fill (matrix.hpp:342-348), then CSR_append_T over the
+ * blocks (spmv.cpp:150-163) with the block append_T (matrix.hpp:299-312) */
+void oc_bsr_spmv_T(int nbr, int nbc, int br, int bc, const int* rowptr, const int* cols,
+                   const double* vals, const double* x, double* b) {
+    const size_t bs = (size_t)br * bc;
+    for (size_t c = 0; c < (size_t)nbc * bc; c++) b[c] = 0.0;
+    for (int i = 0; i < nbr; i++)
+        for (int j = rowptr[i]; j < rowptr[i + 1]; j++) {
+            const size_t first_row = (size_t)i * br, first_col = (size_t)cols[j] * bc;
+            const double* block = vals + (size_t)j * bs;
+            for (int row = 0; row < br; row++) {
+                const double x_val = x[first_row + row];
+                for (int col = 0; col < bc; col++)
+                    b[first_col + col] += block[row * bc + col] * x_val;
+            }
+        }
+}
+
+/* BSR_to_CSR, core/matrix.cpp:358-395: scalar rows in order, a row's blocks
+ * in storage order, a block row's columns in order, |v| > zero_tol kept */
+oc_csr* oc_bsr_to_csr(int nbr, int nbc, int br, int bc, const int* rowptr, const int* cols,
+                      const double* vals) {
+    const size_t bs = (size_t)br * bc;
+    oc_csr* B = csr_alloc(nbr * br, nbc * bc, rowptr[nbr] > 0 ? rowptr[nbr] : 1);
+    for (int i = 0; i < nbr; i++)
+        for (int row = 0; row < br; row++) {
+            for (int j = rowptr[i]; j < rowptr[i + 1]; j++)
+                for (int col = 0; col < bc; col++) {
+                    const double v = vals[(size_t)j * bs + (size_t)row * bc + col];
+                    if (fabs(v) > ZERO_TOL) csr_push(B, cols[j] * bc + col, v);
+                }
+            B->rowptr[i * br + row + 1] = B->nnz;
+        }
+    return B;
+}
+
+/* ------------------------------------------------------------------------ */
 /* strength of connection (par_strength.cpp)                                */
 /* ------------------------------------------------------------------------ */
 

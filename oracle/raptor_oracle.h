@@ -127,6 +127,19 @@ void oc_residual(const oc_csr* A, const double* x, const double* b, double* r);
 void oc_spmv_T(const oc_csr* A, const double* x, double* b);
 void oc_spmv_append(const oc_csr* A, const double* x, double* b);
 
+/* block CSR: nbr x nbc blocks of br x bc values, block j's values at
+ * vals[j*br*bc], row-major (core/matrix.hpp:962-1060, util/linalg/spmv.cpp) */
+void oc_bsr_spmv(int nbr, int br, int bc, const int* rowptr, const int* cols,
+                 const double* vals, const double* x, double* b);
+void oc_bsr_append(int nbr, int br, int bc, const int* rowptr, const int* cols,
+                   const double* vals, const double* x, double* b);
+void oc_bsr_residual(int nbr, int br, int bc, const int* rowptr, const int* cols,
+                     const double* vals, const double* x, const double* b, double* r);
+void oc_bsr_spmv_T(int nbr, int nbc, int br, int bc, const int* rowptr, const int* cols,
+                   const double* vals, const double* x, double* b);
+oc_csr* oc_bsr_to_csr(int nbr, int nbc, int br, int bc, const int* rowptr, const int* cols,
+                      const double* vals);
+
 /* setup components */
 oc_csr* oc_classical_strength(const oc_csr* A, double theta);
 oc_csr* oc_symmetric_strength(const oc_csr* A, double theta);

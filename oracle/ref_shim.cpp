@@ -6,6 +6,7 @@
 // CSRMatrix, calls the reference routine, and hands the result back as a
 // malloc'd triple that rs_free() releases.  It is used only to cross-check the
 // C restatement in raptor_oracle.c on inputs larger than the golden fixtures.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 
@@ -51,6 +52,27 @@ Out* export_csr(CSRMatrix* A) {
         memcpy(o->vals, A->vals.data(), sizeof(double) * o->nnz);
     }
     return o;
+}
+
+// A reference BSRMatrix holding block CSR arrays (block j's values at
+// vals[j*br*bc], row-major).  The members are filled directly: the
+// (rowptr, cols, data) constructor (core/matrix.hpp:984-993) starts from
+// CSRMatrix(n, m, 0), whose n+1 zero row pointers init_from_lists then
+// appends the given ones to, leaving every block row empty.
+BSRMatrix* make_bsr(int nbr, int nbc, int br, int bc, const int* rp, const int* ci,
+                    const double* v) {
+    BSRMatrix* A = new BSRMatrix(nbr, nbc, br, bc);
+    const int nnz = rp[nbr];
+    std::copy(rp, rp + nbr + 1, A->idx1.begin());
+    A->idx2.assign(ci, ci + nnz);
+    const size_t bs = (size_t)br * bc;
+    for (int j = 0; j < nnz; j++) {
+        double* blk = new double[bs];
+        std::copy(v + j * bs, v + (j + 1) * bs, blk);
+        A->block_vals.push_back(blk);
+    }
+    A->nnz = nnz;
+    return A;
 }
 
 }  // namespace
@@ -179,6 +201,53 @@ Out* rs_interp(int n, const int* arp, const int* aci, const double* acv, const i
     delete S;
     delete P;
     return o;
+}
+
+// Block products through the reference's Matrix templates
+// (core/matrix.hpp:338-368): op 0 mult (out = A x), 1 mult_append (out = b,
+// then += A x), 2 residual (out = b - A x), 3 mult_T (out = A^T x).
+void rs_bsr_apply(int nbr, int nbc, int br, int bc, const int* rp, const int* ci,
+                  const double* v, int op, const double* x, const double* b, double* out) {
+    BSRMatrix* A = make_bsr(nbr, nbc, br, bc, rp, ci, v);
+    double* xp = const_cast<double*>(x);
+    double* bp = const_cast<double*>(b);
+    switch (op) {
+        case 0: A->mult(xp, out); break;
+        case 1:
+            std::copy(b, b + (size_t)nbr * br, out);
+            A->mult_append(xp, out);
+            break;
+        case 2: A->residual(xp, bp, out); break;
+        case 3: A->mult_T(xp, out); break;
+    }
+    delete A;
+}
+
+// BSRMatrix::to_CSR (core/matrix.cpp:1180-1185).
+Out* rs_bsr_to_csr(int nbr, int nbc, int br, int bc, const int* rp, const int* ci,
+                   const double* v) {
+    BSRMatrix* A = make_bsr(nbr, nbc, br, bc, rp, ci, v);
+    CSRMatrix* C = A->to_CSR();
+    Out* o = export_csr(C);
+    delete C;
+    delete A;
+    return o;
+}
+
+// BCOOMatrix::add_value per block, then to_BSR (core/matrix.cpp:1116-1123):
+// the block CSR arrays are written to rp (nbr+1), ci (nnz) and v (nnz*br*bc).
+void rs_bcoo_to_bsr(int nbr, int nbc, int br, int bc, int nnz, const int* rows,
+                    const int* cols, const double* vals, int* rp, int* ci, double* v) {
+    BCOOMatrix* B = new BCOOMatrix(nbr, nbc, br, bc);
+    const size_t bs = (size_t)br * bc;
+    for (int k = 0; k < nnz; k++)
+        B->add_value(rows[k], cols[k], const_cast<double*>(vals + k * bs));
+    BSRMatrix* A = (BSRMatrix*)B->to_BSR();
+    std::copy(A->idx1.begin(), A->idx1.begin() + nbr + 1, rp);
+    std::copy(A->idx2.begin(), A->idx2.begin() + A->nnz, ci);
+    for (int j = 0; j < A->nnz; j++) std::copy(A->block_vals[j], A->block_vals[j] + bs, v + j * bs);
+    delete A;
+    delete B;
 }
 
 }  // extern "C"

@@ -225,6 +225,123 @@ class ParCSRMatrix:
         return ParCSRMatrix(h)
 
 
+def bcoo_to_bsr_arrays(n_rows, b_rows, b_cols, rows, cols, blocks):
+    """Block COO -> block CSR arrays on the host, as BCOOMatrix::to_BSR does
+    (core/matrix.cpp:1116-1123 with COO_to_CSR, :285-330): blocks grouped by
+    block row, in the order they were added within a row.  Returns (rowptr,
+    cols, blocks) with blocks of shape (nnz, b_rows, b_cols)."""
+    rows = np.asarray(rows, dtype=np.int64).reshape(-1)
+    cols = np.asarray(cols, dtype=np.int64).reshape(-1)
+    blocks = np.asarray(blocks, dtype=np.float64).reshape(len(rows), int(b_rows), int(b_cols))
+    if len(cols) != len(rows):
+        raise RaptorError(-1, "rows and cols must have one entry a block")
+    if rows.size and (rows.min() < 0 or rows.max() >= n_rows):
+        raise RaptorError(-1, "block row index out of range")
+    order = np.argsort(rows, kind="stable")
+    rowptr = np.zeros(int(n_rows) + 1, np.int32)
+    rowptr[1:] = np.cumsum(np.bincount(rows, minlength=int(n_rows)))
+    return rowptr, cols[order].astype(np.int32), blocks[order]
+
+
+class BSRMatrix:
+    """Device block CSR matrix (core/matrix.hpp:962-1060): n_rows x n_cols
+    blocks of b_rows x b_cols FP64 values, int32 block indices.  Block j's
+    values are the j-th b_rows x b_cols slice of the value array, row-major
+    (the reference's block_vals[j][r * b_cols + c]).  Products take and give
+    scalar vectors: n_cols * b_cols entries in, n_rows * b_rows out."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def from_arrays(cls, n_rows, n_cols, b_rows, b_cols, rowptr, cols, block_vals):
+        """From block CSR arrays; block_vals holds nnz blocks (any shape with
+        nnz * b_rows * b_cols values, block after block, row-major)."""
+        rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+        ci = np.ascontiguousarray(cols, dtype=np.int32)
+        bv = np.ascontiguousarray(block_vals, dtype=np.float64).reshape(-1)
+        if bv.size != ci.size * int(b_rows) * int(b_cols):
+            raise RaptorError(-1, "block_vals must hold nnz * b_rows * b_cols values")
+        if ci.size == 0:
+            ci = np.zeros(1, np.int32)
+            bv = np.zeros(1, np.float64)
+        h = C.c_void_p()
+        check(lib().rb_bsr_create(int(n_rows), int(n_cols), int(b_rows), int(b_cols), int(rp[-1]),
+                                  _ptr(rp), _ptr(ci), _ptr(bv), 0, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_blocks(cls, n_rows, n_cols, b_rows, b_cols, rows, cols, blocks):
+        """BCOOMatrix::add_value for each (rows[k], cols[k], blocks[k]), then
+        to_BSR (core/matrix.cpp:1116-1123 with COO_to_CSR, :285-330): blocks
+        grouped by block row, in the order they were added within a row."""
+        rowptr, cols, blocks = bcoo_to_bsr_arrays(n_rows, b_rows, b_cols, rows, cols, blocks)
+        return cls.from_arrays(n_rows, n_cols, b_rows, b_cols, rowptr, cols, blocks)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().rb_bsr_destroy(self.h)
+            except Exception:  # noqa: BLE001
+                pass
+            self.h = None
+
+    def info(self):
+        r, c, br, bc, z = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+        check(lib().rb_bsr_info(self.h, C.byref(r), C.byref(c), C.byref(br), C.byref(bc),
+                                C.byref(z)))
+        return r.value, c.value, br.value, bc.value, z.value
+
+    @property
+    def n_rows(self):
+        return self.info()[0]
+
+    @property
+    def n_cols(self):
+        return self.info()[1]
+
+    @property
+    def b_rows(self):
+        return self.info()[2]
+
+    @property
+    def b_cols(self):
+        return self.info()[3]
+
+    @property
+    def nnz(self):
+        return self.info()[4]
+
+    def arrays(self):
+        """(rowptr, cols, blocks) on the host; blocks has shape (nnz, b_rows, b_cols)."""
+        n, _, br, bc, z = self.info()
+        rp = np.zeros(n + 1, np.int32)
+        ci = np.zeros(max(z, 1), np.int32)
+        bv = np.zeros(max(z * br * bc, 1), np.float64)
+        check(lib().rb_bsr_download(self.h, _ptr(rp), _ptr(ci), _ptr(bv)))
+        return rp, ci[:z], bv[: z * br * bc].reshape(z, br, bc)
+
+    # Matrix::mult / mult_T / mult_append / residual (core/matrix.hpp:338-368)
+    def mult(self, x, b):
+        check(lib().rb_bsr_spmv(self.h, x.h, b.h))
+
+    def mult_T(self, x, b):
+        check(lib().rb_bsr_spmv_T(self.h, x.h, b.h))
+
+    def mult_append(self, x, b):
+        check(lib().rb_bsr_spmv_append(self.h, x.h, b.h))
+
+    def residual(self, x, b, r):
+        check(lib().rb_bsr_residual(self.h, x.h, b.h, r.h))
+
+    def to_CSR(self):
+        """BSRMatrix::to_CSR (core/matrix.cpp:1180-1185): the scalar matrix,
+        entries with |v| > 1e-16, unsorted as the reference leaves them."""
+        h = C.c_void_p()
+        check(lib().rb_bsr_to_csr(self.h, C.byref(h)))
+        return ParCSRMatrix(h)
+
+
 # gallery ---------------------------------------------------------------------
 def diffusion_stencil_2d(eps=1.0, theta=0.0):
     out = np.zeros(9)

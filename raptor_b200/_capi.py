@@ -71,6 +71,17 @@ SIGNATURES = {
     "rb_csr_device_arrays": (C.c_int, [_P, _PP, _PP, _PP]),
     "rb_csr_sort_diag_first": (C.c_int, [_P]),
     "rb_csr_transpose": (C.c_int, [_P, _PP]),
+    "rb_bsr_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _i64, _P, _P, _P, C.c_int,
+                                _PP]),
+    "rb_bsr_destroy": (C.c_int, [_P]),
+    "rb_bsr_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                              C.POINTER(C.c_int), C.POINTER(_i64)]),
+    "rb_bsr_download": (C.c_int, [_P, _P, _P, _P]),
+    "rb_bsr_spmv": (C.c_int, [_P, _P, _P]),
+    "rb_bsr_spmv_append": (C.c_int, [_P, _P, _P]),
+    "rb_bsr_residual": (C.c_int, [_P, _P, _P, _P]),
+    "rb_bsr_spmv_T": (C.c_int, [_P, _P, _P]),
+    "rb_bsr_to_csr": (C.c_int, [_P, _PP]),
     "rb_vec_create": (C.c_int, [C.c_int, _PP]),
     "rb_vec_destroy": (C.c_int, [_P]),
     "rb_vec_size": (C.c_int, [_P, C.POINTER(C.c_int)]),

@@ -4,7 +4,8 @@
 
 Every ``csrc/*.cu`` file is compiled with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; the setup kernels
-(``setup.cu``, ``aggregation.cu``) add ``-fmad=false`` so FP64 products and sums round separately
+(``setup.cu``, ``aggregation.cu``) and the block CSR products (``bsr.cu``) add
+``-fmad=false`` so FP64 products and sums round separately
 as in the reference's x86-64 build.  Objects go to ``raptor_b200/_build`` and
 the library to ``raptor_b200/libraptor_b200.so`` (git-ignored, shipped with the
 working tree).
@@ -26,7 +27,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr",
                  "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
                  "-I", CSRC, "-I", INCLUDE]
-PER_FILE = {"setup.cu": ["-fmad=false"], "aggregation.cu": ["-fmad=false"]}
+PER_FILE = {"setup.cu": ["-fmad=false"], "aggregation.cu": ["-fmad=false"],
+            "bsr.cu": ["-fmad=false"]}
 
 
 def nvcc():

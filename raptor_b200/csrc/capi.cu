@@ -5,6 +5,7 @@
 // boundary.  There is no host fallback: without a device every compute call
 // fails with RB_ERR_NO_DEVICE.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -12,6 +13,7 @@
 #include <vector>
 
 #include "blas1.cuh"
+#include "bsr.cuh"
 #include "hierarchy.cuh"
 #include "rb_internal.cuh"
 
@@ -380,6 +382,135 @@ int rb_spmv_append(rb_csr A, rb_vec x, rb_vec b) {
         NEED(A); NEED(x); NEED(b);
         RB_REQUIRE(x->n == A->n_cols && b->n == A->n_rows, "spmv_append: sizes do not match");
         spmv_append64(view(*A), x->v.get(), b->v.get(), handle_lanes(*A, x->v.get()));
+        return RB_OK;
+    });
+}
+
+// ---------------------------------------------------------- block CSR --
+int rb_bsr_create(int n_block_rows, int n_block_cols, int b_rows, int b_cols, int64_t nnz,
+                  const int* rowptr, const int* cols, const double* vals, int on_device,
+                  rb_bsr* out) {
+    return guarded([&]() -> int {
+        ensure_device();
+        NEED(out); NEED(rowptr);
+        RB_REQUIRE(n_block_rows >= 0 && n_block_cols >= 0 && nnz >= 0, "negative matrix dimension");
+        RB_REQUIRE(b_rows >= 1 && b_cols >= 1, "block dimensions must be at least 1");
+        RB_REQUIRE((long long)n_block_rows * b_rows <= INT_MAX &&
+                       (long long)n_block_cols * b_cols <= INT_MAX,
+                   "scalar dimension exceeds the int32 index range");
+        RB_REQUIRE(nnz <= INT_MAX, "more than 2^31-1 blocks (int32 indices)");
+        RB_REQUIRE(nnz == 0 || (cols && vals), "cols/vals are NULL");
+        if (!on_device) {
+            RB_REQUIRE(rowptr[0] == 0 && rowptr[n_block_rows] == nnz, "rowptr does not span the blocks");
+            for (int i = 0; i < n_block_rows; i++)
+                RB_REQUIRE(rowptr[i] <= rowptr[i + 1], "rowptr is not monotone");
+            for (int64_t j = 0; j < nnz; j++)
+                RB_REQUIRE(cols[j] >= 0 && cols[j] < n_block_cols, "block column index out of range");
+        }
+        const size_t bs = (size_t)b_rows * b_cols;
+        std::unique_ptr<rb_bsr_s> A(new rb_bsr_s());
+        A->n_block_rows = n_block_rows;
+        A->n_block_cols = n_block_cols;
+        A->b_rows = b_rows;
+        A->b_cols = b_cols;
+        A->nnz = nnz;
+        A->rowptr.alloc((size_t)n_block_rows + 1);
+        A->cols.alloc(nnz > 0 ? (size_t)nnz : 1);
+        A->vals.alloc(nnz > 0 ? (size_t)nnz * bs : 1);
+        auto kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        RB_CUDA(cudaMemcpyAsync(A->rowptr.get(), rowptr, sizeof(int) * ((size_t)n_block_rows + 1),
+                                kind, stream()));
+        if (nnz) {
+            RB_CUDA(cudaMemcpyAsync(A->cols.get(), cols, sizeof(int) * (size_t)nnz, kind, stream()));
+            RB_CUDA(cudaMemcpyAsync(A->vals.get(), vals, sizeof(double) * (size_t)nnz * bs, kind,
+                                    stream()));
+        }
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        *out = A.release();
+        return RB_OK;
+    });
+}
+
+int rb_bsr_destroy(rb_bsr A) {
+    return guarded([&]() -> int {
+        delete A;
+        return RB_OK;
+    });
+}
+
+int rb_bsr_info(rb_bsr A, int* n_block_rows, int* n_block_cols, int* b_rows, int* b_cols,
+                int64_t* nnz_blocks) {
+    return guarded([&]() -> int {
+        NEED(A);
+        if (n_block_rows) *n_block_rows = A->n_block_rows;
+        if (n_block_cols) *n_block_cols = A->n_block_cols;
+        if (b_rows) *b_rows = A->b_rows;
+        if (b_cols) *b_cols = A->b_cols;
+        if (nnz_blocks) *nnz_blocks = A->nnz;
+        return RB_OK;
+    });
+}
+
+int rb_bsr_download(rb_bsr A, int* rowptr, int* cols, double* vals) {
+    return guarded([&]() -> int {
+        NEED(A);
+        if (rowptr) A->rowptr.download(rowptr, (size_t)A->n_block_rows + 1);
+        if (cols) A->cols.download(cols, (size_t)A->nnz);
+        if (vals) A->vals.download(vals, (size_t)A->nnz * A->b_rows * A->b_cols);
+        RB_CUDA(cudaStreamSynchronize(stream()));
+        return RB_OK;
+    });
+}
+
+int rb_bsr_spmv(rb_bsr A, rb_vec x, rb_vec b) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_block_cols * A->b_cols && b->n == A->n_block_rows * A->b_rows,
+                   "bsr spmv: sizes do not match");
+        RB_REQUIRE(x != b, "bsr spmv: x and b must be different vectors");
+        bsr_apply(*A, kBsrMult, x->v.get(), nullptr, b->v.get());
+        return RB_OK;
+    });
+}
+
+int rb_bsr_spmv_append(rb_bsr A, rb_vec x, rb_vec b) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_block_cols * A->b_cols && b->n == A->n_block_rows * A->b_rows,
+                   "bsr spmv_append: sizes do not match");
+        RB_REQUIRE(x != b, "bsr spmv_append: x and b must be different vectors");
+        bsr_apply(*A, kBsrAppend, x->v.get(), b->v.get(), b->v.get());
+        return RB_OK;
+    });
+}
+
+int rb_bsr_residual(rb_bsr A, rb_vec x, rb_vec b, rb_vec r) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b); NEED(r);
+        RB_REQUIRE(x->n == A->n_block_cols * A->b_cols && b->n == A->n_block_rows * A->b_rows &&
+                       r->n == b->n,
+                   "bsr residual: sizes do not match");
+        RB_REQUIRE(x != r, "bsr residual: x and r must be different vectors");
+        bsr_apply(*A, kBsrResidual, x->v.get(), b->v.get(), r->v.get());
+        return RB_OK;
+    });
+}
+
+int rb_bsr_spmv_T(rb_bsr A, rb_vec x, rb_vec b) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(x); NEED(b);
+        RB_REQUIRE(x->n == A->n_block_rows * A->b_rows && b->n == A->n_block_cols * A->b_cols,
+                   "bsr spmv_T: sizes do not match");
+        RB_REQUIRE(x != b, "bsr spmv_T: x and b must be different vectors");
+        bsr_spmv_T(*A, x->v.get(), b->v.get());
+        return RB_OK;
+    });
+}
+
+int rb_bsr_to_csr(rb_bsr A, rb_csr* out) {
+    return guarded([&]() -> int {
+        NEED(A); NEED(out);
+        *out = bsr_to_csr(*A);
         return RB_OK;
     });
 }

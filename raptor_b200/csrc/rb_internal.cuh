@@ -28,6 +28,17 @@ struct rb_csr_s {
 
 struct rb_batch_s;
 
+// Block CSR: block j's values at vals[j * b_rows * b_cols], row-major.
+struct rb_bsr_s {
+    int n_block_rows = 0, n_block_cols = 0, b_rows = 1, b_cols = 1;
+    long long nnz = 0;  // blocks
+    rb::DevArray<int> rowptr, cols;
+    rb::DevArray<double> vals;
+    // block pattern of A^T (rows: block columns; entries: source block row
+    // and source block), built by the first transposed product
+    std::unique_ptr<rb::TransposeMap> tmap;
+};
+
 struct rb_vec_s {
     int n = 0;
     rb::DevArray<double> v;
@@ -90,6 +101,14 @@ void spmv_append64(const CsrView<double>& A, const double* x, double* y, int lan
 int handle_lanes(rb_csr_s& A, const double* x);
 // y = A^T x through the handle's cached transpose map (built on first use).
 void spmv_T64(rb_csr_s& A, const double* x, double* y);
+
+// Block CSR products and expansion (bsr.cu).  op: kBsrMult (y = A x, b
+// unused), kBsrAppend (y = b + A x, b may be y), kBsrResidual (y = b - A x).
+void bsr_apply(const rb_bsr_s& A, int op, const double* x, const double* b, double* y);
+// y = A^T x (builds A.tmap on first use).
+void bsr_spmv_T(rb_bsr_s& A, const double* x, double* y);
+// Scalar CSR of A, entries with |v| > 1e-16, in the reference's order.
+rb_csr_s* bsr_to_csr(const rb_bsr_s& A);
 
 // Setup components (setup.cu).
 // vars (the unknown-based systems form, num_variables > 1; NULL otherwise):
