@@ -85,6 +85,9 @@ def parse():
     p.add_argument("--plain-size", type=int, default=128,
                    help="grid side of the all-FP64 plain-method workload with its "
                         "SpMV and V-cycle bandwidth figures (0 skips it)")
+    p.add_argument("--bsr-cases", default="96x3,112x2,64x4",
+                   help="block CSR product workloads as grid-side x block-size, "
+                        "comma-separated (empty skips them)")
     return p.parse_args()
 
 
@@ -395,6 +398,67 @@ def run_plain_fp64(rb, ev, sync, S, steps=3):
             "vcycle": {"ms": cyc_ms, "alg_bytes": cb,
                        "gbs": cb / (cyc_ms * 1e-3) / 1e9,
                        "frac_of_%s_peak" % kind: cb / (cyc_ms * 1e-3) / 1e9 / peak}}
+
+
+def block_stencil_pattern(m):
+    """Block pattern of a periodic 7-point stencil on an m^3 grid of blocks:
+    every block row holds 7 blocks (itself first, then its six neighbours)."""
+    idx = np.arange(m ** 3).reshape(m, m, m)
+    cols = [np.roll(idx, (-dz, -dy, -dx), axis=(0, 1, 2)).reshape(-1)
+            for dz, dy, dx in [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0),
+                               (0, 0, -1), (0, 0, 1)]]
+    cols = np.stack(cols, axis=1).astype(np.int32).reshape(-1)
+    rowptr = (np.arange(m ** 3 + 1) * 7).astype(np.int32)
+    return rowptr, cols
+
+
+def run_block_csr(rb, ev, sync, cases, reps=40):
+    """Block CSR (BSRMatrix) products: b = A x and b = A^T x on a 7-point
+    block pattern with b x b blocks of uniform values, and b = A x on the
+    same matrix expanded to CSR (to_CSR).  Algorithmic bytes of the block
+    product: the blocks (b^2 8 + 4 B each), the row pointers, x and b."""
+    peak, kind = peaks()
+    out = []
+    for m, bsz in cases:
+        rowptr, cols = block_stencil_pattern(m)
+        nb = m ** 3
+        vals = np.random.default_rng(SEED).uniform(-1.0, 1.0, len(cols) * bsz * bsz)
+        A = rb.BSRMatrix.from_arrays(nb, nb, bsz, bsz, rowptr, cols, vals)
+        n = nb * bsz
+        x = rb.ParVector(n, values=np.random.default_rng(SEED + 1).uniform(-1.0, 1.0, n))
+        y = rb.ParVector(n)
+
+        def timed(f):
+            for _ in range(5):
+                f()
+            sync()
+            e0 = ev()
+            for _ in range(reps):
+                f()
+            e1 = ev()
+            sync()
+            return e0.elapsed_time(e1) / reps
+
+        alg = len(cols) * (bsz * bsz * 8 + 4) + (nb + 1) * 4 + 2 * n * 8
+        mult_ms = timed(lambda: A.mult(x, y))
+        mult_t_ms = timed(lambda: A.mult_T(x, y))
+        Acsr = A.to_CSR()
+        z = Acsr.local_nnz
+        csr_alg = z * 12 + (n + 1) * 4 + 2 * n * 8
+        csr_ms = timed(lambda: Acsr.mult(x, y))
+        out.append({"grid": "%d^3 blocks" % m, "block": "%dx%d" % (bsz, bsz),
+                    "block_rows": nb, "blocks": len(cols), "alg_bytes": alg,
+                    "mult_ms": mult_ms, "mult_gbs": alg / (mult_ms * 1e-3) / 1e9,
+                    "mult_frac_of_%s_peak" % kind: alg / (mult_ms * 1e-3) / 1e9 / peak,
+                    "mult_T_ms": mult_t_ms,
+                    "mult_T_gbs": alg / (mult_t_ms * 1e-3) / 1e9,
+                    "csr_nnz": z, "csr_alg_bytes": csr_alg, "csr_mult_ms": csr_ms,
+                    "csr_mult_gbs": csr_alg / (csr_ms * 1e-3) / 1e9,
+                    "bsr_speedup_over_csr": csr_ms / mult_ms})
+        del A, Acsr, x, y
+    return {"workload": "BSRMatrix products on a periodic 7-point block pattern, FP64 "
+                        "blocks ~ U[-1, 1]; CSR product of the same matrix after to_CSR",
+            "cases": out}
 
 
 def run_uneven_batch(rb, ev, sync, count=64, steps=2):
@@ -753,6 +817,12 @@ def run_b200(args, rank, world, local):
     if args.plain_size > 0:
         out["plain_fp64"] = run_plain_fp64(rb, ev, lambda: rb.lib().rb_synchronize(),
                                            args.plain_size)
+    if args.bsr_cases:
+        cases = [tuple(int(v) for v in c.split("x")) for c in args.bsr_cases.split(",")]
+        try:
+            out["block_csr"] = run_block_csr(rb, ev, lambda: rb.lib().rb_synchronize(), cases)
+        except Exception as e:  # noqa: BLE001 - a side workload must not void the line
+            out["block_csr"] = {"error": str(e)}
     if rank == 0 and args.cpu_sample > 0:
         out["cpu_baseline"], x_ref = cpu_baseline(ml32, bh, args.cpu_sample, S)
         if x_ref is not None:
