@@ -19,7 +19,8 @@ namespace rb {
 namespace {
 
 constexpr int kBsrBlock = 256;
-// six resident blocks an SM (1536 threads): 40 registers, no spills
+// six resident blocks an SM (1536 threads): 40 registers; the append and
+// residual forms keep one 8-byte value on the stack
 constexpr int kBsrMinBlocks = 6;
 
 template <int OP>

@@ -61,6 +61,25 @@ RB_HD inline double bsr_row(int row, int br, int bc, const int* rowptr, const in
     for (int j = rowptr[i]; j < rowptr[i + 1]; j++) {
         const double* blk = vals + (size_t)j * bs + (size_t)r * bc;
         const double* xx = x + (size_t)cols[j] * bc;
+#if defined(__CUDA_ARCH__)
+        // even block width: a block row and its x slice start on 16-byte
+        // boundaries (cudaMalloc'd arrays), so they load as double2 pairs;
+        // the products are added in the same order as below
+        if ((bc & 1) == 0) {
+            for (int c = 0; c < bc; c += 2) {
+                const double2 v = *reinterpret_cast<const double2*>(blk + c);
+                const double2 w = *reinterpret_cast<const double2*>(xx + c);
+                if (OP == kBsrResidual) {
+                    acc -= v.x * w.x;
+                    acc -= v.y * w.y;
+                } else {
+                    acc += v.x * w.x;
+                    acc += v.y * w.y;
+                }
+            }
+            continue;
+        }
+#endif
         for (int c = 0; c < bc; c++) {
             if (OP == kBsrResidual)
                 acc -= blk[c] * xx[c];
