@@ -499,6 +499,9 @@ def ref_lib():
                                    _D, _D]
         L.rs_bsr_to_csr.restype = _P
         L.rs_bsr_to_csr.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _D]
+        L.rs_bsr_sort_diag_first.restype = C.c_int
+        L.rs_bsr_sort_diag_first.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _D, _I,
+                                             _I, _D]
         L.rs_bcoo_to_bsr.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _D, _I,
                                      _I, _D]
         L.rs_interp.restype = _P

@@ -234,6 +234,27 @@ Out* rs_bsr_to_csr(int nbr, int nbc, int br, int bc, const int* rp, const int* c
     return o;
 }
 
+// BSRMatrix::sort, move_diag, remove_duplicates (the order of the
+// reference's test_block_matrix.cpp); writes the result, returns its blocks.
+// The block pointers are released here, not by the destructor: dropping a
+// block in remove_duplicates_helper copies pointers between slots.
+int rs_bsr_sort_diag_first(int nbr, int nbc, int br, int bc, const int* rp, const int* ci,
+                           const double* v, int* out_rp, int* out_ci, double* out_v) {
+    BSRMatrix* A = make_bsr(nbr, nbc, br, bc, rp, ci, v);
+    A->sort();
+    A->move_diag();
+    A->remove_duplicates();
+    const size_t bs = (size_t)br * bc;
+    std::copy(A->idx1.begin(), A->idx1.begin() + nbr + 1, out_rp);
+    std::copy(A->idx2.begin(), A->idx2.begin() + A->nnz, out_ci);
+    for (int j = 0; j < A->nnz; j++)
+        std::copy(A->block_vals[j], A->block_vals[j] + bs, out_v + j * bs);
+    const int nnz = A->nnz;
+    A->block_vals.clear();
+    delete A;
+    return nnz;
+}
+
 // BCOOMatrix::add_value per block, then to_BSR (core/matrix.cpp:1116-1123):
 // the block CSR arrays are written to rp (nbr+1), ci (nnz) and v (nnz*br*bc).
 void rs_bcoo_to_bsr(int nbr, int nbc, int br, int bc, int nnz, const int* rows,

@@ -243,6 +243,39 @@ def bcoo_to_bsr_arrays(n_rows, b_rows, b_cols, rows, cols, blocks):
     return rowptr, cols[order].astype(np.int32), blocks[order]
 
 
+def bsr_sort_diag_first(n_rows, b_rows, b_cols, rowptr, cols, blocks):
+    """BSRMatrix::sort, move_diag and remove_duplicates on host block CSR
+    arrays (core/matrix.cpp:588-618 sort_helper, :730-786 move_diag_helper,
+    remove_duplicates_helper): a block row's blocks ordered by block column
+    with the diagonal block (column == row) first, blocks whose absolute
+    entries sum below 1e-16 dropped.  Blocks of one column in one row are
+    summed entry by entry, in storage order; the reference's block
+    append_vals (core/matrix.hpp:219-226) adds the first entries of the
+    following blocks instead, so rows with repeated columns differ from it
+    there.  Returns (rowptr, cols, blocks), blocks of shape (nnz, b_rows,
+    b_cols)."""
+    rp = np.asarray(rowptr, dtype=np.int64)
+    ci = np.asarray(cols, dtype=np.int64)
+    bs = int(b_rows) * int(b_cols)
+    bl = np.asarray(blocks, dtype=np.float64).reshape(len(ci), bs)
+    rows = np.repeat(np.arange(int(n_rows)), np.diff(rp))
+    order = np.lexsort((ci, rows))                      # stable: storage order among equals
+    rows, ci, bl = rows[order], ci[order], bl[order]
+    if len(ci):
+        first = np.ones(len(ci), bool)
+        first[1:] = (rows[1:] != rows[:-1]) | (ci[1:] != ci[:-1])
+        starts = np.nonzero(first)[0]
+        bl = np.add.reduceat(bl, starts, axis=0)
+        rows, ci = rows[starts], ci[starts]
+        keep = np.abs(bl).sum(axis=1) >= 1e-16
+        rows, ci, bl = rows[keep], ci[keep], bl[keep]
+        order = np.lexsort((ci, ci != rows, rows))      # diagonal block first
+        rows, ci, bl = rows[order], ci[order], bl[order]
+    out_rp = np.zeros(int(n_rows) + 1, np.int32)
+    out_rp[1:] = np.cumsum(np.bincount(rows, minlength=int(n_rows)))
+    return out_rp, ci.astype(np.int32), bl.reshape(len(ci), int(b_rows), int(b_cols))
+
+
 class BSRMatrix:
     """Device block CSR matrix (core/matrix.hpp:962-1060): n_rows x n_cols
     blocks of b_rows x b_cols FP64 values, int32 block indices.  Block j's
@@ -333,6 +366,14 @@ class BSRMatrix:
 
     def residual(self, x, b, r):
         check(lib().rb_bsr_residual(self.h, x.h, b.h, r.h))
+
+    def sort_diag_first(self):
+        """BSRMatrix::sort, move_diag and remove_duplicates (see
+        bsr_sort_diag_first, done on the host): a new matrix."""
+        n, m, br, bc, _ = self.info()
+        rp, ci, bl = self.arrays()
+        rp, ci, bl = bsr_sort_diag_first(n, br, bc, rp, ci, bl)
+        return BSRMatrix.from_arrays(n, m, br, bc, rp, ci, bl)
 
     def to_CSR(self):
         """BSRMatrix::to_CSR (core/matrix.cpp:1180-1185): the scalar matrix,

@@ -7,7 +7,10 @@ Three layers are checked here, each bit for bit:
   * the per-row code the CUDA kernels run (raptor_b200/csrc/bsr.cuh), built
     for the host, against the restatement;
   * the host block COO -> block CSR conversion of the Python mirror against
-    the reference's BCOOMatrix::to_BSR.
+    the reference's BCOOMatrix::to_BSR, and its sort / move_diag /
+    remove_duplicates against the reference's (rows with distinct block
+    columns; repeated ones are summed entry by entry, which the reference's
+    block append_vals does not do).
 The reference's own known-answer test for block matrices
 (raptor/core/tests/test_block_matrix.cpp) is replayed on its fixture
 (tests/golden/block_matrix.json): the block and the scalar forms of its
@@ -233,3 +236,76 @@ def test_bsr_host_conversion_checks_its_input():
         rb.bcoo_to_bsr_arrays(2, 1, 1, [0, 2], [0, 0], [1.0, 2.0])
     with pytest.raises(rb.RaptorError):
         rb.bcoo_to_bsr_arrays(2, 1, 1, [0, 1], [0], [1.0, 2.0])
+
+
+# ------------------------------------------- sort, move_diag, remove_duplicates --
+def random_distinct_bsr(nb, br, bc, seed):
+    """Square block matrix whose block rows hold distinct block columns in
+    random order (the diagonal block in about half of them), with all-zero
+    blocks and blocks whose entries sum below the 1e-16 drop tolerance."""
+    rng = np.random.default_rng(seed)
+    rowptr, cols, blocks = [0], [], []
+    for i in range(nb):
+        k = int(rng.integers(0, 7))
+        c = rng.choice(nb, size=min(k, nb), replace=False)
+        if rng.random() < 0.5 and i not in c:
+            c = np.append(c, i)
+        rng.shuffle(c)
+        cols.extend(c.tolist())
+        rowptr.append(len(cols))
+    blocks = rng.uniform(-1, 1, (len(cols), br, bc))
+    pick = rng.random(len(cols))
+    blocks[pick < 0.1] = 0.0
+    blocks[(pick >= 0.1) & (pick < 0.15)] = 1e-18
+    return O.BSR(nb, nb, br, bc, rowptr, cols, blocks)
+
+
+@pytest.mark.parametrize("br,bc", [(1, 1), (2, 2), (3, 2)])
+def test_sort_diag_first_equals_reference(ref, br, bc):
+    A = random_distinct_bsr(60, br, bc, seed=br * 7 + bc)
+    rp, ci, v = A._args()
+    z = len(A.cols)
+    out_rp = np.zeros(A.n_rows + 1, np.int32)
+    out_ci = np.zeros(max(z, 1), np.int32)
+    out_v = np.zeros(max(z * br * bc, 1))
+    nnz = ref.rs_bsr_sort_diag_first(A.n_rows, A.n_cols, br, bc, rp, ci, v, out_rp, out_ci, out_v)
+    hrp, hci, hv = rb.bsr_sort_diag_first(A.n_rows, br, bc, A.rowptr, A.cols, A.blocks)
+    np.testing.assert_array_equal(hrp, out_rp)
+    np.testing.assert_array_equal(hci, out_ci[:nnz])
+    np.testing.assert_array_equal(hv.reshape(-1), out_v[:nnz * br * bc])
+
+
+def test_sort_diag_first_sums_repeated_blocks():
+    """Repeated block columns are summed entry by entry (where the reference
+    adds the wrong entries): the matrix is unchanged, each row holds distinct
+    columns with the diagonal block first, the rest in increasing order."""
+    A = random_bsr(40, 40, 2, 3, seed=17, per_row=5)
+    rp, ci, bl = rb.bsr_sort_diag_first(A.n_rows, 2, 3, A.rowptr, A.cols, A.blocks)
+    B = O.BSR(40, 40, 2, 3, rp, ci, bl)
+    np.testing.assert_allclose(O.bsr_to_csr(B).to_scipy().toarray(),
+                               O.bsr_to_csr(A).to_scipy().toarray(), rtol=0, atol=1e-15)
+    for i in range(40):
+        row = ci[rp[i]:rp[i + 1]].tolist()
+        rest = row[1:] if row and row[0] == i else row
+        assert i not in rest and rest == sorted(set(rest))
+    assert np.all(np.abs(bl).reshape(len(ci), -1).sum(axis=1) >= 1e-16)
+
+
+def test_fixture_sort_diag_first_equals_reference(ref):
+    """test_block_matrix.cpp sorts, moves the diagonal and removes duplicates
+    of its block matrix before comparing it with the scalar form."""
+    _, A, dense, _ = fixture_matrices()
+    rp, ci, v = A._args()
+    z = len(A.cols)
+    out_rp = np.zeros(A.n_rows + 1, np.int32)
+    out_ci = np.zeros(z, np.int32)
+    out_v = np.zeros(z * A.b_rows * A.b_cols)
+    nnz = ref.rs_bsr_sort_diag_first(A.n_rows, A.n_cols, A.b_rows, A.b_cols, rp, ci, v, out_rp,
+                                     out_ci, out_v)
+    hrp, hci, hv = rb.bsr_sort_diag_first(A.n_rows, A.b_rows, A.b_cols, A.rowptr, A.cols,
+                                          A.blocks)
+    np.testing.assert_array_equal(hrp, out_rp)
+    np.testing.assert_array_equal(hci, out_ci[:nnz])
+    np.testing.assert_array_equal(hv.reshape(-1), out_v[:nnz * A.b_rows * A.b_cols])
+    B = O.BSR(A.n_rows, A.n_cols, A.b_rows, A.b_cols, hrp, hci, hv)
+    np.testing.assert_array_equal(O.bsr_to_csr(B).to_scipy().toarray(), dense)
