@@ -293,6 +293,11 @@ class BSRMatrix:
         rp = np.ascontiguousarray(rowptr, dtype=np.int32)
         ci = np.ascontiguousarray(cols, dtype=np.int32)
         bv = np.ascontiguousarray(block_vals, dtype=np.float64).reshape(-1)
+        # the C ABI reads rowptr[n_rows] and nnz entries: refuse short arrays here
+        if rp.size != int(n_rows) + 1:
+            raise RaptorError(-1, "rowptr must have n_rows + 1 entries")
+        if ci.size != int(rp[-1]):
+            raise RaptorError(-1, "cols must have rowptr[n_rows] entries")
         if bv.size != ci.size * int(b_rows) * int(b_cols):
             raise RaptorError(-1, "block_vals must hold nnz * b_rows * b_cols values")
         if ci.size == 0:

@@ -231,6 +231,17 @@ def test_bsr_entry_points_refuse_without_a_device():
     assert e.value.code == -6
 
 
+def test_bsr_arrays_are_checked_before_any_device_call():
+    """Short arrays are refused by the mirror (RB_ERR_INVALID), so the C ABI
+    never reads past them; no device is needed to see it."""
+    for args in [(2, 2, 1, 1, [0, 1], [0], [1.0]),            # rowptr too short
+                 (1, 2, 1, 1, [0, 2], [0], [1.0]),            # cols too short
+                 (1, 2, 2, 2, [0, 1], [1], np.ones(3))]:      # values too short
+        with pytest.raises(rb.RaptorError) as e:
+            rb.BSRMatrix.from_arrays(*args)
+        assert e.value.code == -1
+
+
 def test_bsr_host_conversion_checks_its_input():
     with pytest.raises(rb.RaptorError):
         rb.bcoo_to_bsr_arrays(2, 1, 1, [0, 2], [0, 0], [1.0, 2.0])
