@@ -108,6 +108,31 @@ def split_rows(rowptr, cols, vals, first, last):
     return on_blk, off_blk, colmap.astype(np.int64)
 
 
+def global_rows(on, off, first, colmap):
+    """A rank's rows with global column indices, each row's on_proc entries
+    then its off_proc entries: the rows CommPkg::init_par_mat_comm packs
+    (core/comm_mat.cpp:53-96).  on and off are host (rowptr, cols, vals);
+    on_proc columns are local (global - first), off_proc columns index
+    colmap.  Returns (rowptr int64, cols int64, vals float64)."""
+    orp, oci, ocv = (np.asarray(a) for a in on)
+    frp, fci, fcv = (np.asarray(a) for a in off)
+    n = len(orp) - 1
+    on_len, off_len = np.diff(orp), np.diff(frp)
+    rowptr = np.zeros(n + 1, np.int64)
+    rowptr[1:] = np.cumsum(on_len + off_len)
+    cols = np.empty(int(rowptr[-1]), np.int64)
+    vals = np.empty(int(rowptr[-1]), np.float64)
+    r_on = np.repeat(np.arange(n), on_len)
+    dest = rowptr[r_on] + (np.arange(len(oci)) - orp[r_on])
+    cols[dest] = np.asarray(oci, np.int64) + first
+    vals[dest] = ocv
+    r_off = np.repeat(np.arange(n), off_len)
+    dest = rowptr[r_off] + on_len[r_off] + (np.arange(len(fci)) - frp[r_off])
+    cols[dest] = np.asarray(colmap, np.int64)[np.asarray(fci, np.int64)]
+    vals[dest] = fcv
+    return rowptr, cols, vals
+
+
 class ParComm:
     """Halo-exchange plan of one rank (core/comm_pkg.hpp:400-466).
 
@@ -220,6 +245,60 @@ class ParComm:
             ops.append(dist.P2POp(dist.isend, send_buf[a:b], q, group=group))
         return dist.batch_isend_irecv(ops) if ops else []
 
+    def communicate_rows(self, rowptr, cols, vals, group=None, device="cpu"):
+        """Matrix rows along the halo plan (CommPkg::communicate(ParCSRMatrix*),
+        core/comm_mat.cpp:39-96, 145-192): each receiver gets the rows of this
+        rank that its column map names, whole, in the order it lists them; this
+        rank gets, in its column-map order, the rows the other ranks own.
+        rowptr / cols / vals are this rank's rows on the host (global column
+        indices, global_rows); ``device`` is where the messages live (CUDA for
+        NCCL).  Row lengths go first, then the column indices, then the values;
+        a message without entries is not sent.  Every rank of the group must
+        call it.  Returns the received rows (rowptr int64, cols int64, vals
+        float64) on the host."""
+        import torch
+        import torch.distributed as dist
+
+        rowptr = np.asarray(rowptr, np.int64)
+        cols = np.asarray(cols, np.int64)
+        vals = np.asarray(vals, np.float64)
+        lens = np.diff(rowptr)
+        sent_len = lens[self.send_idx] if self.num_send else np.zeros(0, np.int64)
+        send_len = torch.as_tensor(sent_len if len(sent_len) else np.zeros(1, np.int64),
+                                   device=device)
+        recv_len = torch.zeros(max(self.num_recv, 1), dtype=torch.int64, device=device)
+        for w in self.exchange_packed(send_len, recv_len, group=group):
+            w.wait()
+        got_len = recv_len.cpu().numpy()[:self.num_recv]
+        # the entries of the sent rows, row after row, message after message
+        starts = rowptr[self.send_idx] if self.num_send else np.zeros(0, np.int64)
+        total = int(sent_len.sum())
+        pos = np.repeat(starts, sent_len) + (np.arange(total) - np.repeat(
+            np.cumsum(sent_len) - sent_len, sent_len))
+        send_eptr = np.concatenate([[0], np.cumsum(sent_len)])[self.send_ptr]
+        recv_eptr = np.concatenate([[0], np.cumsum(got_len)])[self.recv_ptr]
+        out = {}
+        for name, data, dtype in (("cols", cols, torch.int64), ("vals", vals, torch.float64)):
+            sbuf = torch.as_tensor(np.ascontiguousarray(data[pos]) if total else
+                                   np.zeros(1, data.dtype), device=device)
+            rbuf = torch.zeros(max(int(recv_eptr[-1]), 1), dtype=dtype, device=device)
+            ops = []
+            for k, q in enumerate(self.recv_procs):
+                a, b = int(recv_eptr[k]), int(recv_eptr[k + 1])
+                if b > a:
+                    ops.append(dist.P2POp(dist.irecv, rbuf[a:b], q, group=group))
+            for k, q in enumerate(self.send_procs):
+                a, b = int(send_eptr[k]), int(send_eptr[k + 1])
+                if b > a:
+                    ops.append(dist.P2POp(dist.isend, sbuf[a:b], q, group=group))
+            if ops:
+                for w in dist.batch_isend_irecv(ops):
+                    w.wait()
+            out[name] = rbuf.cpu().numpy()[:int(recv_eptr[-1])]
+        out_rowptr = np.zeros(self.num_recv + 1, np.int64)
+        out_rowptr[1:] = np.cumsum(got_len)
+        return out_rowptr, out["cols"], out["vals"]
+
     def exchange_packed_T(self, ghost_buf, recv_buf, group=None):
         """The transpose exchange (init_comm_T, core/comm_pkg.hpp:187-196):
         ghost_buf holds values in column-map order, each owner's run sent
@@ -298,6 +377,23 @@ class DistParCSRMatrix:
         with _on_stream():
             for w in reqs:
                 w.wait()
+
+    # ---------------------------------------------------------- row exchange
+    def communicate_rows(self, device="cuda"):
+        """The P-row exchange of the distributed Galerkin product
+        (CommPkg::communicate(ParCSRMatrix*), core/comm_mat.cpp:39-96): this
+        rank's rows that the other ranks' column maps name go to them, and the
+        rows this rank's column map names arrive, whole, with global column
+        indices (on_proc entries first), in column-map order, on the host."""
+        on = self.on_proc.arrays()
+        if self.off_proc is not None:
+            off = self.off_proc.arrays()
+        else:
+            off = (np.zeros(self.local_num_rows + 1, np.int32), np.zeros(0, np.int32),
+                   np.zeros(0, np.float64))
+        first = self.partition.local_range(self.rank)[0]
+        rows = global_rows(on, off, first, self.colmap)
+        return self.comm.communicate_rows(*rows, group=self.group, device=device)
 
     # ------------------------------------------------------------ products
     def mult(self, x, b):

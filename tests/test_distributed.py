@@ -8,8 +8,11 @@ must equal the plan computed for all ranks in one process, the exchange must
 deliver x at the column map, and on_proc x_local + off_proc x_ghost (taken
 here with numpy, as a check) must be that rank's rows of A x; the transpose
 exchange (off_proc^T x_local sent back to the owners and added into their
-rows) must give that rank's rows of A^T x.  The device
-products are covered by tests/test_gpu_distributed.py.
+rows) must give that rank's rows of A^T x.  The
+matrix-row exchange that the distributed Galerkin product needs
+(CommPkg::communicate, core/comm_mat.cpp:39-192) must deliver, in column-map
+order, the owners' rows with global columns, on_proc entries first.  The
+device products are covered by tests/test_gpu_distributed.py.
 """
 import os
 import socket
@@ -17,7 +20,7 @@ import socket
 import numpy as np
 import pytest
 
-from raptor_b200.distributed import ParComm, RowPartition, split_rows
+from raptor_b200.distributed import ParComm, RowPartition, global_rows, split_rows
 
 
 def random_csr(n, density, seed):
@@ -180,3 +183,66 @@ def test_gloo_plan_and_exchange(tmp_path, world, kind):
         assert same == 1.0, "plan differs on rank %d" % r
         assert ghost_ok == 1.0, "halo values wrong on rank %d" % r
         assert err < 1e-13 and err_t < 1e-13
+
+
+def owner_rows(rp, ci, cv, part, r):
+    f, l = part.local_range(r)
+    on, off, colmap = split_rows(rp[f:l + 1] - rp[f], ci[rp[f]:rp[l]], cv[rp[f]:rp[l]], f, l)
+    return global_rows(on, off, f, colmap), colmap
+
+
+def test_global_rows_keep_each_row():
+    """On_proc entries (global columns) then off_proc entries, per row; the
+    row's entries are the matrix row's."""
+    rp, ci, cv = random_csr(60, 0.08, 4)
+    part = RowPartition([0, 17, 41, 60])
+    for r in range(3):
+        f, l = part.local_range(r)
+        (grp, gci, gcv), _ = owner_rows(rp, ci, cv, part, r)
+        for i in range(l - f):
+            row_c, row_v = gci[grp[i]:grp[i + 1]], gcv[grp[i]:grp[i + 1]]
+            inside = (row_c >= f) & (row_c < l)
+            k = int(inside.sum())
+            assert inside[:k].all() and not inside[k:].any()
+            assert sorted(zip(row_c, row_v)) == sorted(zip(ci[rp[f + i]:rp[f + i + 1]],
+                                                            cv[rp[f + i]:rp[f + i + 1]]))
+
+
+def _rows_rank_main(rank, world, port, kind, out):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        n = 144 if kind == "stencil" else 90
+        rp, ci, cv = stencil_csr(12) if kind == "stencil" else random_csr(n, 0.06, 9)
+        part = (RowPartition.even(n, world) if kind == "stencil"
+                else RowPartition([0, 50, 51, 90][:world] + [n]))
+        (grp, gci, gcv), colmap = owner_rows(rp, ci, cv, part, rank)
+        plan = ParComm.build(part, colmap, rank)
+        rrp, rci, rcv = plan.communicate_rows(grp, gci, gcv)
+        ok = len(rrp) == len(colmap) + 1
+        for k, g in enumerate(colmap):
+            q = int(part.owner(np.array([g]))[0])
+            (orp, oci, ocv), _ = owner_rows(rp, ci, cv, part, q)
+            i = g - part.local_range(q)[0]
+            ok = ok and np.array_equal(rci[rrp[k]:rrp[k + 1]], oci[orp[i]:orp[i + 1]])
+            ok = ok and np.array_equal(rcv[rrp[k]:rrp[k + 1]], ocv[orp[i]:orp[i + 1]])
+        np.save(out % rank, np.array([float(ok), float(len(colmap)), float(rrp[-1])]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,kind", [(2, "stencil"), (3, "stencil"), (3, "random")])
+def test_gloo_matrix_rows_exchange(tmp_path, world, kind):
+    import torch.multiprocessing as mp
+
+    out = str(tmp_path / "r%d.npy")
+    mp.start_processes(_rows_rank_main, args=(world, _free_port(), kind, out), nprocs=world,
+                       start_method="spawn", join=True)
+    for r in range(world):
+        ok, n_ghost, n_entries = np.load(out % r)
+        assert ok == 1.0, "received rows differ on rank %d" % r
+        assert n_ghost == 0 or n_entries > 0
