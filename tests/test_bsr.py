@@ -320,3 +320,26 @@ def test_fixture_sort_diag_first_equals_reference(ref):
     np.testing.assert_array_equal(hv.reshape(-1), out_v[:nnz * A.b_rows * A.b_cols])
     B = O.BSR(A.n_rows, A.n_cols, A.b_rows, A.b_cols, hrp, hci, hv)
     np.testing.assert_array_equal(O.bsr_to_csr(B).to_scipy().toarray(), dense)
+
+
+def test_bench_block_pattern_is_in_bounds():
+    """bench.py's block CSR workload: 7 distinct in-range block columns a
+    block row, the diagonal block first, and the CLI default cases parse."""
+    import sys
+
+    import bench
+    rowptr, cols = bench.block_stencil_pattern(6)
+    nb = 6 ** 3
+    assert rowptr[0] == 0 and rowptr[-1] == len(cols) == 7 * nb
+    assert cols.min() >= 0 and cols.max() < nb
+    per_row = cols.reshape(nb, 7)
+    assert np.array_equal(per_row[:, 0], np.arange(nb))
+    assert all(len(set(r)) == 7 for r in per_row.tolist())
+    argv = sys.argv
+    try:
+        sys.argv = ["bench.py"]
+        cases = bench.parse().bsr_cases
+    finally:
+        sys.argv = argv
+    assert [tuple(int(v) for v in c.split("x")) for c in cases.split(",")] == [
+        (96, 3), (112, 2), (64, 4)]
